@@ -1,0 +1,465 @@
+"""Benchmark of the B200 Lagrangian parcel step (one JSON line on stdout, rank 0).
+
+Workload: 128^3 uniform hex mesh (2,097,152 cells) on
+[0, 0.1 m]^3, 1e7 parcels, Schiller-Naumann drag with explicit Euler, dt = 1e-4 s, one
+substep, mixed precision (FP64 positions, FP32 drag/velocity, deterministic fixed-point
+source reduced to FP64), Morton re-sort every 20 steps, time-varying Taylor-Green-like
+fluid field, seeded synthetic inputs.  A step = one call of the parcel step over every
+parcel (including the source finalize and, every 20th step, the re-sort).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+  value      particle-steps/s of the mixed deterministic step, inputs resident in HBM
+  e2e        same metric through the reference-facing C ABI (st_evolve_cloud) with pinned
+             host exchange arrays: U copied in and the source copied out every step
+  roofline   the step kernel's algorithmic bytes / its event-timed duration vs measured HBM
+  cpu_baseline  the CPU oracle (restatement of the reference's CPU path) on this host
+  fp64_*     the plain all-FP64 GPU step (FP64 atomics) on the same inputs
+--impl reference times the CPU restatement of the reference's path with all host threads.
+Multi-GPU (torchrun): every rank steps its own 1e7 parcels (weak scaling) against the
+replicated U, and the per-cell source is summed over ranks with an NCCL all-reduce.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "scale-track_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+for p in (PKG, ORACLE):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import workload  # noqa: E402
+
+METRIC = "particle-steps/s mixed vs FP64 on 1 B200 at src rel err<=1e-5; adjoint/fwd cost"
+UNIT = "particle-steps/s"
+CONFIG = workload.CONFIGS["c1_mixed_128"]
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nparcels", type=int, default=CONFIG["nparcels"])
+    ap.add_argument("--ncells", type=int, default=CONFIG["n"], help="cells per direction")
+    ap.add_argument("--fp64-steps", type=int, default=100)
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--accuracy-steps", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-extras", action="store_true", help="only the headline timing")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ----------------------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_index):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        self.gpu = ids[local_index] if local_index < len(ids) else str(local_index)
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic_per_parcel(precision):
+    """DRAM bytes per parcel of the step kernel from a committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "k_step_traffic.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)[precision]["dram_bytes_per_parcel"])
+    except Exception:
+        return None
+
+
+def make_params(st, precision, deposit="deterministic", sort_interval=None):
+    return st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                     drag_model="schiller_naumann", precision=precision, n_substeps=1,
+                     deposit=deposit,
+                     sort_interval=CONFIG["sort_interval"] if sort_interval is None
+                     else sort_interval)
+
+
+class DeviceTimer:
+    """CUDA events recorded on the library's stream (the launching stream)."""
+
+    def __init__(self, torch, stream_ptr, device):
+        self.torch = torch
+        self.stream = torch.cuda.ExternalStream(stream_ptr, device=device)
+        self.a = torch.cuda.Event(enable_timing=True)
+        self.b = torch.cuda.Event(enable_timing=True)
+
+    def start(self):
+        self.a.record(self.stream)
+
+    def stop(self):
+        self.b.record(self.stream)
+        self.b.synchronize()
+        return self.a.elapsed_time(self.b)  # ms
+
+
+class DevArray:
+    """Zero-copy view of a library-owned device array for torch (__cuda_array_interface__)."""
+
+    def __init__(self, ptr, n, typestr="<f8"):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3, "strides": None}
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import scaletrack as st
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+
+    n = args.ncells
+    npcl = args.nparcels
+    ncells = n ** 3
+    xyz, uvw, d = workload.parcels(npcl, CONFIG["seed"] + rank)
+    U = workload.tgv_field(n, dtype=np.float32)
+    mesh = st.mesh_desc(n, 0.0, workload.L_BOX)
+    dt = workload.DT
+    fs = lambda k: workload.fluid_scale(k, dt, CONFIG["time_varying"])  # noqa: E731
+
+    def barrier_sync():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    extras = {}
+    # ---- accuracy: mixed vs all-FP64 on the same inputs (source of the last step) ----
+    if not args.no_extras and rank == 0:
+        S = {}
+        for prec, dep in (("mixed", "deterministic"), ("fp64", "deterministic")):
+            with st.ParcelTracker(make_params(st, prec, dep), mesh, device=local) as h:
+                h.set_parcels(xyz, uvw, d)
+                h.set_fluid_velocity(U.astype(np.float64 if prec == "fp64" else np.float32))
+                for k in range(args.accuracy_steps):
+                    h.step(dt, fs(k))
+                h.synchronize()
+                S[prec] = h.get_source()
+                if prec == "mixed":
+                    cells_m = h.get_cells()
+                    pos_m = h.get_parcels()[0]
+                else:
+                    cells_d = h.get_cells()
+                    pos_d = h.get_parcels()[0]
+        ref = S["fp64"]
+        extras["src_rel_err_mixed_vs_fp64"] = float(np.abs(S["mixed"] - ref).max() /
+                                                    np.abs(ref).max())
+        extras["src_rel_err_l2_mixed_vs_fp64"] = float(np.linalg.norm(S["mixed"] - ref) /
+                                                       np.linalg.norm(ref))
+        extras["pos_rel_err_mixed_vs_fp64"] = float(np.abs(pos_m - pos_d).max() /
+                                                    workload.L_BOX)
+        extras["cells_differing_mixed_vs_fp64"] = int(np.sum(cells_m != cells_d))
+        extras["accuracy_steps"] = args.accuracy_steps
+
+    # ---- headline: mixed deterministic step, device-resident ----
+    h = st.ParcelTracker(make_params(st, "mixed"), mesh, device=local)
+    h.set_parcels(xyz, uvw, d)
+    h.set_fluid_velocity(U)
+    src_view = None
+    if pg is not None:
+        src_view = torch.as_tensor(DevArray(h.source_device_ptr(0), 3 * ncells), device=dev)
+        # one stream for the library and the collective
+        st.lib().st_set_stream(h.handle, torch.cuda.current_stream(dev).cuda_stream)
+    timer = DeviceTimer(torch, h.stream(), dev)
+    k = 0
+    for _ in range(args.warmup):
+        h.step(dt, fs(k))
+        if src_view is not None:
+            pg.all_reduce(src_view)
+        k += 1
+    h.synchronize()
+    barrier_sync()
+    h.profile(True)
+    h.profile_read("step", reset=True)
+    launches0 = h.launch_count()
+    with ClockSampler(local) as clk:
+        timer.start()
+        for _ in range(args.steps):
+            h.step(dt, fs(k))
+            if src_view is not None:
+                pg.all_reduce(src_view)
+            k += 1
+        ms = timer.stop()
+    launches = h.launch_count() - launches0
+    nstep, step_ms = h.profile_read("step")
+    nfin, fin_ms = h.profile_read("finalize")
+    nsort, sort_ms = h.profile_read("sort")
+    h.profile(False)
+    h.synchronize()
+    barrier_sync()
+    if pg is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
+    ms_per_step = ms / args.steps
+    value = ws * npcl * args.steps / (ms / 1e3)
+
+    peak, peak_src = measured_hbm_peak()
+    algo_step = workload.step_kernel_bytes("mixed", npcl, ncells)
+    step_avg_ms = step_ms / max(nstep, 1)
+    achieved = algo_step / (step_avg_ms / 1e3) / 1e9
+    tpp = ncu_traffic_per_parcel("mixed")
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4),
+                "traffic": None if tpp is None else round(tpp * npcl),
+                "kernel": "k_step<double,float,DET1>", "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": algo_step,
+                "avg_launch_ms": round(step_avg_ms, 5)}
+    whole_step_frac = workload.algorithmic_bytes("mixed", npcl, ncells) / (ms_per_step / 1e3) \
+        / 1e9 / peak
+    extras["kernel_ms_per_step"] = {"step": round(step_avg_ms, 5),
+                                    "finalize": round(fin_ms / max(nfin, 1), 5),
+                                    "sort_per_call": round(sort_ms / max(nsort, 1), 5),
+                                    "sort_calls": nsort}
+    extras["whole_step_hbm_frac"] = round(whole_step_frac, 4)
+    h.close()
+
+    # ---- the plain FP64 GPU step (FP64 atomics), same inputs ----
+    if not args.no_extras and rank == 0 and args.fp64_steps > 0:
+        with st.ParcelTracker(make_params(st, "fp64", "atomic"), mesh, device=local) as h64:
+            h64.set_parcels(xyz, uvw, d)
+            h64.set_fluid_velocity(U.astype(np.float64))
+            t64 = DeviceTimer(torch, h64.stream(), dev)
+            for j in range(args.warmup):
+                h64.step(dt, fs(j))
+            h64.synchronize()
+            t64.start()
+            for j in range(args.fp64_steps):
+                h64.step(dt, fs(args.warmup + j))
+            ms64 = t64.stop()
+        extras["fp64_value"] = npcl * args.fp64_steps / (ms64 / 1e3)
+        extras["fp64_ms_per_step"] = ms64 / args.fp64_steps
+        extras["mixed_over_fp64"] = round(value / ws / extras["fp64_value"], 3)
+
+    # ---- end to end through the reference-facing shim (pinned host exchange arrays) ----
+    e2e = None
+    if not args.no_extras and rank == 0 and args.e2e_steps > 0:
+        st.setup(make_params(st, "mixed"), mesh)
+        hd = st.default_handle()
+        if st.lib().st_set_parcels(hd, 0, npcl, xyz.ctypes.data, uvw.ctypes.data,
+                                   d.ctypes.data) != 0:
+            raise RuntimeError(st.last_error())
+        Uh = st.allocate_array("U", ncells, 3, 4)
+        UT = st.allocate_array("UTrans", ncells, 3, 4)
+        Uh[:] = U
+        for j in range(args.warmup):
+            st.evolve_cloud(dt)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for j in range(args.e2e_steps):
+            st.evolve_cloud(dt)
+        el = time.perf_counter() - t0
+        assert np.isfinite(UT).all()
+        st.finalize()
+        e2e = {"value": npcl * args.e2e_steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": ncells * 3 * 4, "d2h_bytes_per_step": ncells * 3 * 4,
+               "steps": args.e2e_steps,
+               "path": "st_evolve_cloud: U (float32 [nCells][3], pinned) H2D, step, source "
+                       "(float32 UTrans, pinned) D2H; fixed fluid scale"}
+
+    # ---- CPU baseline: the oracle on this host's cores (bounded sample) ----
+    cpu = None
+    if not args.no_extras and rank == 0 and args.cpu_seconds > 0:
+        cpu = cpu_rate(n, xyz, uvw, d, U, args.cpu_seconds)
+
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 positions / f32 drag+velocity "
+        "/ int64 fixed-point source -> f64",
+        "data": "synthetic (seeded uniform parcels, lognormal diameters, analytic TGV field)",
+        "config": {"workload": "BASELINE config 1: 128^3 hex (2,097,152 cells), 1e7 parcels "
+                               "per GPU, Schiller-Naumann explicit, dt=1e-4 s, 1 substep, "
+                               "mixed precision, Morton re-sort every 20 steps, "
+                               "time-varying field",
+                   "nparcels_per_gpu": npcl, "ncells": ncells,
+                   "sort_interval": CONFIG["sort_interval"],
+                   "l2": "inputs larger than L2: parcel state %d MB per GPU" % (npcl * 40 // 10**6),
+                   "parallelism": "dp%d (parcels sharded, U replicated, source all-reduced)" % ws},
+        "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    line.update(extras)
+    print(json.dumps(line), flush=True)
+
+
+def cpu_rate(n, xyz, uvw, d, U, budget_s, threads=None):
+    """The CPU oracle (mixed precision, same physics) on a bounded sample of the workload."""
+    import oracle
+    threads = threads or len(os.sched_getaffinity(0))
+    cfg = oracle.make_cfg(n, 0.0, workload.L_BOX, workload.MU_F, workload.RHO_F,
+                          workload.RHO_P, drag="sn_explicit", precision="mixed", n_substeps=1)
+    U64 = U.astype(np.float64)
+    # calibrate on a small sample, then size the measured sample to the time budget
+    m = min(200_000, d.size)
+    t0 = time.perf_counter()
+    oracle.run(cfg, xyz[:, :m], uvw[:, :m], d[:m], U64, 1, workload.DT, want_seq=False,
+               nthreads=threads)
+    t1 = time.perf_counter() - t0
+    rate0 = m / max(t1, 1e-6)
+    steps = 3
+    m2 = int(min(d.size, max(m, rate0 * budget_s / steps)))
+    t0 = time.perf_counter()
+    oracle.run(cfg, xyz[:, :m2], uvw[:, :m2], d[:m2], U64, steps, workload.DT,
+               fscale=[workload.fluid_scale(k) for k in range(steps)], want_seq=False,
+               nthreads=threads)
+    el = time.perf_counter() - t0
+    return {"value": m2 * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{m2} parcels x {steps} steps of the same 128^3 workload "
+                      f"(deterministic fixed-point source), {threads} OpenMP threads"}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    """The reference's path on the host cores: its CPU executor (a serial loop over the
+    parcels calling evolve_particle!, asyncParallelTracking.jl:818-823) restated in C++ (the
+    oracle; Julia is not available), parallelised over all host threads."""
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    threads = len(os.sched_getaffinity(0))
+    n = args.ncells
+    npcl = args.nparcels
+    xyz, uvw, d = workload.parcels(npcl, CONFIG["seed"])
+    U = workload.tgv_field(n, dtype=np.float32).astype(np.float64)
+    cfg = oracle.make_cfg(n, 0.0, workload.L_BOX, workload.MU_F, workload.RHO_F,
+                          workload.RHO_P, drag="sn_explicit", precision="mixed", n_substeps=1)
+    # bounded per-step sample so that warmup + steps finish in a few minutes
+    m = min(100_000, npcl)
+    t0 = time.perf_counter()
+    oracle.run(cfg, xyz[:, :m], uvw[:, :m], d[:m], U, 1, workload.DT, want_quant=False,
+               nthreads=threads)
+    per = (time.perf_counter() - t0) / m
+    total_steps = args.warmup + args.steps
+    budget = 150.0
+    sample = int(max(10_000, min(npcl, budget / max(total_steps, 1) / max(per, 1e-9))))
+    xs, us, ds = xyz[:, :sample].copy(), uvw[:, :sample].copy(), d[:sample]
+    fsw = [workload.fluid_scale(k) for k in range(args.warmup)]
+    # the reference's own accumulation: a plain sum into UTrans (A:706), no fixed point
+    r = oracle.run(cfg, xs, us, ds, U, args.warmup, workload.DT, fscale=fsw, want_quant=False,
+                   nthreads=threads)
+    fst = [workload.fluid_scale(args.warmup + k) for k in range(args.steps)]
+    t0 = time.perf_counter()
+    oracle.run(cfg, r["xyz"], r["uvw"], ds, U, args.steps, workload.DT, fscale=fst,
+               want_quant=False, nthreads=threads)
+    el = time.perf_counter() - t0
+    value = sample * args.steps / el
+    desc = (f"{sample} of {npcl} parcels per step (128^3 mesh, same physics and inputs), "
+            f"{threads} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 positions / f32 drag+velocity",
+        "data": "synthetic (seeded uniform parcels, lognormal diameters, analytic TGV field)",
+        "config": {"workload": "BASELINE config 1 on the host CPU: 128^3 hex, Schiller-Naumann "
+                               "explicit, dt=1e-4 s, mixed precision; bounded parcel sample",
+                   "nparcels_sampled": sample, "ncells": n ** 3},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -1,0 +1,174 @@
+/*
+ * scaletrack.h -- C ABI of the B200 Lagrangian parcel step (libscaletrack.so).
+ *
+ * The library replaces the parcel step that SCALE-TRACK's icoFoam coupling calls once per
+ * fluid time step: cell-value fluid velocity lookup at each parcel, drag plus time
+ * integration, relocation into the owning cell with wall bounce, and the two-way momentum
+ * source deposited back to the cells.  Exchange arrays keep the reference layout: cell
+ * velocity U in, per-cell momentum source out, both cell-major [nCells][3].
+ *
+ * Reference files cited below:
+ *   A: run/icoJuliaParcelFoam/cavity3D/asyncParallelTracking.jl
+ *   F: sol/icoJuliaParcelFoam/  (the C++ side of the coupling)
+ *
+ * Conventions: every function returns an int status (ST_OK = 0) unless stated otherwise;
+ * st_last_error() returns a thread-local message for the last failure on the calling
+ * thread.  Host pointers are plain host memory (pageable or pinned); "_device" entry points
+ * take device pointers.  No CUDA types appear in the signatures: a stream is passed as
+ * void* holding a cudaStream_t.  Cell indices are 0-based (the reference's posI - 1).
+ */
+#ifndef SCALETRACK_H
+#define SCALETRACK_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ST_API __attribute__((visibility("default")))
+#else
+#define ST_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------- */
+enum {
+    ST_OK = 0,
+    ST_ERR_INVALID_ARGUMENT = 1, /* bad size, pointer, name or parameter                    */
+    ST_ERR_CUDA = 2,             /* a CUDA runtime call failed (message has the CUDA error) */
+    ST_ERR_PARCEL_OUTSIDE = 3,   /* a parcel could not be located inside the mesh           */
+    ST_ERR_SOURCE_RANGE = 4,     /* a deposit exceeded the deterministic fixed-point range  */
+    ST_ERR_NOT_INITIALISED = 5,  /* shim called before st_setup                             */
+    ST_ERR_OUT_OF_MEMORY = 6
+};
+
+/* ---- models and modes ---------------------------------------------------------------- */
+enum {
+    ST_DRAG_STOKES_IMPLICIT = 0, /* f = 18 mu dt/(rho_d d^2); v' = (v + f u)/(1 + f): A:1294-1295 */
+    ST_DRAG_SCHILLER_NAUMANN = 1 /* v' = v + f (1 + 0.15 Re^0.687)(u - v), explicit Euler       */
+};
+enum {
+    ST_PREC_FP32 = 0,  /* all single precision: the reference's arithmetic (A:172)   */
+    ST_PREC_MIXED = 1, /* FP64 positions and cell location, FP32 drag and velocity   */
+    ST_PREC_FP64 = 2   /* all double precision                                        */
+};
+enum {
+    ST_DEPOSIT_DETERMINISTIC = 0, /* warp-aggregated fixed-point sums: bitwise reproducible */
+    ST_DEPOSIT_ATOMIC = 1         /* one FP64 atomicAdd per deposit (A:714-725 in FP64)     */
+};
+
+/* Uniform cuboid mesh, cells numbered x fastest (A:222-270, A:684-691). */
+typedef struct st_mesh_desc {
+    int32_t n[3];      /* cells per direction */
+    double origin[3];  /* lower corner */
+    double ending[3];  /* upper corner */
+} st_mesh_desc;
+
+typedef struct st_params {
+    double mu_c;              /* carrier dynamic viscosity      (A: μᶜ)   */
+    double rho_c;             /* carrier density                (A: ρᶜ)   */
+    double rho_d;             /* parcel density                 (A: ρᵈ)   */
+    int32_t drag_model;       /* ST_DRAG_*                                 */
+    int32_t precision;        /* ST_PREC_*                                 */
+    int32_t deposit;          /* ST_DEPOSIT_*                              */
+    int32_t n_substeps;       /* substeps per call; 10 in the reference (A:1260) */
+    int32_t sort_interval;    /* Morton re-sort of the parcels every k steps; 0 = never */
+    int32_t n_clouds;         /* independent parcel clouds, each with its own source field */
+    int32_t block_size;       /* threads per block of the step kernel; 0 = default (256) */
+    int32_t grid_blocks;      /* blocks of the step kernel; 0 = from occupancy x SM count */
+    double drag_multiplier;   /* multiplies the drag factor; 1 reproduces the reference */
+    double diameter_scale;    /* multiplies every diameter;  1 reproduces the reference */
+} st_params;
+
+typedef struct st_handle st_handle;
+
+/* Library version, e.g. "scaletrack-b200 0.1 sm_100a". */
+ST_API const char* st_version(void);
+/* Thread-local message describing the last failure on this thread ("" if none). */
+ST_API const char* st_last_error(void);
+
+/* Defaults: the reference's physics (setup.jl: mu_c 1e-3, rho_c 1e3, rho_d 1), Stokes
+ * implicit drag, FP32, deterministic deposit, 10 substeps, one cloud, no re-sort. */
+ST_API void st_params_default(st_params* p);
+
+/* Creates a handle on CUDA device `device`.  Allocates the per-cell arrays (U, source,
+ * fixed-point accumulators) and a stream.  Replaces the Julia-side set-up of Mesh,
+ * TwoWayEulerian and the device arrays (A:1560-1620, A:934-964). */
+ST_API int st_create(const st_params* p, const st_mesh_desc* mesh, int device, st_handle** out);
+ST_API int st_destroy(st_handle* h);
+
+/* Parcels of cloud `cloud` (0 <= cloud < n_clouds), SoA host arrays: xyz = [3][n]
+ * (x block, y block, z block), uvw = [3][n], d = [n].  Values are converted to the handle's
+ * precision.  Every parcel must lie inside the mesh (else ST_ERR_PARCEL_OUTSIDE).  Replaces
+ * allocate!/initWithHilbert! (A:474-482, A:559-638) with caller-provided parcels. */
+ST_API int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
+                   const double* d);
+/* Current parcel state in the order given to st_set_parcels (re-sorting is undone). */
+ST_API int st_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d);
+/* 0-based owning cell of each parcel (locate, A:680-693), order as st_set_parcels. */
+ST_API int st_get_cells(st_handle* h, int cloud, int32_t* cells);
+ST_API int64_t st_num_parcels(st_handle* h, int cloud);
+ST_API int64_t st_num_cells(st_handle* h);
+
+/* Cell velocity U, [nCells][3] with 4- or 8-byte components (host or device memory).
+ * Replaces copyto!(deviceEulerian.U, eulerian.U) (A:1079-1083). */
+ST_API int st_set_fluid_velocity(st_handle* h, const void* U, int elem_bytes);
+ST_API int st_set_fluid_velocity_device(st_handle* h, const void* U, int elem_bytes);
+
+/* One call of the parcel step for every cloud: n_substeps substeps of dt/n_substeps
+ * (evolve_on_device!, A:1258-1365), fluid velocity U scaled by fluid_scale, followed by the
+ * source reduction.  Asynchronous on the handle's stream.  Errors found on the device
+ * (lost parcels, fixed-point range) are reported by the next st_synchronize,
+ * st_get_source, st_get_parcels or st_get_cells. */
+ST_API int st_step(st_handle* h, double dt, double fluid_scale);
+
+/* Per-cell momentum source of the last step for `cloud`, [nCells][3], 4- or 8-byte
+ * components: the sum over deposits of (rho_d/rho_c)(pi d^3/6)(state0 - v) (A:703-725),
+ * not divided by the cell volume or dt, exactly as the reference's UTrans.  Synchronous. */
+ST_API int st_get_source(st_handle* h, int cloud, void* S, int elem_bytes);
+/* Device pointer to the FP64 source [nCells][3] of `cloud`, valid until st_destroy. */
+ST_API const double* st_source_device(st_handle* h, int cloud);
+
+/* Waits for the handle's stream and reports device-side errors. */
+ST_API int st_synchronize(st_handle* h);
+/* The handle's cudaStream_t, and a way to run on a caller-owned stream instead. */
+ST_API void* st_get_stream(st_handle* h);
+ST_API int st_set_stream(st_handle* h, void* stream);
+
+/* ---- instrumentation --------------------------------------------------------------- */
+enum { ST_KERNEL_STEP = 0, ST_KERNEL_FINALIZE = 1, ST_KERNEL_SORT = 2, ST_KERNEL_PROBE = 3,
+       ST_KERNEL_OTHER = 4, ST_KERNEL_KINDS = 5 };
+/* Record CUDA events around every kernel the library launches (on the launching stream). */
+ST_API int st_profile_enable(st_handle* h, int on);
+/* Launch count and summed device time (ms) of one kernel kind since the last reset;
+ * synchronises the stream.  reset != 0 clears the counters afterwards. */
+ST_API int st_profile_read(st_handle* h, int kind, int64_t* launches, double* ms, int reset);
+/* Total number of kernels the library launched on this handle. */
+ST_API int64_t st_launch_count(st_handle* h);
+
+/* ---- shims with the reference's names and semantics -------------------------------- */
+/* Creates (or replaces) the process-wide default handle used by the two calls below, on
+ * the current CUDA device; then st_default_handle() gives it to st_set_parcels & co. */
+ST_API int st_setup(const st_params* p, const st_mesh_desc* mesh);
+ST_API st_handle* st_default_handle(void);
+/* allocate_array_ptr (A:1436-1483; called from F/juliaWrapper.H:129-141): returns library
+ * owned, pinned host storage [size][nComponents] for "U" or "UTrans" that the caller
+ * adopts as its field storage.  typeByteSize is 4 or 8, size must equal the cell count and
+ * nComponents must be 3; otherwise NULL (the reference throws).  Repeated calls with the
+ * same name return the same pointer while the size and type agree. */
+ST_API void* st_allocate_array(const char* name, int size, int nComponents, int typeByteSize);
+/* evolve_cloud (A:1485-1528; called at F/icoJuliaParcelFoam.C:123): copies the adopted
+ * "U" to the device, runs st_step(dt, 1) on the default handle and writes the source of
+ * cloud 0 into the adopted "UTrans" before returning (the synchronous variant of the
+ * reference's coupling, syncSerialTracking.jl:547-567). */
+ST_API int st_evolve_cloud(double dt);
+/* Releases the default handle and the adopted arrays (F/juliaWrapper.C:33-50 detaches
+ * the caller's fields first). */
+ST_API int st_finalize(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCALETRACK_H */

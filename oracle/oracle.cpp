@@ -1,0 +1,293 @@
+/*
+ * oracle.cpp -- TEST INFRASTRUCTURE ONLY: C entry points around step_oracle.hpp so that the
+ * Python tests, __graft_entry__.smoke() and bench.py's CPU-baseline leg can run the CPU
+ * restatement through ctypes.  Nothing in the shipped library links or calls this file.
+ *
+ * The driver loop follows the reference's CPU executor (A:818-823: a serial loop over the
+ * parcels of a chunk calling evolve_particle!) with the time step handling of A:487-502 and
+ * A:1260 (the substep is Δt/nSteps, with Δt held in the parcel precision).
+ */
+#include <cstdint>
+#include <cstring>
+#include <climits>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "step_oracle.hpp"
+
+using namespace st_oracle;
+
+extern "C" {
+
+typedef struct oracle_cfg {
+    int32_t n[3];
+    double origin[3];
+    double ending[3];
+    double mu_c;
+    double rho_c;
+    double rho_d;
+    int32_t drag;         /* 0 Stokes implicit (reference), 1 Schiller-Naumann explicit */
+    int32_t precision;    /* 0 FP32 (reference), 1 mixed, 2 FP64 */
+    int32_t n_substeps;   /* 10 in the reference (A:1260) */
+    int32_t quant_limbs;  /* 1 or 2: fixed-point model of the deterministic deposit */
+    double drag_multiplier;
+    double diameter_scale;
+} oracle_cfg;
+
+}  // extern "C"
+
+namespace {
+
+struct Acc {
+    double* seq = nullptr;       /* FP64 sum of the deposits, parcel order */
+    int64_t* q1 = nullptr;       /* one-limb fixed point */
+    int64_t* hi = nullptr;       /* two-limb fixed point: high part */
+    uint64_t* lo = nullptr;      /* two-limb fixed point: low 32 bits */
+    int limbs = 1;
+    int L = 0;
+    int H = 0;
+    bool parallel = false;
+};
+
+template <class V>
+struct AccSink : Sink<V> {
+    Acc* a;
+    bool quant;
+    int emax = EXP_NONE;
+    int64_t overflow = 0;
+    int64_t count = 0;
+    explicit AccSink(Acc* acc, bool q) : a(acc), quant(q) {}
+    void deposit(int32_t posI, V d0, V d1, V d2) override
+    {
+        const int64_t base = 3 * (int64_t)(posI - 1);
+        const V comp[3] = {d0, d1, d2};
+        ++count;
+        for (int k = 0; k < 3; ++k) {
+            double dv = (double)comp[k];
+            if (a->seq) {
+                if (a->parallel) {
+#pragma omp atomic
+                    a->seq[base + k] += dv;
+                } else {
+                    a->seq[base + k] += dv;
+                }
+            }
+            if (!quant || dv == 0.0) continue;
+            if (!std::isfinite(dv)) { ++overflow; continue; }
+            int e = exp_of(dv);
+            emax = std::max(emax, e);
+            if (e - a->L > a->H + QUANT_GROWTH_BITS) { ++overflow; continue; }
+            int64_t q = std::llrint(ldexp2(dv, -a->L));
+            if (!a->q1 && !a->hi) continue;          /* probe pass */
+            if (a->limbs == 1) {
+                uint64_t* p = reinterpret_cast<uint64_t*>(a->q1 + base + k);
+                if (a->parallel) {
+#pragma omp atomic
+                    *p += (uint64_t)q;
+                } else {
+                    *p += (uint64_t)q;
+                }
+            } else {
+                int64_t h = q >> 32;
+                uint64_t l = (uint64_t)q & 0xffffffffULL;
+                if (a->parallel) {
+#pragma omp atomic
+                    a->hi[base + k] += h;
+#pragma omp atomic
+                    a->lo[base + k] += l;
+                } else {
+                    a->hi[base + k] += h;
+                    a->lo[base + k] += l;
+                }
+            }
+        }
+    }
+};
+
+template <class P, class V>
+int run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const double* d,
+        const double* U, int nsteps, double dt, const double* fscale, double* src_seq,
+        double* src_quant, int32_t* cells, int32_t* scale_io, int64_t* stats, int nthreads)
+{
+    Params<P, V> pr = make_params<P, V>(cfg->n, cfg->origin, cfg->ending, cfg->mu_c, cfg->rho_c,
+                                        cfg->rho_d, cfg->drag, cfg->n_substeps,
+                                        cfg->drag_multiplier, cfg->diameter_scale);
+    const int64_t nC = pr.mesh.nCells;
+    std::vector<P> X(np), Y(np), Z(np);
+    std::vector<V> Uu(np), Vv(np), Ww(np), D(np);
+    for (int64_t i = 0; i < np; ++i) {
+        X[i] = (P)xyz[i]; Y[i] = (P)xyz[np + i]; Z[i] = (P)xyz[2 * np + i];
+        Uu[i] = (V)uvw[i]; Vv[i] = (V)uvw[np + i]; Ww[i] = (V)uvw[2 * np + i];
+        D[i] = (V)d[i];
+    }
+    /* Time step in the parcel precision: Time.Δt is a Float32 (A:324-327), the substep is
+     * Δt/nSteps (A:1260).  Mixed precision keeps the substep in FP64 for positions. */
+    const P dtP = (P)dt / (P)cfg->n_substeps;
+    const V dtV = (V)dtP;
+
+    const bool quant = (src_quant != nullptr);
+    const int limbs = cfg->quant_limbs == 2 ? 2 : 1;
+    std::vector<int64_t> q1, hi;
+    std::vector<uint64_t> lo;
+    std::vector<double> seq;
+    if (quant) {
+        if (limbs == 1) q1.assign(3 * nC, 0);
+        else { hi.assign(3 * nC, 0); lo.assign(3 * nC, 0); }
+    }
+    seq.assign(src_seq ? 3 * nC : 0, 0.0);
+    const int64_t nbound = std::max<int64_t>(2, np * (int64_t)cfg->n_substeps);
+    const int H = quant_headroom(limbs, nbound);
+    int L = scale_io ? *scale_io : INT_MIN;
+    int64_t lost = 0, overflow = 0;
+
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    const bool par = nthreads != 1;
+
+    for (int s = 0; s < nsteps; ++s) {
+        const V fs = fscale ? (V)fscale[s] : (V)1;
+        if (quant && L == INT_MIN) {
+            /* probe: the deposits of this step without committing the state */
+            Acc pa;
+            pa.limbs = limbs; pa.L = 0; pa.H = 1 << 20; pa.parallel = false;
+            int emax = EXP_NONE;
+#pragma omp parallel for schedule(static) reduction(max : emax) if (par)
+            for (int64_t i = 0; i < np; ++i) {
+                AccSink<V> sk(&pa, true);
+                P x = X[i], y = Y[i], z = Z[i];
+                V u = Uu[i], v = Vv[i], w = Ww[i];
+                evolve_parcel<P, V>(pr, dtP, dtV, U, fs, x, y, z, u, v, w, D[i], sk);
+                emax = std::max(emax, sk.emax);
+            }
+            L = (emax == EXP_NONE) ? -H : emax - H;
+        }
+        const bool last = (s == nsteps - 1);
+        Acc acc;
+        acc.limbs = limbs; acc.L = L; acc.H = H; acc.parallel = par;
+        if (src_seq) { std::fill(seq.begin(), seq.end(), 0.0); acc.seq = seq.data(); }
+        if (quant) {
+            if (limbs == 1) { std::fill(q1.begin(), q1.end(), 0); acc.q1 = q1.data(); }
+            else {
+                std::fill(hi.begin(), hi.end(), 0); std::fill(lo.begin(), lo.end(), 0);
+                acc.hi = hi.data(); acc.lo = lo.data();
+            }
+        }
+        int emax = EXP_NONE;
+        int64_t lost_s = 0, ovf_s = 0;
+#pragma omp parallel for schedule(static) reduction(max : emax) reduction(+ : lost_s, ovf_s) if (par)
+        for (int64_t i = 0; i < np; ++i) {
+            AccSink<V> sk(&acc, quant);
+            if (!evolve_parcel<P, V>(pr, dtP, dtV, U, fs, X[i], Y[i], Z[i], Uu[i], Vv[i], Ww[i],
+                                     D[i], sk))
+                ++lost_s;
+            emax = std::max(emax, sk.emax);
+            ovf_s += sk.overflow;
+        }
+        lost += lost_s;
+        overflow += ovf_s;
+        if (last && quant) {
+            for (int64_t j = 0; j < 3 * nC; ++j) {
+                double v;
+                if (limbs == 1) {
+                    v = (double)q1[j];
+                } else {
+                    int64_t h = hi[j] + (int64_t)(lo[j] >> 32);
+                    uint64_t l = lo[j] & 0xffffffffULL;
+                    v = (double)h * 4294967296.0 + (double)l;
+                }
+                src_quant[j] = ldexp2(v, L);
+            }
+        }
+        if (quant && emax != EXP_NONE) L = emax - H;
+    }
+    if (src_seq) std::memcpy(src_seq, seq.data(), sizeof(double) * 3 * nC);
+    if (scale_io) *scale_io = L;
+
+    for (int64_t i = 0; i < np; ++i) {
+        xyz[i] = (double)X[i]; xyz[np + i] = (double)Y[i]; xyz[2 * np + i] = (double)Z[i];
+        uvw[i] = (double)Uu[i]; uvw[np + i] = (double)Vv[i]; uvw[2 * np + i] = (double)Ww[i];
+        if (cells) {
+            bool bad = false;
+            Loc l = locate(pr.mesh, X[i], Y[i], Z[i], bad);
+            cells[i] = (bad || l.partitionI != 1) ? -1 : l.posI - 1;
+        }
+    }
+    if (stats) { stats[0] = lost; stats[1] = overflow; stats[2] = H; }
+    return (int)(lost > 0 ? 1 : 0) | (overflow > 0 ? 2 : 0);
+}
+
+}  // namespace
+
+extern "C" {
+
+/* Runs nsteps steps of the parcel step on the CPU.
+ *  xyz, uvw : [3][np] SoA, in/out (values are converted to the configured precision)
+ *  d        : [np] diameters;  U: [nCells][3] cell velocity (AoS, the exchange layout)
+ *  fscale   : per-step factor on U, or NULL for 1
+ *  src_seq  : [nCells][3] FP64 sum of the last step's deposits in parcel order, or NULL
+ *  src_quant: [nCells][3] fixed-point model of the library's deterministic deposit, or NULL
+ *  cells    : [np] 0-based owning cell after the last step (-1 if lost), or NULL
+ *  scale_io : in: scale exponent for the first step (INT_MIN: probe); out: for the next step
+ *  stats    : [3] lost parcels, overflowing deposits, headroom bits H (or NULL)
+ * Returns 0, or a bit set: 1 = some parcel could not be located, 2 = deposit overflow. */
+int oracle_run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const double* d,
+               const double* U, int nsteps, double dt, const double* fscale, double* src_seq,
+               double* src_quant, int32_t* cells, int32_t* scale_io, int64_t* stats, int nthreads)
+{
+    switch (cfg->precision) {
+    case 0:
+        return run<float, float>(cfg, np, xyz, uvw, d, U, nsteps, dt, fscale, src_seq, src_quant,
+                                 cells, scale_io, stats, nthreads);
+    case 1:
+        return run<double, float>(cfg, np, xyz, uvw, d, U, nsteps, dt, fscale, src_seq, src_quant,
+                                  cells, scale_io, stats, nthreads);
+    case 2:
+        return run<double, double>(cfg, np, xyz, uvw, d, U, nsteps, dt, fscale, src_seq,
+                                   src_quant, cells, scale_io, stats, nthreads);
+    default:
+        return -1;
+    }
+}
+
+/* 0-based owning cell of each position (locate, A:680-693), -1 if outside. */
+int oracle_locate(const oracle_cfg* cfg, int64_t np, const double* xyz, int32_t* cells)
+{
+    for (int64_t i = 0; i < np; ++i) {
+        bool bad = false;
+        Loc l;
+        if (cfg->precision == 0) {
+            Mesh<float> m = make_mesh<float>(cfg->n, cfg->origin, cfg->ending);
+            l = locate<float>(m, (float)xyz[i], (float)xyz[np + i], (float)xyz[2 * np + i], bad);
+        } else {
+            Mesh<double> m = make_mesh<double>(cfg->n, cfg->origin, cfg->ending);
+            l = locate<double>(m, xyz[i], xyz[np + i], xyz[2 * np + i], bad);
+        }
+        cells[i] = (bad || l.partitionI != 1) ? -1 : l.posI - 1;
+    }
+    return 0;
+}
+
+void oracle_pow0687(int64_t n, const double* x, double* y)
+{
+    for (int64_t i = 0; i < n; ++i) y[i] = st_pow0687(x[i]);
+}
+
+void oracle_pow0687f(int64_t n, const float* x, float* y)
+{
+    for (int64_t i = 0; i < n; ++i) y[i] = st_pow0687f(x[i]);
+}
+
+int oracle_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,147 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes access to the CPU oracle (liboracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module; it
+is the checker, never the thing measured for the GPU path or shipped in the library.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+PREC = {"fp32": 0, "mixed": 1, "fp64": 2}
+DRAG = {"stokes_implicit": 0, "sn_explicit": 1}
+INT_MIN = -(2 ** 31)
+
+
+class OracleCfg(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32 * 3),
+        ("origin", ctypes.c_double * 3),
+        ("ending", ctypes.c_double * 3),
+        ("mu_c", ctypes.c_double),
+        ("rho_c", ctypes.c_double),
+        ("rho_d", ctypes.c_double),
+        ("drag", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("n_substeps", ctypes.c_int32),
+        ("quant_limbs", ctypes.c_int32),
+        ("drag_multiplier", ctypes.c_double),
+        ("diameter_scale", ctypes.c_double),
+    ]
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        L.oracle_run.argtypes = [
+            P(OracleCfg), ctypes.c_int64, P(ctypes.c_double), P(ctypes.c_double),
+            P(ctypes.c_double), P(ctypes.c_double), ctypes.c_int, ctypes.c_double,
+            P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_int32),
+            P(ctypes.c_int32), P(ctypes.c_int64), ctypes.c_int,
+        ]
+        L.oracle_run.restype = ctypes.c_int
+        L.oracle_locate.argtypes = [P(OracleCfg), ctypes.c_int64, P(ctypes.c_double),
+                                    P(ctypes.c_int32)]
+        L.oracle_pow0687.argtypes = [ctypes.c_int64, P(ctypes.c_double), P(ctypes.c_double)]
+        L.oracle_pow0687f.argtypes = [ctypes.c_int64, P(ctypes.c_float), P(ctypes.c_float)]
+        L.oracle_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def make_cfg(n, origin, ending, mu_c, rho_c, rho_d, drag="sn_explicit", precision="mixed",
+             n_substeps=1, quant_limbs=1, drag_multiplier=1.0, diameter_scale=1.0):
+    c = OracleCfg()
+    n = [n] * 3 if np.isscalar(n) else list(n)
+    origin = [origin] * 3 if np.isscalar(origin) else list(origin)
+    ending = [ending] * 3 if np.isscalar(ending) else list(ending)
+    c.n = (ctypes.c_int32 * 3)(*n)
+    c.origin = (ctypes.c_double * 3)(*origin)
+    c.ending = (ctypes.c_double * 3)(*ending)
+    c.mu_c, c.rho_c, c.rho_d = mu_c, rho_c, rho_d
+    c.drag = DRAG[drag] if isinstance(drag, str) else int(drag)
+    c.precision = PREC[precision] if isinstance(precision, str) else int(precision)
+    c.n_substeps = n_substeps
+    c.quant_limbs = quant_limbs
+    c.drag_multiplier = drag_multiplier
+    c.diameter_scale = diameter_scale
+    return c
+
+
+def run(cfg, xyz, uvw, d, U, nsteps, dt, fscale=None, want_seq=True, want_quant=True,
+        scale=INT_MIN, nthreads=1):
+    """Runs nsteps steps.  xyz/uvw are [3, np] float64 (copied), d [np], U [ncells, 3].
+
+    Returns dict(xyz, uvw, cells, src_seq, src_quant, scale, lost, overflow, H, status)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+    uvw = np.ascontiguousarray(uvw, dtype=np.float64).copy()
+    d = np.ascontiguousarray(d, dtype=np.float64)
+    U = np.ascontiguousarray(U, dtype=np.float64).reshape(-1)
+    npcl = d.shape[0]
+    ncells = int(cfg.n[0]) * int(cfg.n[1]) * int(cfg.n[2])
+    assert U.shape[0] == 3 * ncells
+    fs = None if fscale is None else np.ascontiguousarray(fscale, dtype=np.float64)
+    src_seq = np.zeros(3 * ncells) if want_seq else None
+    src_q = np.zeros(3 * ncells) if want_quant else None
+    cells = np.zeros(npcl, dtype=np.int32)
+    sc = np.array([scale], dtype=np.int32)
+    stats = np.zeros(3, dtype=np.int64)
+    st = lib().oracle_run(ctypes.byref(cfg), npcl, _ptr(xyz, ctypes.c_double),
+                          _ptr(uvw, ctypes.c_double), _ptr(d, ctypes.c_double),
+                          _ptr(U, ctypes.c_double), nsteps, dt, _ptr(fs, ctypes.c_double),
+                          _ptr(src_seq, ctypes.c_double), _ptr(src_q, ctypes.c_double),
+                          _ptr(cells, ctypes.c_int32), _ptr(sc, ctypes.c_int32),
+                          _ptr(stats, ctypes.c_int64), nthreads)
+    return dict(xyz=xyz, uvw=uvw, cells=cells,
+                src_seq=None if src_seq is None else src_seq.reshape(ncells, 3),
+                src_quant=None if src_q is None else src_q.reshape(ncells, 3),
+                scale=int(sc[0]), lost=int(stats[0]), overflow=int(stats[1]), H=int(stats[2]),
+                status=st)
+
+
+def locate(cfg, xyz):
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    npcl = xyz.shape[1]
+    cells = np.zeros(npcl, dtype=np.int32)
+    lib().oracle_locate(ctypes.byref(cfg), npcl, _ptr(xyz, ctypes.c_double),
+                        _ptr(cells, ctypes.c_int32))
+    return cells
+
+
+def pow0687(x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    lib().oracle_pow0687(x.size, _ptr(x, ctypes.c_double), _ptr(y, ctypes.c_double))
+    return y
+
+
+def pow0687f(x):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.empty_like(x)
+    lib().oracle_pow0687f(x.size, _ptr(x, ctypes.c_float), _ptr(y, ctypes.c_float))
+    return y
+
+
+def num_threads():
+    return lib().oracle_num_threads()

@@ -1,0 +1,1058 @@
+/*
+ * st_abi.cu -- the C ABI of libscaletrack.so (declared in include/scaletrack.h).
+ *
+ * Host side of the parcel step: handle and device memory management, the per-step launch
+ * sequence (probe -> step -> finalize, periodic Morton re-sort), device error reporting and
+ * the two shims with the reference's coupling surface (allocate_array_ptr and
+ * evolve_cloud, A:1436-1528).  There is no CPU fallback: without a CUDA device every entry
+ * point that needs one fails with ST_ERR_CUDA.
+ *
+ * Per-step launch sequence on the handle's stream (all clouds in each launch):
+ *   [probe + set_scale]   only on the first step after st_set_parcels or a new dt
+ *   [zero source]         only in ST_DEPOSIT_ATOMIC mode
+ *   step                  k_step: the parcel step and the warp-aggregated deposit
+ *   finalize              fixed point -> FP64 source, clear accumulators, next scale
+ *   [sort]                every sort_interval steps
+ */
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <cstdint>
+#include <climits>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <map>
+
+#include <cuda_runtime.h>
+
+#include "scaletrack.h"
+#include "st_internal.h"
+
+using namespace st;
+
+/* ------------------------------------------------------------------------------------ */
+/* errors                                                                               */
+/* ------------------------------------------------------------------------------------ */
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(...)                                                                             \
+    do {                                                                                    \
+        cudaError_t e_ = (__VA_ARGS__);                                                     \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(ST_ERR_CUDA, "%s: %s (%s:%d)", #__VA_ARGS__, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                \
+    } while (0)
+
+/* ------------------------------------------------------------------------------------ */
+/* the handle                                                                           */
+/* ------------------------------------------------------------------------------------ */
+struct CloudBufs {
+    int64_t n = 0;
+    int64_t cap = 0;
+    void* x[2] = {nullptr, nullptr};
+    void* y[2] = {nullptr, nullptr};
+    void* z[2] = {nullptr, nullptr};
+    void* u[2] = {nullptr, nullptr};
+    void* v[2] = {nullptr, nullptr};
+    void* w[2] = {nullptr, nullptr};
+    void* d[2] = {nullptr, nullptr};
+    int32_t* id[2] = {nullptr, nullptr};
+    uint32_t* keys[2] = {nullptr, nullptr};
+    uint32_t* perm[2] = {nullptr, nullptr};
+    void* temp = nullptr;
+    size_t temp_bytes = 0;
+    int cur = 0;
+};
+
+struct ProfRec {
+    int kind;
+    cudaEvent_t a, b;
+};
+
+struct st_handle {
+    st_params p;
+    st_mesh_desc m;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int dep = DEP_DET1;
+    int limbs = 1;
+    int64_t ncells = 0;
+    size_t psz = 4, vsz = 4;
+    void* dU = nullptr;
+    double* dsrc = nullptr;
+    unsigned long long* dacc = nullptr;
+    CloudCtl* dctl = nullptr;
+    unsigned int* dcounter = nullptr;
+    unsigned long long* dcount = nullptr;  /* scratch counter (outside parcels) */
+    void* dclouds = nullptr;
+    std::vector<unsigned char> hclouds;      /* host image of the CloudK array */
+    std::vector<CloudBufs> clouds;
+    bool clouds_dirty = true;
+    bool need_probe = true;
+    double last_dt = 0.0;
+    int64_t steps = 0;
+    int steps_since_sort = 0;
+    int block = 256;
+    int grid = 0;
+    int key_bits = 32;
+    bool morton = true;
+    int64_t total_tiles = 0;
+    int64_t launches = 0;
+    bool prof = false;
+    std::vector<ProfRec> recs;
+    std::vector<cudaEvent_t> pool;
+    int64_t prof_launches[ST_KERNEL_KINDS] = {0, 0, 0, 0, 0};
+    double prof_ms[ST_KERNEL_KINDS] = {0, 0, 0, 0, 0};
+    void* dstage = nullptr;
+    size_t stage_bytes = 0;
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int now = -1;
+        if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+    }
+};
+
+template <class P>
+MeshK<P> mesh_k(const st_handle* h)
+{
+    MeshK<P> k;
+    for (int a = 0; a < 3; ++a) {
+        k.N[a] = h->m.n[a];
+        k.origin[a] = (P)h->m.origin[a];
+        double L = h->m.ending[a] - h->m.origin[a];
+        double D = L / (double)h->m.n[a];
+        k.rD[a] = (P)(1.0 / D);
+    }
+    k.NxNy = h->m.n[0] * h->m.n[1];
+    k.pad = 0;
+    k.nCells = h->ncells;
+    return k;
+}
+
+template <class V>
+PhysK<V> phys_k(const st_handle* h)
+{
+    PhysK<V> k;
+    k.mu = (V)h->p.mu_c;
+    k.rho_d = (V)h->p.rho_d;
+    k.rr = (V)(h->p.rho_d / h->p.rho_c);
+    k.nu = (V)(h->p.mu_c / h->p.rho_c);
+    k.alpha = (V)h->p.drag_multiplier;
+    k.dscale = (V)h->p.diameter_scale;
+    k.drag = h->p.drag_model;
+    k.nsub = h->p.n_substeps;
+    return k;
+}
+
+int quant_nbits(int64_t n_bound)
+{
+    int nb = 1;
+    while (nb < 62 && ((int64_t)1 << nb) < n_bound) ++nb;
+    return nb;
+}
+
+cudaEvent_t take_event(st_handle* h)
+{
+    if (!h->pool.empty()) {
+        cudaEvent_t e = h->pool.back();
+        h->pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+/* Brackets one kernel launch with events when profiling is on. */
+struct ProfScope {
+    st_handle* h;
+    int kind;
+    cudaEvent_t a = nullptr;
+    ProfScope(st_handle* hh, int k) : h(hh), kind(k)
+    {
+        if (h->prof) {
+            a = take_event(h);
+            cudaEventRecord(a, h->stream);
+        }
+    }
+    ~ProfScope()
+    {
+        if (h->prof && a) {
+            cudaEvent_t b = take_event(h);
+            cudaEventRecord(b, h->stream);
+            h->recs.push_back({kind, a, b});
+        }
+    }
+};
+
+int ensure_stage(st_handle* h, size_t bytes)
+{
+    if (h->stage_bytes >= bytes) return ST_OK;
+    if (h->dstage) cudaFree(h->dstage);
+    h->dstage = nullptr;
+    h->stage_bytes = 0;
+    CK(cudaMalloc(&h->dstage, bytes));
+    h->stage_bytes = bytes;
+    return ST_OK;
+}
+
+/* Reads the control blocks; reports (and clears) lost parcels and range errors. */
+int check_device_errors(st_handle* h)
+{
+    const int nc = h->p.n_clouds;
+    std::vector<CloudCtl> ctl(nc);
+    CK(cudaMemcpyAsync(ctl.data(), h->dctl, sizeof(CloudCtl) * nc, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    unsigned long long lost = 0, ovf = 0;
+    for (int c = 0; c < nc; ++c) {
+        lost += ctl[c].lost;
+        ovf += ctl[c].overflow;
+    }
+    if (lost || ovf) {
+        for (int c = 0; c < nc; ++c) ctl[c].lost = ctl[c].overflow = 0;
+        CK(cudaMemcpyAsync(h->dctl, ctl.data(), sizeof(CloudCtl) * nc, cudaMemcpyHostToDevice,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (lost)
+            return fail(ST_ERR_PARCEL_OUTSIDE,
+                        "%llu parcel(s) could not be located in the mesh and were left "
+                        "unchanged", lost);
+        return fail(ST_ERR_SOURCE_RANGE,
+                    "%llu deposit component(s) were non-finite or exceeded the fixed-point "
+                    "range of the deterministic source and were dropped", ovf);
+    }
+    return ST_OK;
+}
+
+template <class P, class V>
+SortBufs<P, V> sort_bufs(CloudBufs& c)
+{
+    SortBufs<P, V> b;
+    for (int k = 0; k < 2; ++k) {
+        b.x[k] = (P*)c.x[k];
+        b.y[k] = (P*)c.y[k];
+        b.z[k] = (P*)c.z[k];
+        b.u[k] = (V*)c.u[k];
+        b.v[k] = (V*)c.v[k];
+        b.w[k] = (V*)c.w[k];
+        b.d[k] = (V*)c.d[k];
+        b.id[k] = c.id[k];
+        b.keys[k] = c.keys[k];
+        b.perm[k] = c.perm[k];
+    }
+    b.temp = c.temp;
+    b.temp_bytes = c.temp_bytes;
+    return b;
+}
+
+template <class P, class V>
+int upload_clouds(st_handle* h)
+{
+    const int nc = h->p.n_clouds;
+    std::vector<CloudK<P, V>> v(nc);
+    int64_t tiles = 0;
+    for (int c = 0; c < nc; ++c) {
+        CloudBufs& b = h->clouds[c];
+        CloudK<P, V>& k = v[c];
+        k.x = (P*)b.x[b.cur];
+        k.y = (P*)b.y[b.cur];
+        k.z = (P*)b.z[b.cur];
+        k.u = (V*)b.u[b.cur];
+        k.v = (V*)b.v[b.cur];
+        k.w = (V*)b.w[b.cur];
+        k.d = (const V*)b.d[b.cur];
+        k.n = b.n;
+        k.tile0 = tiles;
+        k.acc = h->dacc + (int64_t)c * h->ncells * 3 * h->limbs;
+        k.src = h->dsrc + (int64_t)c * h->ncells * 3;
+        tiles += (b.n + 31) / 32;
+    }
+    h->total_tiles = tiles;
+    h->hclouds.resize(sizeof(CloudK<P, V>) * nc);
+    memcpy(h->hclouds.data(), v.data(), h->hclouds.size());
+    CK(cudaMemcpyAsync(h->dclouds, h->hclouds.data(), h->hclouds.size(), cudaMemcpyHostToDevice,
+                       h->stream));
+    h->clouds_dirty = false;
+    return ST_OK;
+}
+
+template <class P, class V>
+int do_sort_all(st_handle* h)
+{
+    const MeshK<P> mk = mesh_k<P>(h);
+    for (auto& c : h->clouds) {
+        if (c.n <= 1) continue;
+        SortBufs<P, V> b = sort_bufs<P, V>(c);
+        int nl = 0;
+        {
+            ProfScope ps(h, ST_KERNEL_SORT);
+            CK(sort_cloud<P, V>(b, c.cur, c.n, mk, h->key_bits, h->morton, h->stream, &nl));
+        }
+        h->launches += nl;
+        c.cur = 1 - c.cur;
+    }
+    h->clouds_dirty = true;
+    h->steps_since_sort = 0;
+    return ST_OK;
+}
+
+template <class P, class V>
+int do_step(st_handle* h, double dt, double fscale)
+{
+    int rc;
+    if (h->clouds_dirty && (rc = upload_clouds<P, V>(h)) != ST_OK) return rc;
+    StepArgs<P, V> a;
+    a.mesh = mesh_k<P>(h);
+    a.phys = phys_k<V>(h);
+    a.dtP = (P)dt / (P)h->p.n_substeps;
+    a.dtV = (V)a.dtP;
+    a.fscale = (V)fscale;
+    a.nclouds = h->p.n_clouds;
+    a.U = (const V*)h->dU;
+    a.clouds = (const CloudK<P, V>*)h->dclouds;
+    a.ctl = h->dctl;
+    a.total_tiles = h->total_tiles;
+    if (a.total_tiles == 0) return ST_OK;
+    int grid = h->grid;
+    const int64_t warps_per_block = h->block / 32;
+    const int64_t need = (a.total_tiles + warps_per_block - 1) / warps_per_block;
+    if (grid > need) grid = (int)need;
+    if (grid < 1) grid = 1;
+
+    const bool det = (h->dep == DEP_DET1 || h->dep == DEP_DET2);
+    if (det && (h->need_probe || dt != h->last_dt)) {
+        {
+            ProfScope ps(h, ST_KERNEL_PROBE);
+            CK(launch_step<P, V>(a, DEP_PROBE, grid, h->block, h->stream));
+        }
+        {
+            ProfScope ps(h, ST_KERNEL_OTHER);
+            CK(launch_set_scale(h->dctl, h->p.n_clouds, h->stream));
+        }
+        h->launches += 2;
+        h->need_probe = false;
+    }
+    h->last_dt = dt;
+    if (!det) {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        CK(launch_zero_f64(h->dsrc, (int64_t)h->p.n_clouds * h->ncells * 3, h->stream));
+        h->launches += 1;
+    }
+    {
+        ProfScope ps(h, ST_KERNEL_STEP);
+        CK(launch_step<P, V>(a, h->dep, grid, h->block, h->stream));
+        h->launches += 1;
+    }
+    if (det) {
+        const int64_t ncomp = h->ncells * 3;
+        int64_t gx = (ncomp + 256 * 4 - 1) / (256 * 4);
+        int64_t cap = (148 * 8 + h->p.n_clouds - 1) / h->p.n_clouds;
+        if (gx > cap) gx = cap;
+        if (gx < 1) gx = 1;
+        ProfScope ps(h, ST_KERNEL_FINALIZE);
+        CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter, h->p.n_clouds, ncomp,
+                           (int)gx, h->stream));
+        h->launches += 1;
+    }
+    h->steps += 1;
+    h->steps_since_sort += 1;
+    if (h->p.sort_interval > 0 && h->steps_since_sort >= h->p.sort_interval)
+        return do_sort_all<P, V>(h);
+    return ST_OK;
+}
+
+template <class P, class V>
+int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
+                   const double* d)
+{
+    CloudBufs& c = h->clouds[cloud];
+    if (n > c.cap) {
+        for (int k = 0; k < 2; ++k) {
+            void** arrs[] = {&c.x[k], &c.y[k], &c.z[k], &c.u[k], &c.v[k], &c.w[k], &c.d[k]};
+            for (int a = 0; a < 7; ++a) {
+                if (*arrs[a]) cudaFree(*arrs[a]);
+                *arrs[a] = nullptr;
+                CK(cudaMalloc(arrs[a], (size_t)n * (a < 3 ? sizeof(P) : sizeof(V))));
+            }
+            if (c.id[k]) cudaFree(c.id[k]);
+            if (c.keys[k]) cudaFree(c.keys[k]);
+            if (c.perm[k]) cudaFree(c.perm[k]);
+            c.id[k] = nullptr;
+            c.keys[k] = c.perm[k] = nullptr;
+            CK(cudaMalloc(&c.id[k], (size_t)n * sizeof(int32_t)));
+            CK(cudaMalloc(&c.keys[k], (size_t)n * sizeof(uint32_t)));
+            CK(cudaMalloc(&c.perm[k], (size_t)n * sizeof(uint32_t)));
+        }
+        if (c.temp) cudaFree(c.temp);
+        c.temp = nullptr;
+        c.temp_bytes = sort_temp_bytes<P, V>(n);
+        CK(cudaMalloc(&c.temp, c.temp_bytes > 0 ? c.temp_bytes : 16));
+        c.cap = n;
+    }
+    c.n = n;
+    c.cur = 0;
+    if (n > 0) {
+        std::vector<P> hp(n);
+        std::vector<V> hv(n);
+        std::vector<int32_t> hid(n);
+        for (int a = 0; a < 3; ++a) {
+            for (int64_t i = 0; i < n; ++i) hp[i] = (P)xyz[a * n + i];
+            void* dst = a == 0 ? c.x[0] : (a == 1 ? c.y[0] : c.z[0]);
+            CK(cudaMemcpy(dst, hp.data(), n * sizeof(P), cudaMemcpyHostToDevice));
+        }
+        for (int a = 0; a < 4; ++a) {
+            const double* srcp = a < 3 ? uvw + a * n : d;
+            for (int64_t i = 0; i < n; ++i) hv[i] = (V)srcp[i];
+            void* dst = a == 0 ? c.u[0] : (a == 1 ? c.v[0] : (a == 2 ? c.w[0] : c.d[0]));
+            CK(cudaMemcpy(dst, hv.data(), n * sizeof(V), cudaMemcpyHostToDevice));
+        }
+        for (int64_t i = 0; i < n; ++i) hid[i] = (int32_t)i;
+        CK(cudaMemcpy(c.id[0], hid.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        /* every parcel must start inside the mesh: the reference would index out of bounds */
+        CK(cudaMemsetAsync(h->dcount, 0, sizeof(unsigned long long), h->stream));
+        {
+            ProfScope ps(h, ST_KERNEL_OTHER);
+            CK(cells_cloud<P>((const P*)c.x[0], (const P*)c.y[0], (const P*)c.z[0], nullptr, n,
+                              mesh_k<P>(h), (int32_t*)c.keys[0], h->dcount, h->stream));
+            h->launches += 1;
+        }
+        unsigned long long outside = 0;
+        CK(cudaMemcpyAsync(&outside, h->dcount, sizeof outside, cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (outside) {
+            c.n = 0;
+            h->clouds_dirty = true;
+            return fail(ST_ERR_PARCEL_OUTSIDE,
+                        "%llu of %lld parcels of cloud %d lie outside the mesh", outside,
+                        (long long)n, cloud);
+        }
+    }
+    h->clouds_dirty = true;
+    h->need_probe = true;
+    if (h->p.sort_interval > 0 && n > 1) {
+        CloudBufs& cc = h->clouds[cloud];
+        SortBufs<P, V> b = sort_bufs<P, V>(cc);
+        int nl = 0;
+        ProfScope ps(h, ST_KERNEL_SORT);
+        CK(sort_cloud<P, V>(b, cc.cur, cc.n, mesh_k<P>(h), h->key_bits, h->morton, h->stream,
+                            &nl));
+        h->launches += nl;
+        cc.cur = 1 - cc.cur;
+    }
+    return ST_OK;
+}
+
+template <class P, class V>
+int do_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d)
+{
+    CloudBufs& c = h->clouds[cloud];
+    const int64_t n = c.n;
+    if (n == 0) return ST_OK;
+    SortBufs<P, V> b = sort_bufs<P, V>(c);
+    {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        CK(unpermute_cloud<P, V>(b, c.cur, n, h->stream));
+        h->launches += 1;
+    }
+    const int o = 1 - c.cur;
+    std::vector<P> hp(n);
+    std::vector<V> hv(n);
+    void* ps_[3] = {c.x[o], c.y[o], c.z[o]};
+    for (int a = 0; a < 3; ++a) {
+        CK(cudaMemcpyAsync(hp.data(), ps_[a], n * sizeof(P), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (xyz)
+            for (int64_t i = 0; i < n; ++i) xyz[a * n + i] = (double)hp[i];
+    }
+    void* vs_[4] = {c.u[o], c.v[o], c.w[o], c.d[o]};
+    for (int a = 0; a < 4; ++a) {
+        double* dst = a < 3 ? (uvw ? uvw + a * n : nullptr) : d;
+        if (!dst) continue;
+        CK(cudaMemcpyAsync(hv.data(), vs_[a], n * sizeof(V), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (int64_t i = 0; i < n; ++i) dst[i] = (double)hv[i];
+    }
+    return ST_OK;
+}
+
+template <class P>
+int do_get_cells(st_handle* h, int cloud, int32_t* cells)
+{
+    CloudBufs& c = h->clouds[cloud];
+    const int64_t n = c.n;
+    if (n == 0) return ST_OK;
+    /* the sort key buffer is free between steps */
+    {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        CK(cells_cloud<P>((const P*)c.x[c.cur], (const P*)c.y[c.cur], (const P*)c.z[c.cur],
+                          c.id[c.cur], n, mesh_k<P>(h), (int32_t*)c.keys[0], nullptr, h->stream));
+        h->launches += 1;
+    }
+    CK(cudaMemcpyAsync(cells, c.keys[0], n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ST_OK;
+}
+
+int check_handle(st_handle* h)
+{
+    if (!h) return fail(ST_ERR_INVALID_ARGUMENT, "null handle");
+    return ST_OK;
+}
+
+int check_cloud(st_handle* h, int cloud)
+{
+    if (cloud < 0 || cloud >= h->p.n_clouds)
+        return fail(ST_ERR_INVALID_ARGUMENT, "cloud %d out of range [0, %d)", cloud,
+                    h->p.n_clouds);
+    return ST_OK;
+}
+
+#define DISPATCH(h, FN, ...)                                                                 \
+    ((h)->p.precision == ST_PREC_FP32                                                        \
+         ? FN<float, float>(__VA_ARGS__)                                                     \
+         : ((h)->p.precision == ST_PREC_MIXED ? FN<double, float>(__VA_ARGS__)               \
+                                              : FN<double, double>(__VA_ARGS__)))
+
+void free_cloud(CloudBufs& c)
+{
+    for (int k = 0; k < 2; ++k) {
+        void* arrs[] = {c.x[k], c.y[k], c.z[k], c.u[k], c.v[k], c.w[k], c.d[k],
+                        c.id[k], c.keys[k], c.perm[k]};
+        for (void* p : arrs)
+            if (p) cudaFree(p);
+    }
+    if (c.temp) cudaFree(c.temp);
+    c = CloudBufs();
+}
+
+}  // namespace
+
+/* ------------------------------------------------------------------------------------ */
+/* public API                                                                           */
+/* ------------------------------------------------------------------------------------ */
+extern "C" {
+
+const char* st_version(void) { return "scaletrack-b200 0.1 sm_100a"; }
+
+const char* st_last_error(void) { return g_err.c_str(); }
+
+void st_params_default(st_params* p)
+{
+    if (!p) return;
+    memset(p, 0, sizeof *p);
+    p->mu_c = 1e-3;    /* setup.jl:12 */
+    p->rho_c = 1e3;    /* setup.jl:13 */
+    p->rho_d = 1.0;    /* setup.jl:14 */
+    p->drag_model = ST_DRAG_STOKES_IMPLICIT;
+    p->precision = ST_PREC_FP32;
+    p->deposit = ST_DEPOSIT_DETERMINISTIC;
+    p->n_substeps = 10;  /* A:1260 */
+    p->sort_interval = 0;
+    p->n_clouds = 1;
+    p->block_size = 0;
+    p->grid_blocks = 0;
+    p->drag_multiplier = 1.0;
+    p->diameter_scale = 1.0;
+}
+
+int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle** out)
+{
+    if (!p || !m || !out) return fail(ST_ERR_INVALID_ARGUMENT, "null argument to st_create");
+    *out = nullptr;
+    for (int a = 0; a < 3; ++a) {
+        if (m->n[a] < 1) return fail(ST_ERR_INVALID_ARGUMENT, "mesh n[%d] = %d < 1", a, m->n[a]);
+        if (!(m->ending[a] > m->origin[a]))
+            return fail(ST_ERR_INVALID_ARGUMENT, "mesh ending[%d] must exceed origin[%d]", a, a);
+    }
+    const int64_t ncells = (int64_t)m->n[0] * m->n[1] * m->n[2];
+    if (ncells > INT32_MAX)
+        return fail(ST_ERR_INVALID_ARGUMENT, "mesh has %lld cells; at most 2^31-1 supported",
+                    (long long)ncells);
+    if (p->precision < ST_PREC_FP32 || p->precision > ST_PREC_FP64)
+        return fail(ST_ERR_INVALID_ARGUMENT, "unknown precision %d", p->precision);
+    if (p->drag_model != ST_DRAG_STOKES_IMPLICIT && p->drag_model != ST_DRAG_SCHILLER_NAUMANN)
+        return fail(ST_ERR_INVALID_ARGUMENT, "unknown drag model %d", p->drag_model);
+    if (p->deposit != ST_DEPOSIT_DETERMINISTIC && p->deposit != ST_DEPOSIT_ATOMIC)
+        return fail(ST_ERR_INVALID_ARGUMENT, "unknown deposit mode %d", p->deposit);
+    if (p->n_substeps < 1) return fail(ST_ERR_INVALID_ARGUMENT, "n_substeps must be >= 1");
+    if (p->n_clouds < 1 || p->n_clouds > 4096)
+        return fail(ST_ERR_INVALID_ARGUMENT, "n_clouds must be in [1, 4096]");
+    if (p->sort_interval < 0) return fail(ST_ERR_INVALID_ARGUMENT, "sort_interval must be >= 0");
+    if (!(p->mu_c > 0) || !(p->rho_c > 0) || !(p->rho_d > 0))
+        return fail(ST_ERR_INVALID_ARGUMENT, "mu_c, rho_c and rho_d must be positive");
+    if (p->block_size != 0 && (p->block_size % 32 || p->block_size < 32 || p->block_size > 256))
+        return fail(ST_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 in [32, 256]");
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(ST_ERR_CUDA, "no CUDA device available (the library has no CPU path)");
+    if (device < 0 || device >= ndev)
+        return fail(ST_ERR_INVALID_ARGUMENT, "device %d out of range [0, %d)", device, ndev);
+    DeviceGuard g(device);
+
+    st_handle* h = new st_handle();
+    h->p = *p;
+    h->m = *m;
+    h->device = device;
+    h->ncells = ncells;
+    h->psz = p->precision == ST_PREC_FP32 ? 4 : 8;
+    h->vsz = p->precision == ST_PREC_FP64 ? 8 : 4;
+    if (p->deposit == ST_DEPOSIT_ATOMIC) {
+        h->dep = DEP_ATOMIC;
+        h->limbs = 1;
+    } else if (p->precision == ST_PREC_FP64) {
+        h->dep = DEP_DET2;
+        h->limbs = 2;
+    } else {
+        h->dep = DEP_DET1;
+        h->limbs = 1;
+    }
+    h->morton = m->n[0] <= 1024 && m->n[1] <= 1024 && m->n[2] <= 1024;
+    if (h->morton) {
+        int b = 1;
+        int nmax = std::max(m->n[0], std::max(m->n[1], m->n[2]));
+        while ((1 << b) < nmax) ++b;
+        h->key_bits = 3 * b;
+    } else {
+        h->key_bits = quant_nbits(ncells);
+    }
+    h->block = p->block_size ? p->block_size : 256;
+    h->clouds.resize(p->n_clouds);
+
+    auto bail = [&](int code) {
+        st_destroy(h);
+        return code;
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(fail(ST_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)));
+    h->own_stream = true;
+    const size_t ncomp = (size_t)ncells * 3;
+    if ((e = cudaMalloc(&h->dU, ncomp * h->vsz)) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->dsrc, ncomp * p->n_clouds * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->dacc, ncomp * p->n_clouds * h->limbs * 8)) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->dctl, sizeof(CloudCtl) * p->n_clouds)) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->dcounter, sizeof(unsigned int))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->dcount, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMalloc(&h->dclouds, 256 * (size_t)p->n_clouds)) != cudaSuccess)
+        return bail(fail(e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA,
+                         "device allocation: %s", cudaGetErrorString(e)));
+    cudaMemsetAsync(h->dU, 0, ncomp * h->vsz, h->stream);
+    cudaMemsetAsync(h->dsrc, 0, ncomp * p->n_clouds * sizeof(double), h->stream);
+    cudaMemsetAsync(h->dacc, 0, ncomp * p->n_clouds * h->limbs * 8, h->stream);
+    cudaMemsetAsync(h->dcounter, 0, sizeof(unsigned int), h->stream);
+    {
+        std::vector<CloudCtl> ctl(p->n_clouds);
+        /* bound on the deposits one cloud makes per step: one per parcel and substep */
+        for (auto& c : ctl) {
+            c.L = 0;
+            c.emax = EXP_NONE;
+            c.H = 0;
+            c.pad = 0;
+            c.lost = 0;
+            c.overflow = 0;
+        }
+        if ((e = cudaMemcpy(h->dctl, ctl.data(), sizeof(CloudCtl) * p->n_clouds,
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(fail(ST_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e)));
+    }
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    int occ = DISPATCH(h, step_max_active_blocks, h->dep, h->block);
+    if (occ < 1) occ = 1;
+    h->grid = p->grid_blocks > 0 ? p->grid_blocks : nsm * occ;
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
+        return bail(fail(ST_ERR_CUDA, "set-up: %s", cudaGetErrorString(e)));
+    *out = h;
+    return ST_OK;
+}
+
+int st_destroy(st_handle* h)
+{
+    if (!h) return ST_OK;
+    DeviceGuard g(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& c : h->clouds) free_cloud(c);
+    void* arrs[] = {h->dU, h->dsrc, h->dacc, h->dctl, h->dcounter, h->dcount, h->dclouds,
+                    h->dstage};
+    for (void* p : arrs)
+        if (p) cudaFree(p);
+    for (auto& r : h->recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : h->pool) cudaEventDestroy(e);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return ST_OK;
+}
+
+int64_t st_num_parcels(st_handle* h, int cloud)
+{
+    if (!h || cloud < 0 || cloud >= h->p.n_clouds) return -1;
+    return h->clouds[cloud].n;
+}
+
+int64_t st_num_cells(st_handle* h) { return h ? h->ncells : -1; }
+
+/* Headroom of the fixed-point deposit: H + G bits for the largest deposit of the previous
+ * step, so that the sum of all deposits of one step fits in 63 bits. */
+static int update_headroom(st_handle* h)
+{
+    std::vector<CloudCtl> ctl(h->p.n_clouds);
+    CK(cudaMemcpyAsync(ctl.data(), h->dctl, sizeof(CloudCtl) * ctl.size(), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < h->p.n_clouds; ++c) {
+        int64_t bound = h->clouds[c].n * (int64_t)h->p.n_substeps;
+        if (bound < 2) bound = 2;
+        ctl[c].H = h->limbs == 1 ? 62 - QUANT_GROWTH_BITS - quant_nbits(bound)
+                                 : 62 - QUANT_GROWTH_BITS;
+    }
+    CK(cudaMemcpyAsync(h->dctl, ctl.data(), sizeof(CloudCtl) * ctl.size(), cudaMemcpyHostToDevice,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ST_OK;
+}
+
+int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
+                   const double* d)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    if (n < 0 || n > INT32_MAX)
+        return fail(ST_ERR_INVALID_ARGUMENT, "parcel count %lld out of range", (long long)n);
+    if (n > 0 && (!xyz || !uvw || !d))
+        return fail(ST_ERR_INVALID_ARGUMENT, "null parcel array");
+    DeviceGuard g(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    rc = DISPATCH(h, do_set_parcels, h, cloud, n, xyz, uvw, d);
+    if (rc) return rc;
+    return update_headroom(h);
+}
+
+int st_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    DeviceGuard g(h->device);
+    if ((rc = check_device_errors(h))) {
+        /* still hand back the state: lost parcels were left unchanged */
+        int rc2 = DISPATCH(h, do_get_parcels, h, cloud, xyz, uvw, d);
+        return rc2 ? rc2 : rc;
+    }
+    return DISPATCH(h, do_get_parcels, h, cloud, xyz, uvw, d);
+}
+
+int st_get_cells(st_handle* h, int cloud, int32_t* cells)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    if (!cells && h->clouds[cloud].n > 0) return fail(ST_ERR_INVALID_ARGUMENT, "null cells");
+    DeviceGuard g(h->device);
+    int err = check_device_errors(h);
+    rc = h->p.precision == ST_PREC_FP32 ? do_get_cells<float>(h, cloud, cells)
+                                        : do_get_cells<double>(h, cloud, cells);
+    return rc ? rc : err;
+}
+
+static int set_fluid(st_handle* h, const void* U, int elem_bytes, bool device)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (!U) return fail(ST_ERR_INVALID_ARGUMENT, "null U");
+    if (elem_bytes != 4 && elem_bytes != 8)
+        return fail(ST_ERR_INVALID_ARGUMENT, "elem_bytes must be 4 or 8, got %d", elem_bytes);
+    DeviceGuard g(h->device);
+    const int64_t ncomp = h->ncells * 3;
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if ((size_t)elem_bytes == h->vsz) {
+        CK(cudaMemcpyAsync(h->dU, U, ncomp * elem_bytes, kind, h->stream));
+    } else {
+        if ((rc = ensure_stage(h, ncomp * elem_bytes))) return rc;
+        CK(cudaMemcpyAsync(h->dstage, U, ncomp * elem_bytes, kind, h->stream));
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        if (elem_bytes == 8) CK(launch_f64_to_f32((const double*)h->dstage, (float*)h->dU, ncomp, h->stream));
+        else CK(launch_f32_to_f64((const float*)h->dstage, (double*)h->dU, ncomp, h->stream));
+        h->launches += 1;
+    }
+    if (!device) CK(cudaStreamSynchronize(h->stream));
+    return ST_OK;
+}
+
+int st_set_fluid_velocity(st_handle* h, const void* U, int elem_bytes)
+{
+    return set_fluid(h, U, elem_bytes, false);
+}
+
+int st_set_fluid_velocity_device(st_handle* h, const void* U, int elem_bytes)
+{
+    return set_fluid(h, U, elem_bytes, true);
+}
+
+int st_step(st_handle* h, double dt, double fluid_scale)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (!(dt > 0) || !(dt < 1e300))
+        return fail(ST_ERR_INVALID_ARGUMENT, "dt must be positive and finite, got %g", dt);
+    if (!(fluid_scale == fluid_scale) || fluid_scale > 1e300 || fluid_scale < -1e300)
+        return fail(ST_ERR_INVALID_ARGUMENT, "fluid_scale must be finite");
+    DeviceGuard g(h->device);
+    return DISPATCH(h, do_step, h, dt, fluid_scale);
+}
+
+static int copy_source(st_handle* h, int cloud, void* S, int elem_bytes, bool sync)
+{
+    const int64_t ncomp = h->ncells * 3;
+    const double* src = h->dsrc + (int64_t)cloud * ncomp;
+    int rc;
+    if (elem_bytes == 8) {
+        CK(cudaMemcpyAsync(S, src, ncomp * 8, cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        if ((rc = ensure_stage(h, ncomp * 4))) return rc;
+        {
+            ProfScope ps(h, ST_KERNEL_OTHER);
+            CK(launch_f64_to_f32(src, (float*)h->dstage, ncomp, h->stream));
+            h->launches += 1;
+        }
+        CK(cudaMemcpyAsync(S, h->dstage, ncomp * 4, cudaMemcpyDeviceToHost, h->stream));
+    }
+    if (sync) CK(cudaStreamSynchronize(h->stream));
+    return ST_OK;
+}
+
+int st_get_source(st_handle* h, int cloud, void* S, int elem_bytes)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    if (!S) return fail(ST_ERR_INVALID_ARGUMENT, "null S");
+    if (elem_bytes != 4 && elem_bytes != 8)
+        return fail(ST_ERR_INVALID_ARGUMENT, "elem_bytes must be 4 or 8, got %d", elem_bytes);
+    DeviceGuard g(h->device);
+    if ((rc = copy_source(h, cloud, S, elem_bytes, true))) return rc;
+    return check_device_errors(h);
+}
+
+const double* st_source_device(st_handle* h, int cloud)
+{
+    if (!h || cloud < 0 || cloud >= h->p.n_clouds) return nullptr;
+    return h->dsrc + (int64_t)cloud * h->ncells * 3;
+}
+
+int st_synchronize(st_handle* h)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    DeviceGuard g(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    return check_device_errors(h);
+}
+
+void* st_get_stream(st_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int st_set_stream(st_handle* h, void* stream)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    DeviceGuard g(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->stream = (cudaStream_t)stream;
+    h->own_stream = false;
+    return ST_OK;
+}
+
+int st_profile_enable(st_handle* h, int on)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    h->prof = on != 0;
+    return ST_OK;
+}
+
+int st_profile_read(st_handle* h, int kind, int64_t* launches, double* ms, int reset)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (kind < 0 || kind >= ST_KERNEL_KINDS)
+        return fail(ST_ERR_INVALID_ARGUMENT, "unknown kernel kind %d", kind);
+    DeviceGuard g(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    for (auto& r : h->recs) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, r.a, r.b));
+        h->prof_ms[r.kind] += t;
+        h->prof_launches[r.kind] += 1;
+        h->pool.push_back(r.a);
+        h->pool.push_back(r.b);
+    }
+    h->recs.clear();
+    if (launches) *launches = h->prof_launches[kind];
+    if (ms) *ms = h->prof_ms[kind];
+    if (reset) {
+        for (int k = 0; k < ST_KERNEL_KINDS; ++k) {
+            h->prof_ms[k] = 0;
+            h->prof_launches[k] = 0;
+        }
+    }
+    return ST_OK;
+}
+
+int64_t st_launch_count(st_handle* h) { return h ? h->launches : -1; }
+
+/* ------------------------------------------------------------------------------------ */
+/* reference-compatible shims                                                           */
+/* ------------------------------------------------------------------------------------ */
+struct Adopted {
+    void* ptr = nullptr;
+    int size = 0;
+    int ncomp = 0;
+    int tbytes = 0;
+};
+static std::mutex g_mu;
+static st_handle* g_default = nullptr;
+static std::map<std::string, Adopted> g_arrays;
+
+int st_setup(const st_params* p, const st_mesh_desc* m)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+    st_handle* h = nullptr;
+    int rc = st_create(p, m, dev, &h);
+    if (rc) return rc;
+    if (g_default) st_destroy(g_default);
+    g_default = h;
+    return ST_OK;
+}
+
+st_handle* st_default_handle(void)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_default;
+}
+
+void* st_allocate_array(const char* name, int size, int nComponents, int typeByteSize)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_default) {
+        fail(ST_ERR_NOT_INITIALISED, "st_allocate_array called before st_setup");
+        return nullptr;
+    }
+    if (!name || (strcmp(name, "U") != 0 && strcmp(name, "UTrans") != 0)) {
+        fail(ST_ERR_INVALID_ARGUMENT, "unknown field name '%s' (expected U or UTrans)",
+             name ? name : "(null)");
+        return nullptr;
+    }
+    if (typeByteSize != 4 && typeByteSize != 8) {  /* A:1444-1452 */
+        fail(ST_ERR_INVALID_ARGUMENT,
+             "size of the library's component type (4 or 8 bytes) is different from the "
+             "extern type: %d", typeByteSize);
+        return nullptr;
+    }
+    if ((int64_t)size != g_default->ncells) {      /* A:1454-1465 */
+        fail(ST_ERR_INVALID_ARGUMENT, "size of the mesh: %lld is different from field's %s size: %d",
+             (long long)g_default->ncells, name, size);
+        return nullptr;
+    }
+    if (nComponents != 3) {
+        fail(ST_ERR_INVALID_ARGUMENT, "field %s must have 3 components, got %d", name,
+             nComponents);
+        return nullptr;
+    }
+    auto it = g_arrays.find(name);
+    if (it != g_arrays.end()) {
+        Adopted& a = it->second;
+        if (a.size == size && a.ncomp == nComponents && a.tbytes == typeByteSize) return a.ptr;
+        fail(ST_ERR_INVALID_ARGUMENT, "field %s already allocated with a different layout", name);
+        return nullptr;
+    }
+    Adopted a;
+    DeviceGuard g(g_default->device);
+    cudaError_t e = cudaHostAlloc(&a.ptr, (size_t)size * nComponents * typeByteSize,
+                                  cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        fail(ST_ERR_CUDA, "cudaHostAlloc: %s", cudaGetErrorString(e));
+        return nullptr;
+    }
+    memset(a.ptr, 0, (size_t)size * nComponents * typeByteSize);
+    a.size = size;
+    a.ncomp = nComponents;
+    a.tbytes = typeByteSize;
+    g_arrays[name] = a;
+    return a.ptr;
+}
+
+int st_evolve_cloud(double dt)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    st_handle* h = g_default;
+    if (!h) return fail(ST_ERR_NOT_INITIALISED, "st_evolve_cloud called before st_setup");
+    auto iu = g_arrays.find("U");
+    auto is = g_arrays.find("UTrans");
+    if (iu == g_arrays.end() || is == g_arrays.end())
+        return fail(ST_ERR_NOT_INITIALISED, "U and UTrans must be allocated with "
+                                            "st_allocate_array before st_evolve_cloud");
+    DeviceGuard g(h->device);
+    const int64_t ncomp = h->ncells * 3;
+    int rc;
+    /* U host -> device (A:1079-1083) */
+    if ((size_t)iu->second.tbytes == h->vsz) {
+        CK(cudaMemcpyAsync(h->dU, iu->second.ptr, ncomp * h->vsz, cudaMemcpyHostToDevice,
+                           h->stream));
+    } else {
+        if ((rc = ensure_stage(h, ncomp * 8))) return rc;
+        CK(cudaMemcpyAsync(h->dstage, iu->second.ptr, ncomp * iu->second.tbytes,
+                           cudaMemcpyHostToDevice, h->stream));
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        if (iu->second.tbytes == 8)
+            CK(launch_f64_to_f32((const double*)h->dstage, (float*)h->dU, ncomp, h->stream));
+        else
+            CK(launch_f32_to_f64((const float*)h->dstage, (double*)h->dU, ncomp, h->stream));
+        h->launches += 1;
+    }
+    if ((rc = DISPATCH(h, do_step, h, dt, 1.0))) return rc;
+    /* source device -> host (A:1148-1152) */
+    if ((rc = copy_source(h, 0, is->second.ptr, is->second.tbytes, true))) return rc;
+    return check_device_errors(h);
+}
+
+int st_finalize(void)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_default) st_destroy(g_default);
+    g_default = nullptr;
+    for (auto& kv : g_arrays)
+        if (kv.second.ptr) cudaFreeHost(kv.second.ptr);
+    g_arrays.clear();
+    return ST_OK;
+}
+
+}  // extern "C"

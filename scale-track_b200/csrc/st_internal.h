@@ -1,0 +1,131 @@
+/*
+ * st_internal.h -- data layout shared by the host side (st_abi.cu) and the kernels.
+ *
+ * HBM layout (one handle):
+ *   parcels, per cloud, structure of arrays, two copies (A and B) so that the Morton
+ *   re-sort can gather out of place:  x,y,z : P[n]   u,v,w,d : V[n]   id : int32[n]
+ *   cell velocity U        : V[nCells][3]            (the exchange layout, A:204)
+ *   source                 : double[nClouds][nCells][3]
+ *   fixed-point accumulator: uint64[nClouds][nCells][3][limbs]   (deterministic deposit)
+ *   control blocks         : CloudCtl[nClouds]
+ * P is the position type and V the velocity/drag type of the precision mode.
+ */
+#ifndef ST_INTERNAL_H
+#define ST_INTERNAL_H
+
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+namespace st {
+
+constexpr int EXP_NONE = -100000;      /* "no deposit seen" for the max-exponent tracker */
+constexpr int QUANT_GROWTH_BITS = 8;   /* deposits may grow 2^8 x between steps          */
+
+enum DepMode { DEP_DET1 = 0, DEP_DET2 = 1, DEP_ATOMIC = 2, DEP_PROBE = 3 };
+
+template <class P>
+struct MeshK {
+    int32_t N[3];
+    P origin[3];
+    P rD[3];        /* 1/Δ per axis, formed in FP64 and rounded to P (A:237-240) */
+    int32_t NxNy;
+    int32_t pad;
+    int64_t nCells;
+};
+
+template <class V>
+struct PhysK {
+    V mu;       /* carrier dynamic viscosity */
+    V rho_d;    /* parcel density */
+    V rr;       /* rho_d / rho_c */
+    V nu;       /* carrier kinematic viscosity */
+    V alpha;    /* drag multiplier */
+    V dscale;   /* diameter scale */
+    int32_t drag;
+    int32_t nsub;
+};
+
+/* Device-resident per-cloud control block. */
+struct CloudCtl {
+    int32_t L;                   /* fixed-point scale exponent of the current step        */
+    int32_t emax;                /* max frexp exponent of this step's deposits            */
+    int32_t H;                   /* headroom bits: first step maps 2^emax to 2^H          */
+    int32_t pad;
+    unsigned long long lost;     /* parcels that could not be located (sticky)            */
+    unsigned long long overflow; /* deposits beyond the fixed-point range (sticky)        */
+};
+
+template <class P, class V>
+struct CloudK {
+    P* x;
+    P* y;
+    P* z;
+    V* u;
+    V* v;
+    V* w;
+    const V* d;
+    int64_t n;
+    int64_t tile0;              /* first warp tile of this cloud in the launch */
+    unsigned long long* acc;    /* [nCells*3*limbs] */
+    double* src;                /* [nCells*3] */
+};
+
+template <class P, class V>
+struct StepArgs {
+    MeshK<P> mesh;
+    PhysK<V> phys;
+    P dtP;                      /* substep for positions  */
+    V dtV;                      /* substep for drag       */
+    V fscale;                   /* factor on U            */
+    int32_t nclouds;
+    const V* U;                 /* [nCells*3] */
+    const CloudK<P, V>* clouds; /* [nclouds] device array */
+    CloudCtl* ctl;              /* [nclouds] */
+    int64_t total_tiles;        /* warp tiles (32 parcels) over all clouds */
+};
+
+/* Launchers implemented in st_kernels.cu (all asynchronous on `s`). */
+template <class P, class V>
+cudaError_t launch_step(const StepArgs<P, V>& a, int dep, int grid, int block, cudaStream_t s);
+template <class P, class V>
+int step_max_active_blocks(int dep, int block);
+
+cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, CloudCtl* ctl,
+                            unsigned int* counter, int nclouds, int64_t ncomp, int grid_x,
+                            cudaStream_t s);
+cudaError_t launch_set_scale(CloudCtl* ctl, int nclouds, cudaStream_t s);
+cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s);
+cudaError_t launch_f64_to_f32(const double* in, float* out, int64_t n, cudaStream_t s);
+cudaError_t launch_f32_to_f64(const float* in, double* out, int64_t n, cudaStream_t s);
+
+/* Morton re-sort and order restoration (st_sort.cu). */
+template <class P, class V>
+struct SortBufs {
+    P* x[2];
+    P* y[2];
+    P* z[2];
+    V* u[2];
+    V* v[2];
+    V* w[2];
+    V* d[2];
+    int32_t* id[2];
+    uint32_t* keys[2];
+    uint32_t* perm[2];
+    void* temp;
+    size_t temp_bytes;
+};
+template <class P, class V>
+size_t sort_temp_bytes(int64_t n);
+template <class P, class V>
+cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& mesh, int key_bits,
+                       bool morton, cudaStream_t s, int* launches);
+template <class P, class V>
+cudaError_t unpermute_cloud(SortBufs<P, V>& b, int cur, int64_t n, cudaStream_t s);
+template <class P>
+cudaError_t cells_cloud(const P* x, const P* y, const P* z, const int32_t* id, int64_t n,
+                        const MeshK<P>& mesh, int32_t* cells_out, unsigned long long* outside,
+                        cudaStream_t s);
+
+}  // namespace st
+
+#endif

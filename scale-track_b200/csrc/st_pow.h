@@ -1,0 +1,142 @@
+/*
+ * st_pow.h -- x^0.687 for the Schiller-Naumann drag correction, written for this project.
+ *
+ * The drag correction 1 + 0.15 Re^0.687 decides how far a parcel moves, and therefore
+ * which cell it ends up in.  Cell indices must agree bit for bit between the CUDA kernels
+ * and the CPU oracle, so the power function cannot come from two different math libraries
+ * (CUDA's pow and glibc's pow differ in the last ulp for some arguments).  This header is
+ * compiled unchanged by nvcc (device) and gcc (host) and uses only IEEE-754 +, -, *, /
+ * (correctly rounded on both), integer bit manipulation and comparisons.  Both sides must be
+ * built without contraction of a*b+c into fma: nvcc --fmad=false, gcc -ffp-contract=off.
+ *
+ * Method (textbook, no library constants):
+ *   pow(x, a) = exp(a ln x)
+ *   ln x : x = 2^e m with m in [sqrt(1/2), sqrt(2));  ln m = 2 atanh(s), s = (m-1)/(m+1),
+ *          atanh s = s (1 + z/3 + z^2/5 + ...), z = s^2 <= 0.0295  (series truncated after z^11,
+ *          remainder < 1e-18 relative).  See Abramowitz & Stegun 4.1.28 (ln((1+s)/(1-s))).
+ *   exp y: Cody & Waite (1980) reduction y = k ln2 + r, |r| <= ln2/2, e^r by its Taylor series
+ *          to r^14/14! (remainder < 5e-18), result scaled by 2^k through the exponent field.
+ * Accuracy: a few ulp in double, far below what the drag model needs; the point is that host
+ * and device produce the same bits.  Checked against libm pow by the CPU tests and host vs
+ * device bit-equality by the GPU tests.
+ */
+#ifndef ST_POW_H
+#define ST_POW_H
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define ST_HD __host__ __device__ __forceinline__
+#else
+#define ST_HD static inline
+#include <string.h>
+#endif
+
+ST_HD uint64_t st_bits_of(double x)
+{
+#if defined(__CUDA_ARCH__)
+    return (uint64_t)__double_as_longlong(x);
+#else
+    uint64_t b;
+    memcpy(&b, &x, sizeof b);
+    return b;
+#endif
+}
+
+ST_HD double st_double_of(uint64_t b)
+{
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double((long long)b);
+#else
+    double x;
+    memcpy(&x, &b, sizeof x);
+    return x;
+#endif
+}
+
+/* 2^k for -1022 <= k <= 1023, built from the exponent field (exact). */
+ST_HD double st_pow2i(int k)
+{
+    return st_double_of((uint64_t)(k + 1023) << 52);
+}
+
+/* Natural logarithm for finite x > 0. */
+ST_HD double st_log_pos(double x)
+{
+    const double LN2 = 0.69314718055994530942;
+    const double SQRT2 = 1.41421356237309504880;
+    int e = 0;
+    if (x < 2.2250738585072014e-308) { /* subnormal: scale into the normal range first */
+        x = x * 18014398509481984.0;    /* 2^54, exact */
+        e = -54;
+    }
+    uint64_t b = st_bits_of(x);
+    e += (int)((b >> 52) & 0x7ff) - 1023;
+    double m = st_double_of((b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL); /* [1,2) */
+    if (m > SQRT2) {
+        m = m * 0.5;
+        e += 1;
+    }
+    double s = (m - 1.0) / (m + 1.0);
+    double z = s * s;
+    double p = 1.0 / 23.0;
+    p = p * z + 1.0 / 21.0;
+    p = p * z + 1.0 / 19.0;
+    p = p * z + 1.0 / 17.0;
+    p = p * z + 1.0 / 15.0;
+    p = p * z + 1.0 / 13.0;
+    p = p * z + 1.0 / 11.0;
+    p = p * z + 1.0 / 9.0;
+    p = p * z + 1.0 / 7.0;
+    p = p * z + 1.0 / 5.0;
+    p = p * z + 1.0 / 3.0;
+    p = p * z + 1.0;
+    double lnm = (2.0 * s) * p;
+    return (double)e * LN2 + lnm;
+}
+
+/* Exponential for |y| <= 700. */
+ST_HD double st_exp_small(double y)
+{
+    const double LN2 = 0.69314718055994530942;
+    const double INV_LN2 = 1.44269504088896340736;
+    double t = y * INV_LN2;
+    /* round to nearest integer without library calls: |t| < 1100 */
+    int k = (int)(t >= 0.0 ? t + 0.5 : t - 0.5);
+    double r = y - (double)k * LN2;
+    double p = 1.0 / 87178291200.0;          /* 1/14! */
+    p = p * r + 1.0 / 6227020800.0;          /* 1/13! */
+    p = p * r + 1.0 / 479001600.0;           /* 1/12! */
+    p = p * r + 1.0 / 39916800.0;            /* 1/11! */
+    p = p * r + 1.0 / 3628800.0;             /* 1/10! */
+    p = p * r + 1.0 / 362880.0;              /* 1/9!  */
+    p = p * r + 1.0 / 40320.0;               /* 1/8!  */
+    p = p * r + 1.0 / 5040.0;                /* 1/7!  */
+    p = p * r + 1.0 / 720.0;                 /* 1/6!  */
+    p = p * r + 1.0 / 120.0;                 /* 1/5!  */
+    p = p * r + 1.0 / 24.0;                  /* 1/4!  */
+    p = p * r + 1.0 / 6.0;                   /* 1/3!  */
+    p = p * r + 0.5;                         /* 1/2!  */
+    p = p * r + 1.0;
+    p = p * r + 1.0;
+    /* scale by 2^k in two halves so that k down to -1074 does not leave the exponent range */
+    int k1 = k / 2;
+    int k2 = k - k1;
+    return (p * st_pow2i(k1)) * st_pow2i(k2);
+}
+
+/* x^0.687 for x >= 0 (0 for x <= 0, x itself for inf/nan). */
+ST_HD double st_pow0687(double x)
+{
+    if (!(x > 0.0)) return x != x ? x : 0.0;
+    if (x > 1.0e300) return x;
+    return st_exp_small(0.687 * st_log_pos(x));
+}
+
+/* Single-precision entry used by the mixed and FP32 paths: evaluate in double, round once. */
+ST_HD float st_pow0687f(float x)
+{
+    return (float)st_pow0687((double)x);
+}
+
+#endif /* ST_POW_H */

@@ -1,0 +1,225 @@
+/*
+ * st_sort.cu -- periodic Morton re-sort of a cloud's parcels by owning cell, and the
+ * kernels that hand the state back in the caller's order.
+ *
+ * Sorting keeps parcels of the same cell next to each other, so the warp-level run
+ * reduction of the deposit collapses most of a tile into a few atomics, and neighbouring
+ * warps gather neighbouring cells of U (L2 locality).  Keys are the Morton code of the cell
+ * (i, j, k) (or the linear cell index for meshes wider than 1024 cells), sorted with CUB's
+ * stable LSD radix sort, then every SoA array and the parcel id are gathered out of place
+ * into the other buffer.  The reference has no re-sort: its parcels keep their Hilbert
+ * ordered initial positions inside each chunk (A:559-638).
+ */
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+
+#include "st_internal.h"
+
+namespace st {
+
+__device__ __forceinline__ uint32_t spread3(uint32_t v)
+{
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__device__ __forceinline__ float fl(float v) { return floorf(v); }
+__device__ __forceinline__ double fl(double v) { return floor(v); }
+
+/* cell (i,j,k) of a parcel clamped to the mesh; only an ordering key, never an index */
+template <class P>
+__device__ __forceinline__ void cell_ijk(const MeshK<P>& m, P x, P y, P z, int32_t& i,
+                                         int32_t& j, int32_t& k)
+{
+    P fx = fl((x - m.origin[0]) * m.rD[0]);
+    P fy = fl((y - m.origin[1]) * m.rD[1]);
+    P fz = fl((z - m.origin[2]) * m.rD[2]);
+    i = fx < (P)0 ? 0 : (fx >= (P)m.N[0] ? m.N[0] - 1 : (int32_t)fx);
+    j = fy < (P)0 ? 0 : (fy >= (P)m.N[1] ? m.N[1] - 1 : (int32_t)fy);
+    k = fz < (P)0 ? 0 : (fz >= (P)m.N[2] ? m.N[2] - 1 : (int32_t)fz);
+}
+
+template <class P>
+__global__ void k_sort_keys(const P* __restrict__ x, const P* __restrict__ y,
+                            const P* __restrict__ z, int64_t n, MeshK<P> m, int morton,
+                            uint32_t* __restrict__ keys, uint32_t* __restrict__ perm)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        int32_t i, j, k;
+        cell_ijk(m, x[p], y[p], z[p], i, j, k);
+        uint32_t key = morton ? (spread3((uint32_t)i) | (spread3((uint32_t)j) << 1) |
+                                 (spread3((uint32_t)k) << 2))
+                              : (uint32_t)(k * m.NxNy + j * m.N[0] + i);
+        keys[p] = key;
+        perm[p] = (uint32_t)p;
+    }
+}
+
+template <class P, class V>
+__global__ void k_gather(const uint32_t* __restrict__ perm, int64_t n,
+                         const P* __restrict__ x0, const P* __restrict__ y0,
+                         const P* __restrict__ z0, const V* __restrict__ u0,
+                         const V* __restrict__ v0, const V* __restrict__ w0,
+                         const V* __restrict__ d0, const int32_t* __restrict__ id0,
+                         P* __restrict__ x1, P* __restrict__ y1, P* __restrict__ z1,
+                         V* __restrict__ u1, V* __restrict__ v1, V* __restrict__ w1,
+                         V* __restrict__ d1, int32_t* __restrict__ id1)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = perm[p];
+        x1[p] = x0[s];
+        y1[p] = y0[s];
+        z1[p] = z0[s];
+        u1[p] = u0[s];
+        v1[p] = v0[s];
+        w1[p] = w0[s];
+        d1[p] = d0[s];
+        id1[p] = id0[s];
+    }
+}
+
+/* out[id[p]] = in[p]: back to the order of st_set_parcels */
+template <class P, class V>
+__global__ void k_unpermute(const int32_t* __restrict__ id, int64_t n,
+                            const P* __restrict__ x0, const P* __restrict__ y0,
+                            const P* __restrict__ z0, const V* __restrict__ u0,
+                            const V* __restrict__ v0, const V* __restrict__ w0,
+                            const V* __restrict__ d0, P* __restrict__ x1, P* __restrict__ y1,
+                            P* __restrict__ z1, V* __restrict__ u1, V* __restrict__ v1,
+                            V* __restrict__ w1, V* __restrict__ d1)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = id[p];
+        x1[t] = x0[p];
+        y1[t] = y0[p];
+        z1[t] = z0[p];
+        u1[t] = u0[p];
+        v1[t] = v0[p];
+        w1[t] = w0[p];
+        d1[t] = d0[p];
+    }
+}
+
+/* Owning cell with the step's own locate semantics (A:680-693), 0-based; -1 and a count
+ * when the parcel is outside the mesh. */
+template <class P>
+__global__ void k_cells(const P* __restrict__ x, const P* __restrict__ y,
+                        const P* __restrict__ z, const int32_t* __restrict__ id, int64_t n,
+                        MeshK<P> m, int32_t* __restrict__ cells, unsigned long long* outside)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        P fv[3] = {fl((x[p] - m.origin[0]) * m.rD[0]), fl((y[p] - m.origin[1]) * m.rD[1]),
+                   fl((z[p] - m.origin[2]) * m.rD[2])};
+        int32_t g[3];
+        bool bad = false;
+        for (int a = 0; a < 3; ++a) {
+            if (!(fv[a] >= (P)-2147483648.0 && fv[a] < (P)2147483648.0)) {
+                bad = true;
+                g[a] = 0;
+            } else {
+                g[a] = (int32_t)fv[a];
+            }
+        }
+        int32_t part = 1, pos = 0;
+        if (!bad) {
+            int32_t q[3], r[3];
+            for (int a = 0; a < 3; ++a) {
+                q[a] = g[a] / m.N[a];
+                r[a] = g[a] - q[a] * m.N[a];
+            }
+            part = abs(q[2]) + abs(q[1]) + abs(q[0]) + 1;
+            pos = abs(r[2]) * m.NxNy + abs(r[1]) * m.N[0] + abs(r[0]);
+        }
+        const bool out = bad || part != 1;
+        if (out && outside) atomicAdd(outside, 1ULL);
+        cells[id ? id[p] : p] = out ? -1 : pos;
+    }
+}
+
+static int grid_for(int64_t n)
+{
+    int64_t g = (n + 255) / 256;
+    if (g > 148 * 16) g = 148 * 16;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+template <class P, class V>
+size_t sort_temp_bytes(int64_t n)
+{
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t*)nullptr,
+                                    (uint32_t*)nullptr, (const uint32_t*)nullptr,
+                                    (uint32_t*)nullptr, (int)n, 0, 32);
+    return bytes;
+}
+
+template <class P, class V>
+cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& mesh, int key_bits,
+                       bool morton, cudaStream_t s, int* launches)
+{
+    if (n <= 1) return cudaSuccess;
+    const int o = 1 - cur;
+    k_sort_keys<P><<<grid_for(n), 256, 0, s>>>(b.x[cur], b.y[cur], b.z[cur], n, mesh,
+                                               morton ? 1 : 0, b.keys[0], b.perm[0]);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    size_t bytes = b.temp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(b.temp, bytes, b.keys[0], b.keys[1], b.perm[0],
+                                        b.perm[1], (int)n, 0, key_bits, s);
+    if (e != cudaSuccess) return e;
+    k_gather<P, V><<<grid_for(n), 256, 0, s>>>(b.perm[1], n, b.x[cur], b.y[cur], b.z[cur],
+                                               b.u[cur], b.v[cur], b.w[cur], b.d[cur],
+                                               b.id[cur], b.x[o], b.y[o], b.z[o], b.u[o],
+                                               b.v[o], b.w[o], b.d[o], b.id[o]);
+    if (launches) *launches += 2;  /* our keys and gather kernels; CUB's own are not counted */
+    return cudaGetLastError();
+}
+
+template <class P, class V>
+cudaError_t unpermute_cloud(SortBufs<P, V>& b, int cur, int64_t n, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const int o = 1 - cur;
+    k_unpermute<P, V><<<grid_for(n), 256, 0, s>>>(b.id[cur], n, b.x[cur], b.y[cur], b.z[cur],
+                                                  b.u[cur], b.v[cur], b.w[cur], b.d[cur],
+                                                  b.x[o], b.y[o], b.z[o], b.u[o], b.v[o],
+                                                  b.w[o], b.d[o]);
+    return cudaGetLastError();
+}
+
+template <class P>
+cudaError_t cells_cloud(const P* x, const P* y, const P* z, const int32_t* id, int64_t n,
+                        const MeshK<P>& mesh, int32_t* cells_out, unsigned long long* outside,
+                        cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    k_cells<P><<<grid_for(n), 256, 0, s>>>(x, y, z, id, n, mesh, cells_out, outside);
+    return cudaGetLastError();
+}
+
+#define ST_INST(P, V)                                                                         \
+    template size_t sort_temp_bytes<P, V>(int64_t);                                           \
+    template cudaError_t sort_cloud<P, V>(SortBufs<P, V>&, int, int64_t, const MeshK<P>&, int, \
+                                          bool, cudaStream_t, int*);                          \
+    template cudaError_t unpermute_cloud<P, V>(SortBufs<P, V>&, int, int64_t, cudaStream_t);
+ST_INST(float, float)
+ST_INST(double, float)
+ST_INST(double, double)
+template cudaError_t cells_cloud<float>(const float*, const float*, const float*,
+                                        const int32_t*, int64_t, const MeshK<float>&, int32_t*,
+                                        unsigned long long*, cudaStream_t);
+template cudaError_t cells_cloud<double>(const double*, const double*, const double*,
+                                         const int32_t*, int64_t, const MeshK<double>&, int32_t*,
+                                         unsigned long long*, cudaStream_t);
+
+}  // namespace st

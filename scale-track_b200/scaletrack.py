@@ -1,0 +1,296 @@
+"""Python host side of libscaletrack.so (ctypes), mirroring the reference's coupling surface.
+
+The reference's host language for this path is Julia calling CUDA.jl kernels, driven by an
+OpenFOAM solver through two C function pointers (allocate_array_ptr and evolve_cloud_ptr,
+A:1436-1528).  Julia is not available here, so this module is the host used by the tests
+and the benchmark; it calls the same C ABI that a Julia `ccall` or the C++ solver would
+(see include/scaletrack.h).  There is no CPU fallback: if the shared library or a CUDA
+device is missing, the calls raise.
+
+    A: run/icoJuliaParcelFoam/cavity3D/asyncParallelTracking.jl
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libscaletrack.so")
+
+ST_OK = 0
+ST_ERR_INVALID_ARGUMENT = 1
+ST_ERR_CUDA = 2
+ST_ERR_PARCEL_OUTSIDE = 3
+ST_ERR_SOURCE_RANGE = 4
+ST_ERR_NOT_INITIALISED = 5
+ST_ERR_OUT_OF_MEMORY = 6
+
+DRAG = {"stokes_implicit": 0, "schiller_naumann": 1, "sn_explicit": 1}
+PRECISION = {"fp32": 0, "mixed": 1, "fp64": 2}
+DEPOSIT = {"deterministic": 0, "atomic": 1}
+KERNEL_KINDS = {"step": 0, "finalize": 1, "sort": 2, "probe": 3, "other": 4}
+
+# every symbol include/scaletrack.h declares
+EXPORTS = [
+    "st_version", "st_last_error", "st_params_default", "st_create", "st_destroy",
+    "st_set_parcels", "st_get_parcels", "st_get_cells", "st_num_parcels", "st_num_cells",
+    "st_set_fluid_velocity", "st_set_fluid_velocity_device", "st_step", "st_get_source",
+    "st_source_device", "st_synchronize", "st_get_stream", "st_set_stream",
+    "st_profile_enable", "st_profile_read", "st_launch_count", "st_setup", "st_default_handle",
+    "st_allocate_array", "st_evolve_cloud", "st_finalize",
+]
+
+
+class ScaleTrackError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"scaletrack error {code}: {msg}")
+        self.code = code
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32 * 3), ("origin", ctypes.c_double * 3),
+                ("ending", ctypes.c_double * 3)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("mu_c", ctypes.c_double), ("rho_c", ctypes.c_double), ("rho_d", ctypes.c_double),
+        ("drag_model", ctypes.c_int32), ("precision", ctypes.c_int32),
+        ("deposit", ctypes.c_int32), ("n_substeps", ctypes.c_int32),
+        ("sort_interval", ctypes.c_int32), ("n_clouds", ctypes.c_int32),
+        ("block_size", ctypes.c_int32), ("grid_blocks", ctypes.c_int32),
+        ("drag_multiplier", ctypes.c_double), ("diameter_scale", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libscaletrack.so; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ScaleTrackError(-1, f"{LIB_PATH} is missing: run scale-track_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    c_h = ctypes.c_void_p
+    sig = {
+        "st_version": ([], ctypes.c_char_p),
+        "st_last_error": ([], ctypes.c_char_p),
+        "st_params_default": ([P(Params)], None),
+        "st_create": ([P(Params), P(MeshDesc), ctypes.c_int, P(c_h)], ctypes.c_int),
+        "st_destroy": ([c_h], ctypes.c_int),
+        "st_set_parcels": ([c_h, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p,
+                            ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+        "st_get_parcels": ([c_h, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_void_p], ctypes.c_int),
+        "st_get_cells": ([c_h, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+        "st_num_parcels": ([c_h, ctypes.c_int], ctypes.c_int64),
+        "st_num_cells": ([c_h], ctypes.c_int64),
+        "st_set_fluid_velocity": ([c_h, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+        "st_set_fluid_velocity_device": ([c_h, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+        "st_step": ([c_h, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+        "st_get_source": ([c_h, ctypes.c_int, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+        "st_source_device": ([c_h, ctypes.c_int], ctypes.c_void_p),
+        "st_synchronize": ([c_h], ctypes.c_int),
+        "st_get_stream": ([c_h], ctypes.c_void_p),
+        "st_set_stream": ([c_h, ctypes.c_void_p], ctypes.c_int),
+        "st_profile_enable": ([c_h, ctypes.c_int], ctypes.c_int),
+        "st_profile_read": ([c_h, ctypes.c_int, P(ctypes.c_int64), P(ctypes.c_double),
+                             ctypes.c_int], ctypes.c_int),
+        "st_launch_count": ([c_h], ctypes.c_int64),
+        "st_setup": ([P(Params), P(MeshDesc)], ctypes.c_int),
+        "st_default_handle": ([], c_h),
+        "st_allocate_array": ([ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+                              ctypes.c_void_p),
+        "st_evolve_cloud": ([ctypes.c_double], ctypes.c_int),
+        "st_finalize": ([], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def last_error():
+    return lib().st_last_error().decode()
+
+
+def _check(rc):
+    if rc != ST_OK:
+        raise ScaleTrackError(rc, last_error())
+    return rc
+
+
+def _vec3(v):
+    return [v] * 3 if np.isscalar(v) else list(v)
+
+
+def mesh_desc(n, origin, ending):
+    """Uniform cuboid mesh; like the reference's Mesh(N, origin, ending) (A:259-268)."""
+    m = MeshDesc()
+    m.n = (ctypes.c_int32 * 3)(*[int(x) for x in _vec3(n)])
+    m.origin = (ctypes.c_double * 3)(*[float(x) for x in _vec3(origin)])
+    m.ending = (ctypes.c_double * 3)(*[float(x) for x in _vec3(ending)])
+    return m
+
+
+def params(**kw):
+    """st_params with the library defaults (the reference's setup.jl) overridden by kw.
+    String values are accepted for drag_model, precision and deposit."""
+    p = Params()
+    lib().st_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        if k == "drag_model" and isinstance(v, str):
+            v = DRAG[v]
+        elif k == "precision" and isinstance(v, str):
+            v = PRECISION[v]
+        elif k == "deposit" and isinstance(v, str):
+            v = DEPOSIT[v]
+        if not hasattr(p, k):
+            raise TypeError(f"unknown parameter {k}")
+        setattr(p, k, v)
+    return p
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class ParcelTracker:
+    """One handle: a mesh, its cell fields and n_clouds parcel clouds on one GPU."""
+
+    def __init__(self, prm, mesh, device=0):
+        self._h = ctypes.c_void_p()
+        self.params = prm
+        self.mesh = mesh
+        _check(lib().st_create(ctypes.byref(prm), ctypes.byref(mesh), device,
+                               ctypes.byref(self._h)))
+        self.ncells = int(lib().st_num_cells(self._h))
+
+    def close(self):
+        if self._h:
+            lib().st_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_parcels(self, xyz, uvw, d, cloud=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        uvw = np.ascontiguousarray(uvw, dtype=np.float64)
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        n = d.shape[0]
+        assert xyz.shape == (3, n) and uvw.shape == (3, n)
+        _check(lib().st_set_parcels(self._h, cloud, n, _dptr(xyz), _dptr(uvw), _dptr(d)))
+
+    def num_parcels(self, cloud=0):
+        return int(lib().st_num_parcels(self._h, cloud))
+
+    def get_parcels(self, cloud=0, check=True):
+        n = self.num_parcels(cloud)
+        xyz = np.empty((3, n))
+        uvw = np.empty((3, n))
+        d = np.empty(n)
+        rc = lib().st_get_parcels(self._h, cloud, _dptr(xyz), _dptr(uvw), _dptr(d))
+        if check:
+            _check(rc)
+        return xyz, uvw, d
+
+    def get_cells(self, cloud=0, check=True):
+        n = self.num_parcels(cloud)
+        cells = np.empty(n, dtype=np.int32)
+        rc = lib().st_get_cells(self._h, cloud, _dptr(cells))
+        if check:
+            _check(rc)
+        return cells
+
+    def set_fluid_velocity(self, U):
+        U = np.ascontiguousarray(U)
+        assert U.shape == (self.ncells, 3) and U.dtype in (np.float32, np.float64)
+        _check(lib().st_set_fluid_velocity(self._h, _dptr(U), U.dtype.itemsize))
+
+    def set_fluid_velocity_device(self, ptr, elem_bytes):
+        _check(lib().st_set_fluid_velocity_device(self._h, ctypes.c_void_p(ptr), elem_bytes))
+
+    def step(self, dt, fluid_scale=1.0):
+        _check(lib().st_step(self._h, dt, fluid_scale))
+
+    def get_source(self, cloud=0, dtype=np.float64, check=True):
+        S = np.empty((self.ncells, 3), dtype=dtype)
+        rc = lib().st_get_source(self._h, cloud, _dptr(S), S.dtype.itemsize)
+        if check:
+            _check(rc)
+        return S
+
+    def source_device_ptr(self, cloud=0):
+        return lib().st_source_device(self._h, cloud)
+
+    def synchronize(self):
+        _check(lib().st_synchronize(self._h))
+
+    def stream(self):
+        return lib().st_get_stream(self._h)
+
+    def profile(self, on=True):
+        _check(lib().st_profile_enable(self._h, 1 if on else 0))
+
+    def profile_read(self, kind, reset=False):
+        n = ctypes.c_int64()
+        ms = ctypes.c_double()
+        k = KERNEL_KINDS[kind] if isinstance(kind, str) else kind
+        _check(lib().st_profile_read(self._h, k, ctypes.byref(n), ctypes.byref(ms),
+                                     1 if reset else 0))
+        return int(n.value), float(ms.value)
+
+    def launch_count(self):
+        return int(lib().st_launch_count(self._h))
+
+
+# ---------------------------------------------------------------------------------------
+# the reference's coupling surface (process-wide default handle)
+# ---------------------------------------------------------------------------------------
+def setup(prm, mesh):
+    """Creates the default handle used by allocate_array and evolve_cloud."""
+    _check(lib().st_setup(ctypes.byref(prm), ctypes.byref(mesh)))
+
+
+def default_handle():
+    return lib().st_default_handle()
+
+
+def allocate_array(name, size, n_components, type_byte_size):
+    """allocate_array_ptr (A:1436-1483): library-owned pinned storage [size][n_components]
+    returned as a numpy view, which the caller fills (U) or reads (UTrans) in place."""
+    p = lib().st_allocate_array(name.encode(), size, n_components, type_byte_size)
+    if not p:
+        raise ScaleTrackError(ST_ERR_INVALID_ARGUMENT, last_error())
+    ctype = ctypes.c_float if type_byte_size == 4 else ctypes.c_double
+    buf = (ctype * (size * n_components)).from_address(p)
+    return np.ctypeslib.as_array(buf).reshape(size, n_components)
+
+
+def evolve_cloud(dt):
+    """evolve_cloud (A:1485-1528): one synchronous step on the default handle."""
+    _check(lib().st_evolve_cloud(dt))
+
+
+def finalize():
+    _check(lib().st_finalize())

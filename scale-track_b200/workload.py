@@ -1,0 +1,86 @@
+"""Synthetic inputs of the benchmark configurations (seeded, host-generated).
+
+No public dataset or benchmark suite is involved; the reference itself uses random parcels
+(init!/initWithHilbert!, A:504-638) and a random cell velocity in its REPL test (A:1645-1650).
+These generators produce the benchmark's inputs on the host so that the GPU path and the
+CPU oracle consume identical bytes:
+
+  * fluid: U = U0 (sin(pi x/L) cos(pi y/L) cos(pi z/L), -cos(pi x/L) sin(pi y/L) cos(pi z/L), 0)
+    at cell centres, optionally scaled per step by (1 + 0.2 sin(2 pi t / 0.05 s));
+  * parcels: positions uniform in the box, velocity 0, diameters lognormal
+    d = 20 um * exp(0.3 N(0,1)), numpy PCG64 streams seeded per configuration;
+  * physics: rho_p = 1000, rho_f = 1.2 kg/m^3, nu = 1.5e-5 m^2/s (mu_f = 1.8e-5 Pa s),
+    Schiller-Naumann drag, explicit Euler, dt = 1e-4 s, reflecting walls.
+"""
+import numpy as np
+
+RHO_P = 1000.0
+RHO_F = 1.2
+NU_F = 1.5e-5
+MU_F = RHO_F * NU_F
+DT = 1e-4
+L_BOX = 0.1
+
+CONFIGS = {
+    # 32^3 hex, 1e5 parcels, FP64, 100 steps (the CPU-runnable case)
+    "c0_fp64_32": dict(n=32, nparcels=100_000, seed=0, precision="fp64", steps=100,
+                       U0=1.0, time_varying=False, sort_interval=0),
+    # 128^3 hex, 1e7 parcels, mixed precision, 500 steps, Morton re-sort every 20 steps,
+    # time-varying field
+    "c1_mixed_128": dict(n=128, nparcels=10_000_000, seed=0, precision="mixed", steps=500,
+                         U0=1.0, time_varying=True, sort_interval=20),
+}
+
+
+def cell_centres(n, L=L_BOX):
+    h = L / n
+    c = (np.arange(n) + 0.5) * h
+    # cell index k*n*n + j*n + i (x fastest), A:684-691
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    return x.reshape(-1), y.reshape(-1), z.reshape(-1)
+
+
+def tgv_field(n, U0=1.0, L=L_BOX, dtype=np.float32):
+    """Taylor-Green-like analytic field at cell centres, [n^3, 3] (cell-major AoS)."""
+    x, y, z = cell_centres(n, L)
+    a, b, c = np.pi * x / L, np.pi * y / L, np.pi * z / L
+    U = np.empty((x.size, 3), dtype=np.float64)
+    U[:, 0] = U0 * np.sin(a) * np.cos(b) * np.cos(c)
+    U[:, 1] = -U0 * np.cos(a) * np.sin(b) * np.cos(c)
+    U[:, 2] = 0.0
+    return U.astype(dtype)
+
+
+def parcels(nparcels, seed, L=L_BOX, d_median=20e-6, sigma=0.3, dtype_v=np.float32):
+    """Positions uniform in [0, L)^3 (FP64), zero velocity, lognormal diameters rounded to
+    the velocity precision (so that every consumer sees the same values)."""
+    rng = np.random.default_rng(seed)
+    xyz = rng.random((3, nparcels)) * L
+    np.minimum(xyz, L * (1.0 - 1e-6), out=xyz)  # stays inside after rounding to FP32
+    d = (d_median * np.exp(sigma * rng.standard_normal(nparcels))).astype(dtype_v)
+    uvw = np.zeros((3, nparcels), dtype=np.float64)
+    return xyz, uvw, d.astype(np.float64)
+
+
+def fluid_scale(step, dt=DT, time_varying=True):
+    """(1 + 0.2 sin(2 pi t / 0.05 s)) with t at the start of the step."""
+    if not time_varying:
+        return 1.0
+    t = step * dt
+    return 1.0 + 0.2 * np.sin(2.0 * np.pi * t / 0.05)
+
+
+def algorithmic_bytes(precision, nparcels, ncells):
+    """Compulsory HBM traffic of one step (bytes): parcel state read + written once, U read
+    once and the FP64 source written once.  Per parcel: mixed 40 R + 36 W = 76 B, FP64
+    56 R + 48 W = 104 B, FP32 28 R + 24 W = 52 B.  Per cell: U (12 or 24 B) + source 24 B."""
+    bp = {"mixed": 76, "fp64": 104, "fp32": 52}[precision]
+    bc = {"mixed": 36, "fp64": 48, "fp32": 36}[precision]
+    return nparcels * bp + ncells * bc
+
+
+def step_kernel_bytes(precision, nparcels, ncells):
+    """Compulsory traffic of the step kernel alone (the source write belongs to finalize)."""
+    bp = {"mixed": 76, "fp64": 104, "fp32": 52}[precision]
+    bu = {"mixed": 12, "fp64": 24, "fp32": 12}[precision]
+    return nparcels * bp + ncells * bu

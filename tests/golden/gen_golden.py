@@ -1,0 +1,288 @@
+"""Generates the golden fixtures in tests/golden/*.npz.
+
+An independent, line-by-line restatement of the reference's parcel step in numpy float32
+scalars (Julia Float32 arithmetic is IEEE binary32 without fma contraction, and so are
+numpy float32 scalar operations).  It deliberately shares no code with the C++ oracle, so
+agreement between the two is a cross-check of both restatements.
+
+Reference file (A:): run/icoJuliaParcelFoam/cavity3D/asyncParallelTracking.jl
+  locate_ijk / locate ........................ A:663-697
+  update! (CPU, '+=') / update_at_boundary! .. A:703-708, A:731-736
+  evolve_particle! ........................... A:1271-1365
+  CPU executor loop, Δt/nSteps ............... A:818-823, A:1260
+  Mesh construction (Float64 -> Float32) ..... A:237-268
+
+The Schiller-Naumann drag is project-defined (the reference only has Stokes drag); its
+power function follows the same textbook algorithm as scale-track_b200/csrc/st_pow.h,
+restated here in Python floats.
+
+Run:  python tests/golden/gen_golden.py      (rewrites the .npz files next to this script)
+"""
+import math
+import os
+import struct
+
+import numpy as np
+
+F = np.float32
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+# ----------------------------------------------------------------------------- power helper
+def _bits(x):
+    return struct.unpack("<Q", struct.pack("<d", x))[0]
+
+
+def _dbl(b):
+    return struct.unpack("<d", struct.pack("<Q", b))[0]
+
+
+def _pow2i(k):
+    return _dbl((k + 1023) << 52)
+
+
+def _log_pos(x):
+    LN2 = 0.69314718055994530942
+    SQRT2 = 1.41421356237309504880
+    e = 0
+    if x < 2.2250738585072014e-308:
+        x = x * 18014398509481984.0
+        e = -54
+    b = _bits(x)
+    e += ((b >> 52) & 0x7FF) - 1023
+    m = _dbl((b & 0x000FFFFFFFFFFFFF) | 0x3FF0000000000000)
+    if m > SQRT2:
+        m = m * 0.5
+        e += 1
+    s = (m - 1.0) / (m + 1.0)
+    z = s * s
+    p = 1.0 / 23.0
+    for c in (21.0, 19.0, 17.0, 15.0, 13.0, 11.0, 9.0, 7.0, 5.0, 3.0):
+        p = p * z + 1.0 / c
+    p = p * z + 1.0
+    return float(e) * LN2 + (2.0 * s) * p
+
+
+def _exp_small(y):
+    LN2 = 0.69314718055994530942
+    INV_LN2 = 1.44269504088896340736
+    t = y * INV_LN2
+    k = int(t + 0.5) if t >= 0.0 else -int(-t + 0.5)
+    r = y - float(k) * LN2
+    p = 1.0 / 87178291200.0
+    for c in (6227020800.0, 479001600.0, 39916800.0, 3628800.0, 362880.0, 40320.0, 5040.0,
+              720.0, 120.0, 24.0, 6.0):
+        p = p * r + 1.0 / c
+    p = p * r + 0.5
+    p = p * r + 1.0
+    p = p * r + 1.0
+    k1 = int(k / 2)
+    k2 = k - k1
+    return (p * _pow2i(k1)) * _pow2i(k2)
+
+
+def pow0687(x):
+    x = float(x)
+    if not (x > 0.0):
+        return x if x != x else 0.0
+    if x > 1.0e300:
+        return x
+    return _exp_small(0.687 * _log_pos(x))
+
+
+# ----------------------------------------------------------------------------- the step
+class Mesh:
+    """construct_mesh (A:237-268) with decomposition (1,1,1)."""
+
+    def __init__(self, n, origin, ending):
+        self.N = [int(v) for v in n]
+        self.origin = [F(o) for o in origin]
+        self.rD = []
+        for a in range(3):
+            L = float(ending[a]) - float(origin[a])
+            D = L / float(n[a])
+            self.rD.append(F(1.0 / D))
+        self.NxNy = self.N[0] * self.N[1]
+
+
+def floor_label(v):
+    f = np.floor(v)
+    assert -2.0 ** 31 <= float(f) < 2.0 ** 31
+    return int(f)
+
+
+def _divrem(a, b):
+    q = abs(a) // b
+    q = q if a >= 0 else -q
+    return q, a - q * b
+
+
+def locate(m, x, y, z):
+    I = floor_label(F(x - m.origin[0]) * m.rD[0])
+    J = floor_label(F(y - m.origin[1]) * m.rD[1])
+    K = floor_label(F(z - m.origin[2]) * m.rD[2])
+    iP, iL = _divrem(I, m.N[0])
+    jP, jL = _divrem(J, m.N[1])
+    kP, kL = _divrem(K, m.N[2])
+    part = abs(kP) + abs(jP) + abs(iP) + 1
+    pos = abs(kL) * m.NxNy + abs(jL) * m.N[0] + abs(iL) + 1
+    return I, J, K, pos, part
+
+
+def evolve_particle(m, prm, X, Y, Z, U, V, W, dIn, Ucell, fs, dt, nsteps, UTrans32, UTrans64):
+    mu, rho_d, rr, nu, drag = prm["mu"], prm["rho_d"], prm["rr"], prm["nu"], prm["drag"]
+    d = F(dIn * F(1.0))
+    mB = F(F(F(rr * F(math.pi)) * F(F(d * d) * d)) / F(6))
+    pos = [X, Y, Z]
+    vel = [U, V, W]
+    posNew = list(pos)
+    velNew = list(vel)
+    I, J, K, posI, partI = locate(m, *pos)
+    assert partI == 1
+    uc = [F(Ucell[posI - 1][c] * fs) for c in range(3)]
+    state0 = list(vel)
+    f = F(F(F(F(18) * mu) * dt) / F(rho_d * F(d * d)))
+
+    def deposit(cell, s0, vn):
+        for c in range(3):
+            dep = F(mB * F(s0[c] - vn[c]))
+            UTrans32[cell - 1][c] = F(UTrans32[cell - 1][c] + dep)
+            UTrans64[cell - 1][c] = UTrans64[cell - 1][c] + float(dep)
+
+    for t in range(1, nsteps + 1):
+        if drag == 0:
+            for c in range(3):
+                velNew[c] = F(F(vel[c] + F(f * uc[c])) / F(F(1) + f))
+        else:
+            du = [F(uc[c] - vel[c]) for c in range(3)]
+            mag = F(np.sqrt(F(F(F(du[0] * du[0]) + F(du[1] * du[1])) + F(du[2] * du[2]))))
+            Re = F(F(mag * d) / nu)
+            pw = F(pow0687(float(Re)))
+            g = F(f * F(F(1) + F(F(0.15) * pw)))
+            for c in range(3):
+                velNew[c] = F(vel[c] + F(g * du[c]))
+        for c in range(3):
+            posNew[c] = F(pos[c] + F(velNew[c] * dt))
+        I, J, K, posNewI, partNewI = locate(m, *posNew)
+        if posNewI != posI or partNewI != partI:
+            b = [I < 0 or I >= m.N[0], J < 0 or J >= m.N[1], K < 0 or K >= m.N[2]]
+            for c in range(3):
+                if b[c]:
+                    posNew[c] = pos[c]
+                    velNew[c] = F(-vel[c])
+                    state0[c] = F(state0[c] - F(F(2) * vel[c]))
+            if any(b):
+                I, J, K, posNewI, partNewI = locate(m, *posNew)
+            if t != nsteps and posNewI != posI:
+                deposit(posI, state0, velNew)
+                state0 = list(velNew)
+                uc = [F(Ucell[posNewI - 1][c] * fs) for c in range(3)]
+                posI = posNewI
+        vel = list(velNew)
+        pos = list(posNew)
+    deposit(posI, state0, velNew)
+    return posNew, velNew
+
+
+def run_case(n, origin, ending, mu_c, rho_c, rho_d, drag, nsub, xyz, uvw, d, Ucell, dt, nsteps):
+    m = Mesh(n, origin, ending)
+    prm = dict(mu=F(mu_c), rho_d=F(rho_d), rr=F(rho_d / rho_c), nu=F(mu_c / rho_c), drag=drag)
+    npcl = d.shape[0]
+    X = [F(v) for v in xyz[0]]
+    Y = [F(v) for v in xyz[1]]
+    Z = [F(v) for v in xyz[2]]
+    U = [F(v) for v in uvw[0]]
+    V = [F(v) for v in uvw[1]]
+    W = [F(v) for v in uvw[2]]
+    D = [F(v) for v in d]
+    Uc = [[F(v) for v in row] for row in Ucell]
+    dtF = F(F(dt) / F(nsub))
+    ncells = n[0] * n[1] * n[2]
+    for s in range(nsteps):
+        UT32 = [[F(0), F(0), F(0)] for _ in range(ncells)]
+        UT64 = [[0.0, 0.0, 0.0] for _ in range(ncells)]
+        for i in range(npcl):
+            p, v = evolve_particle(m, prm, X[i], Y[i], Z[i], U[i], V[i], W[i], D[i], Uc, F(1),
+                                   dtF, nsub, UT32, UT64)
+            X[i], Y[i], Z[i] = p
+            U[i], V[i], W[i] = v
+    cells = []
+    for i in range(npcl):
+        _, _, _, pos, part = locate(m, X[i], Y[i], Z[i])
+        cells.append(pos - 1 if part == 1 else -1)
+    return dict(
+        xyz=np.array([X, Y, Z], dtype=np.float32),
+        uvw=np.array([U, V, W], dtype=np.float32),
+        cells=np.array(cells, dtype=np.int32),
+        src_f32=np.array(UT32, dtype=np.float32),
+        src_f64=np.array(UT64, dtype=np.float64),
+    )
+
+
+def make_inputs(seed, n, npcl, ending, dmin, dmax, v0_random=False, wall_cases=True):
+    """Parcels uniform in the box (as init! does, A:518-525), diameters U[dmin, dmax),
+    random cell velocity in [-1, 1) (the REPL test block, A:1645-1650), plus hand-placed
+    parcels at walls, on faces and at the origin."""
+    rng = np.random.default_rng(seed)
+    xyz = rng.random((3, npcl)).astype(np.float32) * np.float32(ending)
+    if wall_cases:
+        f = 1.0 / n
+        special = [  # fractions of the box edge: walls, exact faces, the origin
+            (0.0, 0.5, 0.5), (0.99999, 0.5, 0.5), (0.5, 1e-4, 0.5), (0.5, 0.5, 0.9999),
+            (f, f, f), (2 * f, 0.5, 3 * f), (0.0, 0.0, 0.0),
+        ]
+        for k, s in enumerate(special):
+            xyz[:, k] = np.array(s, dtype=np.float32) * np.float32(ending)
+    uvw = np.zeros((3, npcl), dtype=np.float32)
+    if v0_random:
+        uvw = (rng.random((3, npcl)) * 2.0 - 1.0).astype(np.float32)
+    uvw[:, :7] = np.array([[-0.9, 0.1, 0.2], [0.8, -0.3, 0.1], [0.1, -0.95, 0.0],
+                           [0.0, 0.2, 0.9], [-0.5, -0.5, -0.5], [0.3, 0.0, -0.4],
+                           [-1.0, -1.0, -1.0]], dtype=np.float32).T
+    d = (rng.random(npcl) * (dmax - dmin) + dmin).astype(np.float32)
+    ncells = n ** 3
+    Ucell = (rng.random((ncells, 3)) * 2.0 - 1.0).astype(np.float32)
+    return xyz, uvw, d, Ucell
+
+
+CASES = {
+    # reference physics (setup.jl: μᶜ=1e-3, ρᶜ=1e3, ρᵈ=1, d in [5e-3, 1e-2)), Stokes implicit,
+    # 10 substeps, a large Δt so that parcels cross faces and hit walls
+    "ref_stokes_fp32": dict(seed=11, n=8, npcl=96, ending=1.0, dmin=5e-3, dmax=1e-2,
+                            mu_c=1e-3, rho_c=1e3, rho_d=1.0, drag=0, nsub=10, dt=0.6, nsteps=3),
+    # same geometry, Schiller-Naumann explicit drag, one substep
+    "sn_fp32": dict(seed=12, n=8, npcl=96, ending=1.0, dmin=5e-3, dmax=1e-2,
+                    mu_c=1e-3, rho_c=1e3, rho_d=1000.0, drag=1, nsub=1, dt=0.05, nsteps=4,
+                    v0_random=True),
+    # the benchmark's physical constants on a small box
+    "sn_bench_fp32": dict(seed=13, n=6, npcl=64, ending=0.01, dmin=1e-5, dmax=4e-5,
+                          mu_c=1.8e-5, rho_c=1.2, rho_d=1000.0, drag=1, nsub=1, dt=4e-4,
+                          nsteps=3),
+}
+
+
+def _cells0(c, xyz):
+    m = Mesh([c["n"]] * 3, [0.0] * 3, [c["ending"]] * 3)
+    return np.array([locate(m, *xyz[:, i])[3] - 1 for i in range(xyz.shape[1])])
+
+
+def main():
+    for name, c in CASES.items():
+        xyz, uvw, d, Ucell = make_inputs(c["seed"], c["n"], c["npcl"], c["ending"], c["dmin"],
+                                         c["dmax"], c.get("v0_random", False))
+        out = run_case([c["n"]] * 3, [0.0] * 3, [c["ending"]] * 3, c["mu_c"], c["rho_c"],
+                       c["rho_d"], c["drag"], c["nsub"], xyz, uvw, d, Ucell, c["dt"],
+                       c["nsteps"])
+        meta = np.array([c["n"], c["nsub"], c["drag"], c["nsteps"]], dtype=np.int64)
+        phys = np.array([c["ending"], c["mu_c"], c["rho_c"], c["rho_d"], c["dt"]])
+        np.savez(os.path.join(HERE, name + ".npz"), meta=meta, phys=phys, xyz0=xyz, uvw0=uvw,
+                 d=d, U=Ucell, **out)
+        moved = int(np.sum(out["cells"] >= 0))
+        x0 = xyz.astype(np.float64)
+        moved_cells = int(np.sum(out["cells"] != _cells0(c, xyz)))
+        print(f"{name}: {c['npcl']} parcels, located {moved}, changed cell {moved_cells}, "
+              f"|src| max {np.abs(out['src_f64']).max():.3e}")
+
+
+if __name__ == "__main__":
+    main()
