@@ -107,7 +107,8 @@ struct Params {
     V mu;           /* carrier dynamic viscosity */
     V rho_d;        /* parcel density */
     V rhod_by_rhoc; /* rho_d / rho_c */
-    V nu;           /* carrier kinematic viscosity mu/rho_c (Schiller-Naumann Re) */
+    V nu;           /* carrier kinematic viscosity mu/rho_c */
+    V rnu;          /* rho_c/mu_c: Schiller-Naumann Re = |u - v| d rnu */
     V alpha;        /* drag multiplier (1 reproduces the reference) */
     V dscale;       /* diameter scale (1 reproduces the reference) */
     int drag;
@@ -125,6 +126,7 @@ Params<P, V> make_params(const int32_t n[3], const double origin[3], const doubl
     p.rho_d = (V)rho_d;
     p.rhod_by_rhoc = (V)(rho_d / rho_c);
     p.nu = (V)(mu_c / rho_c);
+    p.rnu = (V)(rho_c / mu_c);
     p.alpha = (V)alpha;
     p.dscale = (V)dscale;
     p.drag = drag;
@@ -174,11 +176,11 @@ bool evolve_parcel(const Params<P, V>& pr, P dtP, V dtV, const double* U, V fsca
             for (int c = 0; c < 3; ++c) velNew[c] = (vel[c] + f * uc[c]) / ((V)1 + f);
         } else {
             /* Schiller-Naumann, explicit Euler (project-defined; no reference code):
-             * v' = v + f (1 + 0.15 Re^0.687) (u - v), Re = |u - v| d / nu */
+             * v' = v + f (1 + 0.15 Re^0.687) (u - v), Re = |u - v| d (1/nu) */
             V du[3];
             for (int c = 0; c < 3; ++c) du[c] = uc[c] - vel[c];
             V mag = std::sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
-            V Re = (mag * d) / pr.nu;
+            V Re = (mag * d) * pr.rnu;
             V pw = (sizeof(V) == 4) ? (V)st_pow0687f((float)Re) : (V)st_pow0687((double)Re);
             V g = f * ((V)1 + (V)0.15 * pw);
             for (int c = 0; c < 3; ++c) velNew[c] = vel[c] + g * du[c];

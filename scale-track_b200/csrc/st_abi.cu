@@ -11,7 +11,8 @@
  *   [probe + set_scale]   only on the first step after st_set_parcels or a new dt
  *   [zero source]         only in ST_DEPOSIT_ATOMIC mode
  *   step                  k_step: the parcel step and the warp-aggregated deposit
- *   finalize              fixed point -> FP64 source, clear accumulators, next scale
+ *   finalize              fixed point -> FP64 source and next scale; then a memset clears
+ *                         the accumulators
  *   [sort]                every sort_interval steps
  */
 #include <cstdarg>
@@ -90,6 +91,7 @@ struct st_handle {
     int dep = DEP_DET1;
     int limbs = 1;
     int64_t ncells = 0;
+    int64_t stride = 0;   /* per-cloud component stride of source/accumulator arrays */
     size_t psz = 4, vsz = 4;
     void* dU = nullptr;
     double* dsrc = nullptr;
@@ -161,6 +163,7 @@ PhysK<V> phys_k(const st_handle* h)
     k.rho_d = (V)h->p.rho_d;
     k.rr = (V)(h->p.rho_d / h->p.rho_c);
     k.nu = (V)(h->p.mu_c / h->p.rho_c);
+    k.rnu = (V)(h->p.rho_c / h->p.mu_c);
     k.alpha = (V)h->p.drag_multiplier;
     k.dscale = (V)h->p.diameter_scale;
     k.drag = h->p.drag_model;
@@ -288,9 +291,9 @@ int upload_clouds(st_handle* h)
         k.d = (const V*)b.d[b.cur];
         k.n = b.n;
         k.tile0 = tiles;
-        k.acc = h->dacc + (int64_t)c * h->ncells * 3 * h->limbs;
-        k.src = h->dsrc + (int64_t)c * h->ncells * 3;
-        tiles += (b.n + 31) / 32;
+        k.acc = h->dacc + (int64_t)c * h->stride * h->limbs;
+        k.src = h->dsrc + (int64_t)c * h->stride;
+        tiles += (b.n + WARP_TILE - 1) / WARP_TILE;
     }
     h->total_tiles = tiles;
     h->hclouds.resize(sizeof(CloudK<P, V>) * nc);
@@ -360,7 +363,7 @@ int do_step(st_handle* h, double dt, double fscale)
     h->last_dt = dt;
     if (!det) {
         ProfScope ps(h, ST_KERNEL_OTHER);
-        CK(launch_zero_f64(h->dsrc, (int64_t)h->p.n_clouds * h->ncells * 3, h->stream));
+        CK(launch_zero_f64(h->dsrc, (int64_t)h->p.n_clouds * h->stride, h->stream));
         h->launches += 1;
     }
     {
@@ -369,15 +372,18 @@ int do_step(st_handle* h, double dt, double fscale)
         h->launches += 1;
     }
     if (det) {
-        const int64_t ncomp = h->ncells * 3;
-        int64_t gx = (ncomp + 256 * 4 - 1) / (256 * 4);
+        int64_t gx = (h->stride / COMP_ALIGN + 255) / 256;
         int64_t cap = (148 * 8 + h->p.n_clouds - 1) / h->p.n_clouds;
         if (gx > cap) gx = cap;
         if (gx < 1) gx = 1;
-        ProfScope ps(h, ST_KERNEL_FINALIZE);
-        CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter, h->p.n_clouds, ncomp,
-                           (int)gx, h->stream));
-        h->launches += 1;
+        {
+            ProfScope ps(h, ST_KERNEL_FINALIZE);
+            CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter,
+                               h->p.n_clouds, h->stride, (int)gx, h->stream));
+            h->launches += 1;
+        }
+        CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * h->p.n_clouds * h->limbs * 8,
+                           h->stream));
     }
     h->steps += 1;
     h->steps_since_sort += 1;
@@ -621,6 +627,7 @@ int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle**
     h->m = *m;
     h->device = device;
     h->ncells = ncells;
+    h->stride = (ncells * 3 + COMP_ALIGN - 1) / COMP_ALIGN * COMP_ALIGN;
     h->psz = p->precision == ST_PREC_FP32 ? 4 : 8;
     h->vsz = p->precision == ST_PREC_FP64 ? 8 : 4;
     if (p->deposit == ST_DEPOSIT_ATOMIC) {
@@ -654,9 +661,10 @@ int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle**
         return bail(fail(ST_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)));
     h->own_stream = true;
     const size_t ncomp = (size_t)ncells * 3;
+    const size_t cells_total = (size_t)h->stride * p->n_clouds;
     if ((e = cudaMalloc(&h->dU, ncomp * h->vsz)) != cudaSuccess ||
-        (e = cudaMalloc((void**)&h->dsrc, ncomp * p->n_clouds * sizeof(double))) != cudaSuccess ||
-        (e = cudaMalloc((void**)&h->dacc, ncomp * p->n_clouds * h->limbs * 8)) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->dsrc, cells_total * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->dacc, cells_total * h->limbs * 8)) != cudaSuccess ||
         (e = cudaMalloc((void**)&h->dctl, sizeof(CloudCtl) * p->n_clouds)) != cudaSuccess ||
         (e = cudaMalloc((void**)&h->dcounter, sizeof(unsigned int))) != cudaSuccess ||
         (e = cudaMalloc((void**)&h->dcount, sizeof(unsigned long long))) != cudaSuccess ||
@@ -664,8 +672,8 @@ int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle**
         return bail(fail(e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA,
                          "device allocation: %s", cudaGetErrorString(e)));
     cudaMemsetAsync(h->dU, 0, ncomp * h->vsz, h->stream);
-    cudaMemsetAsync(h->dsrc, 0, ncomp * p->n_clouds * sizeof(double), h->stream);
-    cudaMemsetAsync(h->dacc, 0, ncomp * p->n_clouds * h->limbs * 8, h->stream);
+    cudaMemsetAsync(h->dsrc, 0, cells_total * sizeof(double), h->stream);
+    cudaMemsetAsync(h->dacc, 0, cells_total * h->limbs * 8, h->stream);
     cudaMemsetAsync(h->dcounter, 0, sizeof(unsigned int), h->stream);
     {
         std::vector<CloudCtl> ctl(p->n_clouds);
@@ -831,7 +839,7 @@ int st_step(st_handle* h, double dt, double fluid_scale)
 static int copy_source(st_handle* h, int cloud, void* S, int elem_bytes, bool sync)
 {
     const int64_t ncomp = h->ncells * 3;
-    const double* src = h->dsrc + (int64_t)cloud * ncomp;
+    const double* src = h->dsrc + (int64_t)cloud * h->stride;
     int rc;
     if (elem_bytes == 8) {
         CK(cudaMemcpyAsync(S, src, ncomp * 8, cudaMemcpyDeviceToHost, h->stream));
@@ -863,7 +871,7 @@ int st_get_source(st_handle* h, int cloud, void* S, int elem_bytes)
 const double* st_source_device(st_handle* h, int cloud)
 {
     if (!h || cloud < 0 || cloud >= h->p.n_clouds) return nullptr;
-    return h->dsrc + (int64_t)cloud * h->ncells * 3;
+    return h->dsrc + (int64_t)cloud * h->stride;
 }
 
 int st_synchronize(st_handle* h)

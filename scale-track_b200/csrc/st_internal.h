@@ -5,8 +5,8 @@
  *   parcels, per cloud, structure of arrays, two copies (A and B) so that the Morton
  *   re-sort can gather out of place:  x,y,z : P[n]   u,v,w,d : V[n]   id : int32[n]
  *   cell velocity U        : V[nCells][3]            (the exchange layout, A:204)
- *   source                 : double[nClouds][nCells][3]
- *   fixed-point accumulator: uint64[nClouds][nCells][3][limbs]   (deterministic deposit)
+ *   source                 : double[nClouds][stride]      stride = nCells*3 rounded up to 4
+ *   fixed-point accumulator: uint64[nClouds][stride][limbs]   (deterministic deposit)
  *   control blocks         : CloudCtl[nClouds]
  * P is the position type and V the velocity/drag type of the precision mode.
  */
@@ -19,6 +19,11 @@
 namespace st {
 
 constexpr int EXP_NONE = -100000;      /* "no deposit seen" for the max-exponent tracker */
+#ifndef ST_WARP_TILE
+#define ST_WARP_TILE 32
+#endif
+constexpr int WARP_TILE = ST_WARP_TILE; /* parcels per warp tile of the step kernel        */
+constexpr int COMP_ALIGN = 4;          /* per-cloud cell-array strides are padded to this  */
 constexpr int QUANT_GROWTH_BITS = 8;   /* deposits may grow 2^8 x between steps          */
 
 enum DepMode { DEP_DET1 = 0, DEP_DET2 = 1, DEP_ATOMIC = 2, DEP_PROBE = 3 };
@@ -39,6 +44,7 @@ struct PhysK {
     V rho_d;    /* parcel density */
     V rr;       /* rho_d / rho_c */
     V nu;       /* carrier kinematic viscosity */
+    V rnu;      /* 1/nu, formed in FP64 and rounded to V (Schiller-Naumann Re = |u-v| d / nu) */
     V alpha;    /* drag multiplier */
     V dscale;   /* diameter scale */
     int32_t drag;
@@ -65,9 +71,9 @@ struct CloudK {
     V* w;
     const V* d;
     int64_t n;
-    int64_t tile0;              /* first warp tile of this cloud in the launch */
-    unsigned long long* acc;    /* [nCells*3*limbs] */
-    double* src;                /* [nCells*3] */
+    int64_t tile0;              /* first warp tile (WARP_TILE parcels) of this cloud */
+    unsigned long long* acc;    /* [stride*limbs], stride = nCells*3 padded to COMP_ALIGN */
+    double* src;                /* [stride] */
 };
 
 template <class P, class V>
@@ -91,7 +97,7 @@ template <class P, class V>
 int step_max_active_blocks(int dep, int block);
 
 cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, CloudCtl* ctl,
-                            unsigned int* counter, int nclouds, int64_t ncomp, int grid_x,
+                            unsigned int* counter, int nclouds, int64_t stride, int grid_x,
                             cudaStream_t s);
 cudaError_t launch_set_scale(CloudCtl* ctl, int nclouds, cudaStream_t s);
 cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s);

@@ -1,12 +1,12 @@
 /*
  * st_kernels.cu -- the parcel step and the source reduction, written for sm_100a.
  *
- * One warp owns a tile of 32 consecutive parcels; lanes read the SoA arrays with
- * consecutive addresses (streaming loads that do not displace the L2-resident cell arrays),
- * gather the cell velocity, run the substeps in registers and write back.  The deposit of
- * each parcel into its cell (A:1342-1345, A:1361) is reduced inside the warp over runs of
- * equal cells (parcels are kept Morton-sorted by cell, so neighbours mostly share a cell)
- * and only the last lane of each run touches memory.
+ * One warp owns a tile of 128 consecutive parcels (four slices of 32); lanes read the SoA
+ * arrays with consecutive addresses (streaming loads that do not displace the L2-resident
+ * cell arrays), gather the cell velocity, run the substeps in registers and write back.
+ * The deposit of each parcel into its cell (A:1342-1345, A:1361) is reduced inside the warp
+ * over runs of equal cells (parcels are kept Morton-sorted by cell, so neighbours mostly
+ * share a cell) and only the last lane of each run touches memory.
  *
  * Deterministic deposit: every deposit component is scaled by 2^-L and rounded to a 64-bit
  * integer, so the per-cell sums are integer sums and do not depend on which warp adds
@@ -76,6 +76,12 @@ __device__ __forceinline__ LocK locate(const MeshK<P>& m, P x, P y, P z, bool& b
     r.I = floor_label((x - m.origin[0]) * m.rD[0], bad);
     r.J = floor_label((y - m.origin[1]) * m.rD[1], bad);
     r.K = floor_label((z - m.origin[2]) * m.rD[2], bad);
+    if ((uint32_t)r.I < (uint32_t)m.N[0] && (uint32_t)r.J < (uint32_t)m.N[1] &&
+        (uint32_t)r.K < (uint32_t)m.N[2]) {  /* inside: divrem is (0, i) on every axis */
+        r.part = 1;
+        r.posI = r.K * m.NxNy + r.J * m.N[0] + r.I + 1;
+        return r;
+    }
     int32_t iP, iL, jP, jL, kP, kL;
     divrem_label(r.I, m.N[0], iP, iL);
     divrem_label(r.J, m.N[1], jP, jL);
@@ -108,36 +114,81 @@ __device__ __forceinline__ double ldexp2(double x, int k)
     return (x * st_pow2i(k1)) * st_pow2i(k2);
 }
 
-/* Quantises one deposit component; returns 0 for zero, non-finite or out-of-range values
- * (the latter two are counted in `ovf`).  Updates the running max exponent. */
-__device__ __forceinline__ long long quantize(double dv, int L, int cap, int& emax,
-                                              unsigned& ovf)
+/* largest finite |v| seen (probe pass) */
+template <class V>
+__device__ __forceinline__ void track_max(V v, double& amax)
 {
-    if (dv == 0.0) return 0;
-    if (!isfinite(dv)) {
-        ++ovf;
-        return 0;
-    }
-    int e = exp_of(dv);
-    emax = max(emax, e);
-    if (e - L > cap) {
-        ++ovf;
-        return 0;
-    }
-    return __double2ll_rn(ldexp2(dv, -L));
+    const double a = fabs((double)v);
+    if (a < __longlong_as_double(0x7ff0000000000000LL)) amax = fmax(amax, a);
 }
 
-template <int DEP>
-__device__ __forceinline__ void deposit_direct(const double dep[3], int64_t cell0,
-                                               unsigned long long* acc, double* src, int L,
-                                               int cap, int& emax, unsigned& ovf)
+/* Fixed-point parameters of one cloud for the current step: q = rint(dep * 2^-L), and a
+ * deposit with |dep| >= 2^(cap+L) (i.e. frexp exponent - L > cap) does not fit.  Single
+ * precision deposits are scaled in single precision when 2^-L and 2^(cap+L) are normal
+ * floats: scaling by a power of two is exact, so the integer is the same as through FP64. */
+struct Quant {
+    double scale;   /* 2^-L, or 0 when 2^-L is not a normal double (then ldexp2 is used) */
+    double thr;     /* 2^(cap+L) */
+    float scale_f;  /* 2^-L as float, when `fast` */
+    float thr_f;    /* 2^(cap+L) as float, when `fast` */
+    int L;
+    bool fast;
+};
+
+__device__ __forceinline__ Quant make_quant(int L, int cap)
+{
+    Quant q;
+    q.L = L;
+    q.scale = (-L >= -1022 && -L <= 1023) ? st_pow2i(-L) : 0.0;
+    q.thr = ldexp2(1.0, cap + L);
+    q.fast = (-L >= -126 && -L <= 127) && (cap + L >= -126 && cap + L <= 127);
+    q.scale_f = q.fast ? st_pow2if(-L) : 0.0f;
+    q.thr_f = q.fast ? st_pow2if(cap + L) : 0.0f;
+    return q;
+}
+
+/* Quantises one deposit component: 0 for zero, non-finite or out-of-range values (the
+ * latter two are counted in `ovf`).  `amax` tracks the largest finite |dep| for the next
+ * step's scale (max is order-independent, so the scale is reproducible). */
+__device__ __forceinline__ long long quantize(double dv, const Quant& qp, double& amax,
+                                              unsigned& ovf)
+{
+    const double a = fabs(dv);
+    if (a == 0.0) return 0;
+    if (a < __longlong_as_double(0x7ff0000000000000LL)) amax = fmax(amax, a);
+    if (!(a < qp.thr)) {
+        ++ovf;
+        return 0;
+    }
+    const double x = qp.scale != 0.0 ? dv * qp.scale : ldexp2(dv, -qp.L);
+    return __double2ll_rn(x);
+}
+
+__device__ __forceinline__ long long quantize(float dv, const Quant& qp, double& amax,
+                                              unsigned& ovf)
+{
+    if (!qp.fast) return quantize((double)dv, qp, amax, ovf);
+    const float a = fabsf(dv);
+    if (a == 0.0f) return 0;
+    if (a < __int_as_float(0x7f800000)) amax = fmax(amax, (double)a);
+    if (!(a < qp.thr_f)) {
+        ++ovf;
+        return 0;
+    }
+    return __float2ll_rn(dv * qp.scale_f);
+}
+
+template <int DEP, class V>
+__device__ __forceinline__ void deposit_direct(const V dep[3], int64_t cell0,
+                                               unsigned long long* acc, double* src,
+                                               const Quant& qp, double& amax, unsigned& ovf)
 {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         if (DEP == DEP_ATOMIC) {
-            if (dep[c] != 0.0) atomicAdd(src + 3 * cell0 + c, dep[c]);
+            if (dep[c] != (V)0) atomicAdd(src + 3 * cell0 + c, (double)dep[c]);
         } else {
-            long long q = quantize(dep[c], L, cap, emax, ovf);
+            long long q = quantize(dep[c], qp, amax, ovf);
             if (DEP == DEP_DET1) {
                 if (q) atomicAdd(acc + 3 * cell0 + c, (unsigned long long)q);
             } else if (DEP == DEP_DET2) {
@@ -151,12 +202,19 @@ __device__ __forceinline__ void deposit_direct(const double dep[3], int64_t cell
     }
 }
 
-/* Inclusive scan over the lane's run of equal keys (runs are contiguous lane ranges). */
+#ifndef ST_SCAN_STEPS
+#define ST_SCAN_STEPS 2
+#endif
+constexpr int SCAN_STEPS = ST_SCAN_STEPS;   /* 0..5 */
+constexpr int SPAN = 1 << SCAN_STEPS;        /* lanes summed per emitted chunk */
+
+/* Inclusive scan over the lane's run of equal keys, limited to SPAN lanes (runs are
+ * contiguous lane ranges). */
 template <class T>
 __device__ __forceinline__ T seg_scan(T v, int lane, int segstart)
 {
 #pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
+    for (int off = 1; off < SPAN; off <<= 1) {
         T t = __shfl_up_sync(FULL_MASK, v, off);
         if (lane - off >= segstart) v += t;
     }
@@ -166,6 +224,9 @@ __device__ __forceinline__ T seg_scan(T v, int lane, int segstart)
 /* ------------------------------------------------------------------------------------ */
 /* the step kernel                                                                      */
 /* ------------------------------------------------------------------------------------ */
+
+constexpr int TILE = WARP_TILE;      /* parcels per warp tile (CloudK::tile0 counts these) */
+constexpr int SLICES = TILE / 32;    /* 32-parcel slices per warp tile */
 
 template <class P, class V>
 __device__ __forceinline__ int find_cloud(const StepArgs<P, V>& a, int64_t tile)
@@ -184,233 +245,390 @@ __device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
 template <class T>
 __device__ __forceinline__ void st_stream(T* p, T v) { __stcs(p, v); }
 
+/* One parcel through all substeps (A:1271-1365) after its start cell has been located and
+ * the cell velocity gathered.  pos/vel are updated in place; the final deposit is returned
+ * in (key, dep) for the warp-level reduction; intermediate deposits on cell change
+ * (A:1342-1348, only with substeps > 1) go straight to memory. */
 template <class P, class V, int DEP>
-__global__ void __launch_bounds__(256) k_step(const StepArgs<P, V> a)
+__device__ __forceinline__ void evolve_parcel(const StepArgs<P, V>& a, P pos[3], V vel[3], V d,
+                                              int32_t posI, V uc[3], unsigned long long* acc,
+                                              double* src, const Quant& qp, double& amax,
+                                              unsigned& ovf, bool& lost, int32_t& key,
+                                              V dep[3])
 {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const MeshK<P>& mesh = a.mesh;
     const PhysK<V>& ph = a.phys;
     const P dtP = a.dtP;
-    const V dtV = a.dtV;
-    const V fs = a.fscale;
-
-    for (int64_t tile = warp0; tile < a.total_tiles; tile += nwarps) {
-        const int c = (a.nclouds == 1) ? 0 : find_cloud(a, tile);
-        const CloudK<P, V>* cl = a.clouds + c;
-        const int64_t n = __ldg(&cl->n);
-        const int64_t i = (tile - __ldg(&cl->tile0)) * 32 + lane;
-        const bool active = i < n;
-        CloudCtl* ctl = a.ctl + c;
-        const int L = (DEP == DEP_DET1 || DEP == DEP_DET2) ? ctl->L : 0;
-        const int cap = (DEP == DEP_DET1 || DEP == DEP_DET2) ? ctl->H + QUANT_GROWTH_BITS : 0;
-        unsigned long long* acc = (DEP == DEP_DET1 || DEP == DEP_DET2) ? cl->acc : nullptr;
-        double* src = (DEP == DEP_ATOMIC) ? cl->src : nullptr;
-
-        int emax = EXP_NONE;
-        unsigned ovf = 0;
-        bool lost = false;
-        int32_t key = -1;            /* 0-based cell of the final deposit */
-        double dep[3] = {0.0, 0.0, 0.0};
-
-        if (active) {
-            P pos[3], posNew[3];
-            V vel[3], velNew[3];
-            P* xp = cl->x;
-            P* yp = cl->y;
-            P* zp = cl->z;
-            V* up = cl->u;
-            V* vp = cl->v;
-            V* wp = cl->w;
-            pos[0] = ld_stream(xp + i);
-            pos[1] = ld_stream(yp + i);
-            pos[2] = ld_stream(zp + i);
-            vel[0] = ld_stream(up + i);
-            vel[1] = ld_stream(vp + i);
-            vel[2] = ld_stream(wp + i);
-            const V d = ld_stream(cl->d + i) * ph.dscale;
-            /* mᵈ/ρᶜ = ρᵈ/ρᶜ·π·⌀³/6 (A:1280) */
-            const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
-            /* drag factor 18 μ Δt/(ρᵈ ⌀²) (A:1294), times the drag multiplier */
-            const V f = ((((V)18 * ph.mu) * dtV) / (ph.rho_d * (d * d))) * ph.alpha;
-
-            bool bad = false;
-            LocK l0 = locate(mesh, pos[0], pos[1], pos[2], bad);         /* A:1286 */
-            if (bad || l0.part != 1) {
-                lost = true;
-            } else {
-                int32_t posI = l0.posI;
-                const V* Uc = a.U + 3 * (int64_t)(posI - 1);             /* A:1288 */
-                V uc[3] = {__ldg(Uc) * fs, __ldg(Uc + 1) * fs, __ldg(Uc + 2) * fs};
-                V state0[3] = {vel[0], vel[1], vel[2]};                 /* A:1289 */
-                for (int t = 1; t <= ph.nsub; ++t) {
-                    if (ph.drag == 0) {
+    /* mᵈ/ρᶜ = ρᵈ/ρᶜ·π·⌀³/6 (A:1280) */
+    const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
+    /* drag factor 18 μ Δt/(ρᵈ ⌀²) (A:1294), times the drag multiplier */
+    const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
+    P posNew[3] = {pos[0], pos[1], pos[2]};
+    V velNew[3] = {vel[0], vel[1], vel[2]};
+    V state0[3] = {vel[0], vel[1], vel[2]};                          /* A:1289 */
+    bool bad = false;
+    for (int t = 1; t <= ph.nsub; ++t) {                             /* A:1291 */
+        if (ph.drag == 0) {
 #pragma unroll
-                        for (int k = 0; k < 3; ++k)                      /* A:1295 */
-                            velNew[k] = (vel[k] + f * uc[k]) / ((V)1 + f);
-                    } else {
-                        V du[3];
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) du[k] = uc[k] - vel[k];
-                        V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
-                        V Re = (mag * d) / ph.nu;
-                        V pw;
-                        if (sizeof(V) == 4) pw = (V)st_pow0687f((float)Re);
-                        else pw = (V)st_pow0687((double)Re);
-                        V g = f * ((V)1 + (V)0.15 * pw);
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) velNew[k] = vel[k] + g * du[k];
-                    }
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (P)velNew[k] * dtP;  /* A:1296 */
-
-                    LocK ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);      /* A:1303 */
-                    if (bad) { lost = true; break; }
-                    if (ln.posI != posI || ln.part != 1) {                               /* A:1306 */
-                        const bool bx = (ln.I < 0) || (ln.I >= mesh.N[0]);
-                        const bool by = (ln.J < 0) || (ln.J >= mesh.N[1]);
-                        const bool bz = (ln.K < 0) || (ln.K >= mesh.N[2]);
-                        /* hold position, mirror the old velocity, state0 -= 2 vel (A:1313-1329) */
-                        if (bx) { posNew[0] = pos[0]; velNew[0] = -vel[0]; state0[0] -= (V)2 * vel[0]; }
-                        if (by) { posNew[1] = pos[1]; velNew[1] = -vel[1]; state0[1] -= (V)2 * vel[1]; }
-                        if (bz) { posNew[2] = pos[2]; velNew[2] = -vel[2]; state0[2] -= (V)2 * vel[2]; }
-                        if (bx || by || bz) {                                            /* A:1333-1335 */
-                            ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);
-                            if (bad) { lost = true; break; }
-                        }
-                        if (t != ph.nsub && ln.posI != posI) {                           /* A:1342-1348 */
-                            if (ln.part != 1 || ln.posI < 1 || ln.posI > mesh.nCells) {
-                                lost = true;
-                                break;
-                            }
-                            double di[3];
-#pragma unroll
-                            for (int k = 0; k < 3; ++k) di[k] = (double)(mB * (state0[k] - velNew[k]));
-                            if (DEP == DEP_PROBE) {
-#pragma unroll
-                                for (int k = 0; k < 3; ++k)
-                                    if (di[k] != 0.0 && isfinite(di[k])) emax = max(emax, exp_of(di[k]));
-                            } else {
-                                deposit_direct<DEP>(di, (int64_t)(posI - 1), acc, src, L, cap, emax, ovf);
-                            }
-#pragma unroll
-                            for (int k = 0; k < 3; ++k) state0[k] = velNew[k];
-                            const V* Un = a.U + 3 * (int64_t)(ln.posI - 1);
-                            uc[0] = __ldg(Un) * fs;
-                            uc[1] = __ldg(Un + 1) * fs;
-                            uc[2] = __ldg(Un + 2) * fs;
-                            posI = ln.posI;
-                        }
-                    }
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) { vel[k] = velNew[k]; pos[k] = posNew[k]; }
-                }
-                if (!lost) {
-                    if (DEP != DEP_PROBE) {                                             /* A:1355-1360 */
-                        st_stream(xp + i, posNew[0]);
-                        st_stream(yp + i, posNew[1]);
-                        st_stream(zp + i, posNew[2]);
-                        st_stream(up + i, velNew[0]);
-                        st_stream(vp + i, velNew[1]);
-                        st_stream(wp + i, velNew[2]);
-                    }
-                    key = posI - 1;                                                      /* A:1361 */
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) dep[k] = (double)(mB * (state0[k] - velNew[k]));
-                }
-            }
-        }
-
-        /* ---- final deposit: one per parcel into posI ---- */
-        if (DEP == DEP_PROBE) {
-            if (key >= 0) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    if (dep[k] != 0.0 && isfinite(dep[k])) emax = max(emax, exp_of(dep[k]));
-            }
-        } else if (DEP == DEP_ATOMIC) {
-            if (key >= 0) deposit_direct<DEP_ATOMIC>(dep, key, acc, src, L, cap, emax, ovf);
+            for (int k = 0; k < 3; ++k) velNew[k] = (vel[k] + f * uc[k]) / ((V)1 + f); /* A:1295 */
         } else {
-            long long q[3] = {0, 0, 0};
-            if (key >= 0) {
+            V du[3];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) q[k] = quantize(dep[k], L, cap, emax, ovf);
-            }
-            /* runs of equal cells among the 32 consecutive parcels of this tile */
-            const int prev = __shfl_up_sync(FULL_MASK, key, 1);
-            const bool head = (lane == 0) || (prev != key);
-            const unsigned heads = __ballot_sync(FULL_MASK, head);
-            const int segstart = 31 - __clz(heads & (FULL_MASK >> (31 - lane)));
-            const bool tail = (lane == 31) || ((heads >> (lane + 1)) & 1u);
-            if (DEP == DEP_DET1) {
+            for (int k = 0; k < 3; ++k) du[k] = uc[k] - vel[k];
+            V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
+            V Re = (mag * d) * ph.rnu;
+            V pw;
+            if (sizeof(V) == 4) pw = (V)st_pow0687f((float)Re);
+            else pw = (V)st_pow0687((double)Re);
+            V g = f * ((V)1 + (V)0.15 * pw);
 #pragma unroll
-                for (int k = 0; k < 3; ++k) q[k] = seg_scan(q[k], lane, segstart);
-                if (tail && key >= 0) {
-                    unsigned long long* p = acc + 3 * (int64_t)key;
-#pragma unroll
-                    for (int k = 0; k < 3; ++k)
-                        if (q[k]) atomicAdd(p + k, (unsigned long long)q[k]);
-                }
-            } else {
-                long long hi[3];
-                unsigned long long lo[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    hi[k] = seg_scan(q[k] >> 32, lane, segstart);
-                    lo[k] = seg_scan((unsigned long long)q[k] & 0xffffffffULL, lane, segstart);
-                }
-                if (tail && key >= 0) {
-                    unsigned long long* p = acc + 6 * (int64_t)key;
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        if (hi[k]) atomicAdd(p + 2 * k, (unsigned long long)hi[k]);
-                        if (lo[k]) atomicAdd(p + 2 * k + 1, lo[k]);
-                    }
-                }
-            }
+            for (int k = 0; k < 3; ++k) velNew[k] = vel[k] + g * du[k];
         }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (P)velNew[k] * dtP;  /* A:1296 */
 
-        /* ---- bookkeeping: scale tracker, lost parcels, range errors ---- */
-        if (DEP != DEP_ATOMIC) {
-            const int wmax = __reduce_max_sync(FULL_MASK, emax);
-            if (lane == 0 && wmax != EXP_NONE) atomicMax(&ctl->emax, wmax);
+        LocK ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);          /* A:1303 */
+        if (bad) { lost = true; return; }
+        if (ln.posI != posI || ln.part != 1) {                                   /* A:1306 */
+            const bool bx = (ln.I < 0) || (ln.I >= mesh.N[0]);
+            const bool by = (ln.J < 0) || (ln.J >= mesh.N[1]);
+            const bool bz = (ln.K < 0) || (ln.K >= mesh.N[2]);
+            /* hold position, mirror the old velocity, state0 -= 2 vel (A:1313-1329) */
+            if (bx) { posNew[0] = pos[0]; velNew[0] = -vel[0]; state0[0] -= (V)2 * vel[0]; }
+            if (by) { posNew[1] = pos[1]; velNew[1] = -vel[1]; state0[1] -= (V)2 * vel[1]; }
+            if (bz) { posNew[2] = pos[2]; velNew[2] = -vel[2]; state0[2] -= (V)2 * vel[2]; }
+            if (bx || by || bz) {                                                /* A:1333-1335 */
+                ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);
+                if (bad) { lost = true; return; }
+            }
+            if (t != ph.nsub && ln.posI != posI) {                               /* A:1342-1348 */
+                if (ln.part != 1 || ln.posI < 1 || ln.posI > mesh.nCells) { lost = true; return; }
+                V di[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) di[k] = mB * (state0[k] - velNew[k]);
+                if (DEP == DEP_PROBE) {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) track_max(di[k], amax);
+                } else {
+                    deposit_direct<DEP, V>(di, (int64_t)(posI - 1), acc, src, qp, amax, ovf);
+                }
+#pragma unroll
+                for (int k = 0; k < 3; ++k) state0[k] = velNew[k];
+                const V* Un = a.U + 3 * (int64_t)(ln.posI - 1);
+                uc[0] = __ldg(Un) * a.fscale;
+                uc[1] = __ldg(Un + 1) * a.fscale;
+                uc[2] = __ldg(Un + 2) * a.fscale;
+                posI = ln.posI;
+            }
         }
-        const unsigned nlost = __popc(__ballot_sync(FULL_MASK, lost));
-        const unsigned novf = __reduce_add_sync(FULL_MASK, ovf);
-        if (lane == 0) {
-            if (nlost) atomicAdd(&ctl->lost, (unsigned long long)nlost);
-            if (novf && DEP != DEP_PROBE) atomicAdd(&ctl->overflow, (unsigned long long)novf);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { vel[k] = velNew[k]; pos[k] = posNew[k]; }
+    }
+    key = posI - 1;                                                              /* A:1361 */
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dep[k] = mB * (state0[k] - velNew[k]);
+}
+
+/* One substep (the benchmark configurations): evolve_particle! (A:1271-1365) with
+ * nSteps = 1, where no intermediate deposit can happen and the final deposit goes to the
+ * start cell.  A new position inside the mesh cannot meet a wall, so the reference's
+ * relocation test (A:1303-1335) is only evaluated in full when the position left the index
+ * range of some axis. */
+template <class P, class V>
+__device__ __forceinline__ void evolve_one(const StepArgs<P, V>& a, P pos[3], V vel[3], V d,
+                                           int32_t posI, const V uc[3], bool& lost, V dep[3])
+{
+    const MeshK<P>& mesh = a.mesh;
+    const PhysK<V>& ph = a.phys;
+    const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;  /* A:1280 */
+    const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha; /* A:1294 */
+    V velNew[3];
+    if (ph.drag == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) velNew[k] = (vel[k] + f * uc[k]) / ((V)1 + f);  /* A:1295 */
+    } else {
+        V du[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) du[k] = uc[k] - vel[k];
+        V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
+        V Re = (mag * d) * ph.rnu;
+        V pw;
+        if (sizeof(V) == 4) pw = (V)st_pow0687f((float)Re);
+        else pw = (V)st_pow0687((double)Re);
+        V g = f * ((V)1 + (V)0.15 * pw);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) velNew[k] = vel[k] + g * du[k];
+    }
+    P posNew[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (P)velNew[k] * a.dtP;              /* A:1296 */
+    V state0[3] = {vel[0], vel[1], vel[2]};
+    bool bad = false;
+    const int32_t I = floor_label((posNew[0] - mesh.origin[0]) * mesh.rD[0], bad);
+    const int32_t J = floor_label((posNew[1] - mesh.origin[1]) * mesh.rD[1], bad);
+    const int32_t K = floor_label((posNew[2] - mesh.origin[2]) * mesh.rD[2], bad);
+    if (bad) { lost = true; return; }
+    if (!((uint32_t)I < (uint32_t)mesh.N[0] && (uint32_t)J < (uint32_t)mesh.N[1] &&
+          (uint32_t)K < (uint32_t)mesh.N[2])) {
+        LocK ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);                  /* A:1303 */
+        if (ln.posI != posI || ln.part != 1) {                                          /* A:1306 */
+            const bool bx = (ln.I < 0) || (ln.I >= mesh.N[0]);
+            const bool by = (ln.J < 0) || (ln.J >= mesh.N[1]);
+            const bool bz = (ln.K < 0) || (ln.K >= mesh.N[2]);
+            if (bx) { posNew[0] = pos[0]; velNew[0] = -vel[0]; state0[0] -= (V)2 * vel[0]; }
+            if (by) { posNew[1] = pos[1]; velNew[1] = -vel[1]; state0[1] -= (V)2 * vel[1]; }
+            if (bz) { posNew[2] = pos[2]; velNew[2] = -vel[2]; state0[2] -= (V)2 * vel[2]; }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        pos[k] = posNew[k];
+        vel[k] = velNew[k];
+        dep[k] = mB * (state0[k] - velNew[k]);                                          /* A:1361 */
+    }
+}
+
+/* Final deposits of 32 consecutive parcels (one per lane, key < 0 = none): runs of equal
+ * cells are summed with a segmented warp scan and the last lane of each run adds the sum. */
+template <int DEP, class V>
+__device__ __forceinline__ void deposit_warp(int32_t key, const V dep[3],
+                                             unsigned long long* acc, double* src,
+                                             const Quant& qp, int lane, double& amax,
+                                             unsigned& ovf)
+{
+    if (DEP == DEP_PROBE) {
+        if (key >= 0) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) track_max(dep[k], amax);
+        }
+        return;
+    }
+    if (DEP == DEP_ATOMIC) {
+        if (key >= 0) deposit_direct<DEP_ATOMIC, V>(dep, key, acc, src, qp, amax, ovf);
+        return;
+    }
+    long long q[3] = {0, 0, 0};
+    if (key >= 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) q[k] = quantize(dep[k], qp, amax, ovf);
+    }
+    const int prev = __shfl_up_sync(FULL_MASK, key, 1);
+    const bool head = (lane == 0) || (prev != key);
+    const unsigned heads = __ballot_sync(FULL_MASK, head);
+    const int segstart = 31 - __clz(heads & (FULL_MASK >> (31 - lane)));
+    const bool tail = (lane == 31) || ((heads >> (lane + 1)) & 1u);
+    /* A scan of SCAN_STEPS steps sums runs in chunks of SPAN lanes: lane j holds the sum of
+     * [max(run start, j - SPAN + 1), j]; the run's last lane and every SPAN-th lane before it
+     * add their chunk, which covers the run exactly once. */
+    const unsigned tails = __ballot_sync(FULL_MASK, tail);
+    const int tailpos = lane + __ffs(tails >> lane) - 1;
+    const bool emit = ((tailpos - lane) & (SPAN - 1)) == 0;
+    if (DEP == DEP_DET1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) q[k] = seg_scan(q[k], lane, segstart);
+        if (emit && key >= 0) {
+            unsigned long long* p = acc + 3 * (int64_t)key;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                if (q[k]) atomicAdd(p + k, (unsigned long long)q[k]);
+        }
+    } else {
+        long long hi[3];
+        unsigned long long lo[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            hi[k] = seg_scan(q[k] >> 32, lane, segstart);
+            lo[k] = seg_scan((unsigned long long)q[k] & 0xffffffffULL, lane, segstart);
+        }
+        if (emit && key >= 0) {
+            unsigned long long* p = acc + 6 * (int64_t)key;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (hi[k]) atomicAdd(p + 2 * k, (unsigned long long)hi[k]);
+                if (lo[k]) atomicAdd(p + 2 * k + 1, lo[k]);
+            }
         }
     }
 }
 
-template <class P, class V>
-cudaError_t launch_step(const StepArgs<P, V>& a, int dep, int grid, int block, cudaStream_t s)
+/* Warp-aggregated bookkeeping for one cloud: largest deposit exponent, lost parcels and
+ * range errors.  Called when a warp moves on to another cloud and at the end. */
+template <int DEP>
+__device__ __forceinline__ void flush_ctl(CloudCtl* ctl, int lane, double& amax, unsigned& ovf,
+                                          unsigned& lost)
+{
+    if (DEP != DEP_ATOMIC) {
+        const int e = amax > 0.0 ? exp_of(amax) : EXP_NONE;
+        const int wmax = __reduce_max_sync(FULL_MASK, e);
+        if (lane == 0 && wmax != EXP_NONE) atomicMax(&ctl->emax, wmax);
+    }
+    const unsigned nlost = __reduce_add_sync(FULL_MASK, lost);
+    const unsigned novf = __reduce_add_sync(FULL_MASK, ovf);
+    if (lane == 0) {
+        if (nlost) atomicAdd(&ctl->lost, (unsigned long long)nlost);
+        if (novf && DEP != DEP_PROBE) atomicAdd(&ctl->overflow, (unsigned long long)novf);
+    }
+    amax = 0.0;
+    ovf = 0;
+    lost = 0;
+}
+
+/* The step kernel.  A warp owns a tile of SLICES x 32 consecutive parcels (lane l holds
+ * parcels l, l+32, l+64, l+96 of the tile): all loads of the tile are issued first, then the
+ * start cells are located and the cell velocities gathered for every slice, then each slice
+ * is stepped, stored and its deposits reduced.  Tiles are distributed over the persistent
+ * grid with a fixed stride; the clouds of a multi-cloud launch occupy consecutive tile
+ * ranges. */
+#ifndef ST_MIN_BLOCKS
+#define ST_MIN_BLOCKS 4
+#endif
+template <class P, class V, int DEP, bool ONE>
+__global__ void __launch_bounds__(256, ST_MIN_BLOCKS) k_step(const StepArgs<P, V> a)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    constexpr bool DET = (DEP == DEP_DET1 || DEP == DEP_DET2);
+
+    int cur = -1;
+    Quant qp = {0.0, 0.0, 0};
+    double amax = 0.0;
+    unsigned ovf = 0, nlost = 0;
+
+    for (int64_t tile = warp0; tile < a.total_tiles; tile += nwarps) {
+        const int c = (a.nclouds == 1) ? 0 : find_cloud(a, tile);
+        if (c != cur) {
+            if (cur >= 0) flush_ctl<DEP>(a.ctl + cur, lane, amax, ovf, nlost);
+            cur = c;
+            if (DET) qp = make_quant(a.ctl[c].L, a.ctl[c].H + QUANT_GROWTH_BITS);
+        }
+        const CloudK<P, V>* cl = a.clouds + c;
+        const int64_t n = __ldg(&cl->n);
+        const int64_t base = (tile - __ldg(&cl->tile0)) * TILE + lane;
+        P* const xp = cl->x;
+        P* const yp = cl->y;
+        P* const zp = cl->z;
+        V* const up = cl->u;
+        V* const vp = cl->v;
+        V* const wp = cl->w;
+        const V* const dp = cl->d;
+        unsigned long long* const acc = DET ? cl->acc : nullptr;
+        double* const src = (DEP == DEP_ATOMIC) ? cl->src : nullptr;
+
+        /* phase 1: every load of the tile in flight at once (streaming, evict-first) */
+        P X[SLICES], Y[SLICES], Z[SLICES];
+        V Uv[SLICES], Vv[SLICES], Wv[SLICES], D[SLICES];
+#pragma unroll
+        for (int s = 0; s < SLICES; ++s) {
+            const int64_t i = base + 32 * s;
+            if (i < n) {
+                X[s] = ld_stream(xp + i);
+                Y[s] = ld_stream(yp + i);
+                Z[s] = ld_stream(zp + i);
+                Uv[s] = ld_stream(up + i);
+                Vv[s] = ld_stream(vp + i);
+                Wv[s] = ld_stream(wp + i);
+                D[s] = ld_stream(dp + i);
+            }
+        }
+        /* phase 2: start cells (A:1286) and cell velocities (A:1288) */
+        int32_t pI[SLICES];
+        V uc[SLICES][3];
+#pragma unroll
+        for (int s = 0; s < SLICES; ++s) {
+            pI[s] = 0;
+            if (base + 32 * s < n) {
+                bool bad = false;
+                LocK l0 = locate(a.mesh, X[s], Y[s], Z[s], bad);
+                if (!bad && l0.part == 1) {
+                    pI[s] = l0.posI;
+                    const V* Uc = a.U + 3 * (int64_t)(l0.posI - 1);
+                    uc[s][0] = __ldg(Uc) * a.fscale;
+                    uc[s][1] = __ldg(Uc + 1) * a.fscale;
+                    uc[s][2] = __ldg(Uc + 2) * a.fscale;
+                } else {
+                    ++nlost;
+                }
+            }
+        }
+        /* phase 3: substeps, store, deposit, one slice after the other */
+#pragma unroll
+        for (int s = 0; s < SLICES; ++s) {
+            const int64_t i = base + 32 * s;
+            int32_t key = -1;
+            V dep[3] = {(V)0, (V)0, (V)0};
+            if (pI[s] > 0) {
+                P pos[3] = {X[s], Y[s], Z[s]};
+                V vel[3] = {Uv[s], Vv[s], Wv[s]};
+                bool lost = false;
+                if (ONE) {
+                    evolve_one<P, V>(a, pos, vel, D[s] * a.phys.dscale, pI[s], uc[s], lost, dep);
+                    key = pI[s] - 1;
+                } else {
+                    evolve_parcel<P, V, DEP>(a, pos, vel, D[s] * a.phys.dscale, pI[s], uc[s],
+                                             acc, src, qp, amax, ovf, lost, key, dep);
+                }
+                if (lost) {
+                    ++nlost;
+                    key = -1;
+                } else if (DEP != DEP_PROBE) {                                   /* A:1355-1360 */
+                    st_stream(xp + i, pos[0]);
+                    st_stream(yp + i, pos[1]);
+                    st_stream(zp + i, pos[2]);
+                    st_stream(up + i, vel[0]);
+                    st_stream(vp + i, vel[1]);
+                    st_stream(wp + i, vel[2]);
+                }
+            }
+            deposit_warp<DEP, V>(key, dep, acc, src, qp, lane, amax, ovf);
+        }
+    }
+    if (cur >= 0) flush_ctl<DEP>(a.ctl + cur, lane, amax, ovf, nlost);
+}
+
+template <class P, class V, bool ONE>
+static cudaError_t launch_step_t(const StepArgs<P, V>& a, int dep, int grid, int block,
+                                 cudaStream_t s)
 {
     switch (dep) {
-    case DEP_DET1: k_step<P, V, DEP_DET1><<<grid, block, 0, s>>>(a); break;
-    case DEP_DET2: k_step<P, V, DEP_DET2><<<grid, block, 0, s>>>(a); break;
-    case DEP_ATOMIC: k_step<P, V, DEP_ATOMIC><<<grid, block, 0, s>>>(a); break;
-    case DEP_PROBE: k_step<P, V, DEP_PROBE><<<grid, block, 0, s>>>(a); break;
+    case DEP_DET1: k_step<P, V, DEP_DET1, ONE><<<grid, block, 0, s>>>(a); break;
+    case DEP_DET2: k_step<P, V, DEP_DET2, ONE><<<grid, block, 0, s>>>(a); break;
+    case DEP_ATOMIC: k_step<P, V, DEP_ATOMIC, ONE><<<grid, block, 0, s>>>(a); break;
+    case DEP_PROBE: k_step<P, V, DEP_PROBE, ONE><<<grid, block, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
 template <class P, class V>
-int step_max_active_blocks(int dep, int block)
+cudaError_t launch_step(const StepArgs<P, V>& a, int dep, int grid, int block, cudaStream_t s)
+{
+    return a.phys.nsub == 1 ? launch_step_t<P, V, true>(a, dep, grid, block, s)
+                            : launch_step_t<P, V, false>(a, dep, grid, block, s);
+}
+
+template <class P, class V, bool ONE>
+static int max_active_t(int dep, int block)
 {
     int nb = 0;
     cudaError_t e = cudaErrorInvalidValue;
     switch (dep) {
-    case DEP_DET1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_DET1>, block, 0); break;
-    case DEP_DET2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_DET2>, block, 0); break;
-    case DEP_ATOMIC: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_ATOMIC>, block, 0); break;
-    case DEP_PROBE: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_PROBE>, block, 0); break;
+    case DEP_DET1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_DET1, ONE>, block, 0); break;
+    case DEP_DET2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_DET2, ONE>, block, 0); break;
+    case DEP_ATOMIC: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_ATOMIC, ONE>, block, 0); break;
+    case DEP_PROBE: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_PROBE, ONE>, block, 0); break;
     default: break;
     }
     return e == cudaSuccess ? nb : 0;
+}
+
+template <class P, class V>
+int step_max_active_blocks(int dep, int block)
+{
+    /* both variants are compiled with the same launch bounds; take the smaller */
+    int a = max_active_t<P, V, true>(dep, block);
+    int b = max_active_t<P, V, false>(dep, block);
+    return a < b ? a : b;
 }
 
 template cudaError_t launch_step<float, float>(const StepArgs<float, float>&, int, int, int, cudaStream_t);
@@ -428,28 +646,42 @@ template <int LIMBS>
 __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict__ acc,
                                                   double* __restrict__ src, CloudCtl* ctl,
                                                   unsigned int* counter, int nclouds,
-                                                  int64_t ncomp)
+                                                  int64_t stride)
 {
+    /* stride: per-cloud component count, a multiple of 4 (padding stays zero).  The caller
+     * clears the accumulators after this kernel. */
     const int c = blockIdx.y;
     const int L = ctl[c].L;
-    unsigned long long* a = acc + (int64_t)c * ncomp * LIMBS;
-    double* s = src + (int64_t)c * ncomp;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < ncomp; j += stride) {
-        double v;
+    const ulonglong2* a = reinterpret_cast<const ulonglong2*>(acc + (int64_t)c * stride * LIMBS);
+    double2* s = reinterpret_cast<double2*>(src + (int64_t)c * stride);
+    const int64_t ngroups = stride / 4;
+    const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+    /* read-only pass: the accumulators are cleared afterwards by a memset, which costs less
+     * than writing zeros back into the lines just read; the source is streamed out */
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gstride) {
+        double v[4];
         if (LIMBS == 1) {
-            v = (double)(long long)a[j];
-            a[j] = 0ULL;
+            ulonglong2 q0 = __ldcs(a + 2 * g);
+            ulonglong2 q1 = __ldcs(a + 2 * g + 1);
+            v[0] = (double)(long long)q0.x;
+            v[1] = (double)(long long)q0.y;
+            v[2] = (double)(long long)q1.x;
+            v[3] = (double)(long long)q1.y;
         } else {
-            long long hi = (long long)a[2 * j];
-            unsigned long long lo = a[2 * j + 1];
-            hi += (long long)(lo >> 32);
-            lo &= 0xffffffffULL;
-            v = (double)hi * 4294967296.0 + (double)lo;
-            a[2 * j] = 0ULL;
-            a[2 * j + 1] = 0ULL;
+            ulonglong2 q[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) q[k] = __ldcs(a + 4 * g + k);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                long long hi = (long long)q[k].x;
+                unsigned long long lo = q[k].y;
+                hi += (long long)(lo >> 32);
+                lo &= 0xffffffffULL;
+                v[k] = (double)hi * 4294967296.0 + (double)lo;
+            }
         }
-        __stcs(s + j, ldexp2(v, L));
+        __stcs(s + 2 * g, make_double2(ldexp2(v[0], L), ldexp2(v[1], L)));
+        __stcs(s + 2 * g + 1, make_double2(ldexp2(v[2], L), ldexp2(v[3], L)));
     }
     /* the last block to finish moves every cloud to the scale of its largest deposit */
     __syncthreads();
@@ -471,12 +703,13 @@ __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict
 }
 
 cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, CloudCtl* ctl,
-                            unsigned int* counter, int nclouds, int64_t ncomp, int grid_x,
+                            unsigned int* counter, int nclouds, int64_t stride, int grid_x,
                             cudaStream_t s)
 {
+    if (stride % 4) return cudaErrorInvalidValue;
     dim3 grid(grid_x, nclouds);
-    if (limbs == 1) k_finalize<1><<<grid, 256, 0, s>>>(acc, src, ctl, counter, nclouds, ncomp);
-    else k_finalize<2><<<grid, 256, 0, s>>>(acc, src, ctl, counter, nclouds, ncomp);
+    if (limbs == 1) k_finalize<1><<<grid, 256, 0, s>>>(acc, src, ctl, counter, nclouds, stride);
+    else k_finalize<2><<<grid, 256, 0, s>>>(acc, src, ctl, counter, nclouds, stride);
     return cudaGetLastError();
 }
 
@@ -499,9 +732,11 @@ cudaError_t launch_set_scale(CloudCtl* ctl, int nclouds, cudaStream_t s)
 
 __global__ void k_zero_f64(double* p, int64_t n)
 {
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+    /* n is a multiple of 2 and p 16-byte aligned (padded per-cloud strides) */
+    double2* q = reinterpret_cast<double2*>(p);
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n / 2;
          j += (int64_t)gridDim.x * blockDim.x)
-        p[j] = 0.0;
+        q[j] = make_double2(0.0, 0.0);
 }
 
 cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s)

@@ -16,9 +16,10 @@
  *          remainder < 1e-18 relative).  See Abramowitz & Stegun 4.1.28 (ln((1+s)/(1-s))).
  *   exp y: Cody & Waite (1980) reduction y = k ln2 + r, |r| <= ln2/2, e^r by its Taylor series
  *          to r^14/14! (remainder < 5e-18), result scaled by 2^k through the exponent field.
- * Accuracy: a few ulp in double, far below what the drag model needs; the point is that host
- * and device produce the same bits.  Checked against libm pow by the CPU tests and host vs
- * device bit-equality by the GPU tests.
+ * Accuracy: a few ulp in double (st_pow0687) and 1 ulp in single (st_pow0687f), far below
+ * what the drag model needs; the point is that host and device produce the same bits.
+ * Checked against libm pow by the CPU tests and host vs device bit-equality by the GPU
+ * tests.
  */
 #ifndef ST_POW_H
 #define ST_POW_H
@@ -133,10 +134,83 @@ ST_HD double st_pow0687(double x)
     return st_exp_small(0.687 * st_log_pos(x));
 }
 
-/* Single-precision entry used by the mixed and FP32 paths: evaluate in double, round once. */
+ST_HD uint32_t st_bits_of_f(float x)
+{
+#if defined(__CUDA_ARCH__)
+    return (uint32_t)__float_as_uint(x);
+#else
+    uint32_t b;
+    memcpy(&b, &x, sizeof b);
+    return b;
+#endif
+}
+
+ST_HD float st_float_of(uint32_t b)
+{
+#if defined(__CUDA_ARCH__)
+    return __uint_as_float(b);
+#else
+    float x;
+    memcpy(&x, &b, sizeof x);
+    return x;
+#endif
+}
+
+/* 2^k for -126 <= k <= 127 (exact) */
+ST_HD float st_pow2if(int k)
+{
+    return st_float_of((uint32_t)(k + 127) << 23);
+}
+
+/* x^0.687 for the FP32 and mixed drag (the drag is evaluated in FP32).  Same method as
+ * st_pow0687 with float-sized series: ln m = 2s(1 + z/3 + ... + z^4/9) in float (remainder
+ * < 3e-9), e^r to r^7/7! in float (remainder < 6e-9).  The exponent bookkeeping
+ * y = 0.687 (e ln 2 + ln m) and the reduction r = y - k ln 2 are done in double: in float
+ * their rounding would cost |y| ulp of the result.  At most 1 ulp from the correctly
+ * rounded value over the physical range (the CPU tests check this against libm). */
 ST_HD float st_pow0687f(float x)
 {
-    return (float)st_pow0687((double)x);
+    const double LN2 = 0.69314718055994530942;
+    const double INV_LN2 = 1.44269504088896340736;
+    const float SQRT2 = 1.4142135f;
+    if (!(x > 0.0f)) return x != x ? x : 0.0f;
+    if (x > 3.0e38f) return x;
+    int e = 0;
+    uint32_t b = st_bits_of_f(x);
+    if ((b >> 23) == 0) {                          /* subnormal */
+        x = x * 16777216.0f;                       /* 2^24, exact */
+        e = -24;
+        b = st_bits_of_f(x);
+    }
+    e += (int)((b >> 23) & 0xff) - 127;
+    float m = st_float_of((b & 0x007fffffu) | 0x3f800000u); /* [1,2) */
+    if (m > SQRT2) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    float s = (m - 1.0f) / (m + 1.0f);
+    float z = s * s;
+    float p = 1.0f / 9.0f;
+    p = p * z + 1.0f / 7.0f;
+    p = p * z + 1.0f / 5.0f;
+    p = p * z + 1.0f / 3.0f;
+    p = p * z + 1.0f;
+    float lnm = (2.0f * s) * p;
+    double y = 0.687 * ((double)e * LN2 + (double)lnm);
+    double t = y * INV_LN2;
+    int k = (int)(t >= 0.0 ? t + 0.5 : t - 0.5);
+    float r = (float)(y - (double)k * LN2);
+    float q = 1.0f / 5040.0f;
+    q = q * r + 1.0f / 720.0f;
+    q = q * r + 1.0f / 120.0f;
+    q = q * r + 1.0f / 24.0f;
+    q = q * r + 1.0f / 6.0f;
+    q = q * r + 0.5f;
+    q = q * r + 1.0f;
+    q = q * r + 1.0f;
+    int k1 = k / 2;
+    int k2 = k - k1;
+    return (q * st_pow2if(k1)) * st_pow2if(k2);
 }
 
 #endif /* ST_POW_H */

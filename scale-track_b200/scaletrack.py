@@ -15,7 +15,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libscaletrack.so")
+LIB_PATH = os.environ.get("SCALETRACK_LIB") or os.path.join(HERE, "libscaletrack.so")
 
 ST_OK = 0
 ST_ERR_INVALID_ARGUMENT = 1

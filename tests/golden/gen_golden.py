@@ -13,8 +13,8 @@ Reference file (A:): run/icoJuliaParcelFoam/cavity3D/asyncParallelTracking.jl
   Mesh construction (Float64 -> Float32) ..... A:237-268
 
 The Schiller-Naumann drag is project-defined (the reference only has Stokes drag); its
-power function follows the same textbook algorithm as scale-track_b200/csrc/st_pow.h,
-restated here in Python floats.
+power functions follow the same textbook algorithms as scale-track_b200/csrc/st_pow.h,
+restated here in Python floats (double) and numpy float32 scalars (single).
 
 Run:  python tests/golden/gen_golden.py      (rewrites the .npz files next to this script)
 """
@@ -90,6 +90,57 @@ def pow0687(x):
     return _exp_small(0.687 * _log_pos(x))
 
 
+def _fbits(x):
+    return int(np.array([x], dtype=np.float32).view(np.uint32)[0])
+
+
+def _ffrom(b):
+    return np.array([b], dtype=np.uint32).view(np.float32)[0]
+
+
+def pow0687f(x):
+    """Single-precision x^0.687 (same algorithm as st_pow0687f): float series, double
+    exponent bookkeeping; numpy float32 scalars and Python floats."""
+    x = F(x)
+    if not (x > F(0)):
+        return x if x != x else F(0)
+    if x > F(3.0e38):
+        return x
+    LN2 = 0.69314718055994530942
+    INV_LN2 = 1.44269504088896340736
+    e = 0
+    b = _fbits(x)
+    if (b >> 23) == 0:
+        x = F(x * F(16777216.0))
+        e = -24
+        b = _fbits(x)
+    e += ((b >> 23) & 0xFF) - 127
+    m = _ffrom((b & 0x007FFFFF) | 0x3F800000)
+    if m > F(1.4142135):
+        m = F(m * F(0.5))
+        e += 1
+    s = F(F(m - F(1)) / F(m + F(1)))
+    z = F(s * s)
+    p = F(F(1) / F(9))
+    for c in (7.0, 5.0, 3.0):
+        p = F(F(p * z) + F(F(1) / F(c)))
+    p = F(F(p * z) + F(1))
+    lnm = F(F(F(2) * s) * p)
+    y = 0.687 * (float(e) * LN2 + float(lnm))
+    t = y * INV_LN2
+    k = int(t + 0.5) if t >= 0.0 else -int(-t + 0.5)
+    r = F(y - float(k) * LN2)
+    q = F(F(1) / F(5040))
+    for c in (720.0, 120.0, 24.0, 6.0):
+        q = F(F(q * r) + F(F(1) / F(c)))
+    q = F(F(q * r) + F(0.5))
+    q = F(F(q * r) + F(1))
+    q = F(F(q * r) + F(1))
+    k1 = int(k / 2)
+    k2 = k - k1
+    return F(F(q * _ffrom((k1 + 127) << 23)) * _ffrom((k2 + 127) << 23))
+
+
 # ----------------------------------------------------------------------------- the step
 class Mesh:
     """construct_mesh (A:237-268) with decomposition (1,1,1)."""
@@ -130,7 +181,7 @@ def locate(m, x, y, z):
 
 
 def evolve_particle(m, prm, X, Y, Z, U, V, W, dIn, Ucell, fs, dt, nsteps, UTrans32, UTrans64):
-    mu, rho_d, rr, nu, drag = prm["mu"], prm["rho_d"], prm["rr"], prm["nu"], prm["drag"]
+    mu, rho_d, rr, rnu, drag = prm["mu"], prm["rho_d"], prm["rr"], prm["rnu"], prm["drag"]
     d = F(dIn * F(1.0))
     mB = F(F(F(rr * F(math.pi)) * F(F(d * d) * d)) / F(6))
     pos = [X, Y, Z]
@@ -156,8 +207,8 @@ def evolve_particle(m, prm, X, Y, Z, U, V, W, dIn, Ucell, fs, dt, nsteps, UTrans
         else:
             du = [F(uc[c] - vel[c]) for c in range(3)]
             mag = F(np.sqrt(F(F(F(du[0] * du[0]) + F(du[1] * du[1])) + F(du[2] * du[2]))))
-            Re = F(F(mag * d) / nu)
-            pw = F(pow0687(float(Re)))
+            Re = F(F(mag * d) * rnu)
+            pw = pow0687f(Re)
             g = F(f * F(F(1) + F(F(0.15) * pw)))
             for c in range(3):
                 velNew[c] = F(vel[c] + F(g * du[c]))
@@ -186,7 +237,7 @@ def evolve_particle(m, prm, X, Y, Z, U, V, W, dIn, Ucell, fs, dt, nsteps, UTrans
 
 def run_case(n, origin, ending, mu_c, rho_c, rho_d, drag, nsub, xyz, uvw, d, Ucell, dt, nsteps):
     m = Mesh(n, origin, ending)
-    prm = dict(mu=F(mu_c), rho_d=F(rho_d), rr=F(rho_d / rho_c), nu=F(mu_c / rho_c), drag=drag)
+    prm = dict(mu=F(mu_c), rho_d=F(rho_d), rr=F(rho_d / rho_c), rnu=F(rho_c / mu_c), drag=drag)
     npcl = d.shape[0]
     X = [F(v) for v in xyz[0]]
     Y = [F(v) for v in xyz[1]]
