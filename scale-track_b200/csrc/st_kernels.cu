@@ -479,11 +479,21 @@ __device__ __forceinline__ void flush_ctl(CloudCtl* ctl, int lane, double& amax,
  * is stepped, stored and its deposits reduced.  Tiles are distributed over the persistent
  * grid with a fixed stride; the clouds of a multi-cloud launch occupy consecutive tile
  * ranges. */
+/* Resident blocks of 256 threads per SM the compiler must allow (a register budget):
+ * 4 (64 registers) for FP32 velocities, 3 (80 registers) for FP64, whose state is wider. */
 #ifndef ST_MIN_BLOCKS
 #define ST_MIN_BLOCKS 4
 #endif
+#ifndef ST_MIN_BLOCKS_FP64
+#define ST_MIN_BLOCKS_FP64 3
+#endif
+template <class V>
+struct MinBlocks {
+    static constexpr int value = sizeof(V) == 8 ? ST_MIN_BLOCKS_FP64 : ST_MIN_BLOCKS;
+};
+
 template <class P, class V, int DEP, bool ONE>
-__global__ void __launch_bounds__(256, ST_MIN_BLOCKS) k_step(const StepArgs<P, V> a)
+__global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArgs<P, V> a)
 {
     const int lane = threadIdx.x & 31;
     const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
