@@ -167,6 +167,34 @@ ST_API int st_evolve_cloud(double dt);
  * the caller's fields first). */
 ST_API int st_finalize(void);
 
+/* ---- allocation-free step (no counterpart in the reference) ------------------------- */
+/* Largest mesh (cells) that st_step_noalloc accepts: the size of its fixed device scratch
+ * array, 3 x 8 bytes per cell (6 MiB), which every GPU that loads the library holds until
+ * the process exits. */
+#define ST_NOALLOC_MAX_CELLS 262144
+/* One call of the mixed-precision parcel step (ST_PREC_MIXED, deterministic deposit, one
+ * cloud, Morton re-sort not applied) for callers that cannot allocate device memory: a
+ * host that hands all device memory to its own pool, or a plugin that must not grow the
+ * process's device footprint after set-up.  Every array is caller-owned device memory:
+ * positions x,y,z (double[n]), velocities u,v,w and diameters d (float[n]), cell velocity
+ * U (float[nCells][3]) and the output source (double[nCells][3]); the parcel state is
+ * updated in place.  The only scratch (fixed-point accumulator and control block) is a
+ * fixed-size device array inside the library; no cudaMalloc, cudaFree or allocating
+ * library routine is called.  Meshes above ST_NOALLOC_MAX_CELLS cells are rejected with
+ * ST_ERR_INVALID_ARGUMENT.  Runs on the current device and `stream` (a cudaStream_t, NULL
+ * for the default stream) and returns after the stream has finished, with device-side
+ * errors reported.  The first call on a device looks up the scratch array's address: make
+ * it before any stream capture.  All calls share the one array: calls that overlap on the
+ * GPU race.  Each call chooses its fixed-point scale from its own deposits, so the source
+ * agrees with st_step's to the fixed-point resolution and positions and velocities are
+ * bit-identical. */
+ST_API int st_step_noalloc(const st_params* p, const st_mesh_desc* mesh, int64_t n, double* x,
+                           double* y, double* z, float* u, float* v, float* w, const float* d,
+                           const float* U, double* source, double dt, double fluid_scale,
+                           void* stream);
+/* ST_NOALLOC_MAX_CELLS, for callers that bind the library at run time. */
+ST_API int64_t st_noalloc_max_cells(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,6 +48,8 @@ static int fail(int code, const char* fmt, ...)
     return code;
 }
 
+void st::st_set_last_error(const char* msg) { g_err = msg ? msg : ""; }
+
 #define CK(...)                                                                             \
     do {                                                                                    \
         cudaError_t e_ = (__VA_ARGS__);                                                     \

@@ -90,6 +90,9 @@ struct StepArgs {
     int64_t total_tiles;        /* warp tiles (32 parcels) over all clouds */
 };
 
+/* Sets the thread-local message returned by st_last_error (st_abi.cu). */
+void st_set_last_error(const char* msg);
+
 /* Launchers implemented in st_kernels.cu (all asynchronous on `s`). */
 template <class P, class V>
 cudaError_t launch_step(const StepArgs<P, V>& a, int dep, int grid, int block, cudaStream_t s);

@@ -37,7 +37,8 @@ EXPORTS = [
     "st_set_fluid_velocity", "st_set_fluid_velocity_device", "st_step", "st_get_source",
     "st_source_device", "st_synchronize", "st_get_stream", "st_set_stream",
     "st_profile_enable", "st_profile_read", "st_launch_count", "st_setup", "st_default_handle",
-    "st_allocate_array", "st_evolve_cloud", "st_finalize",
+    "st_allocate_array", "st_evolve_cloud", "st_finalize", "st_step_noalloc",
+    "st_noalloc_max_cells",
 ]
 
 
@@ -107,6 +108,9 @@ def lib():
                               ctypes.c_void_p),
         "st_evolve_cloud": ([ctypes.c_double], ctypes.c_int),
         "st_finalize": ([], ctypes.c_int),
+        "st_step_noalloc": ([P(Params), P(MeshDesc), ctypes.c_int64] + [ctypes.c_void_p] * 9 +
+                            [ctypes.c_double, ctypes.c_double, ctypes.c_void_p], ctypes.c_int),
+        "st_noalloc_max_cells": ([], ctypes.c_int64),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
