@@ -72,7 +72,7 @@ def dist_env():
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -105,25 +105,42 @@ class ClockSampler:
                 self.proc.kill()
             self.f.close()
 
-    def summary(self):
+    def summary(self, t0=None, t1=None):
+        """Median SM clock and active throttle reasons of the samples taken in [t0, t1]
+        (wall-clock seconds); the nearest samples when the region is shorter than the
+        200 ms sampling period."""
         if not self.path or not os.path.exists(self.path):
             return None
+        import datetime
         rows = []
         with open(self.path) as f:
             for line in f:
                 parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
+                if len(parts) < 10:
+                    continue
+                try:
+                    ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except ValueError:
+                    continue
+                rows.append((ts, parts[1:]))
         os.unlink(self.path)
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        window = "timed region"
+        sel = rows
+        if t0 is not None and t1 is not None:
+            sel = [r for r in rows if t0 - 0.1 <= r[0] <= t1 + 0.1]
+            if not sel:
+                mid = 0.5 * (t0 + t1)
+                sel = sorted(rows, key=lambda r: abs(r[0] - mid))[:2]
+                window = "nearest samples (region shorter than the sampling period)"
+        sm = [float(r[1][1]) for r in sel if r[1][1].replace(".", "").isdigit()]
+        smax = [float(r[1][2]) for r in sel if r[1][2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        reasons = sorted({names[k] for _, r in sel for k in range(4) if r[5 + k] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(sel), "window": window}
 
 
 def measured_hbm_peak():
@@ -250,6 +267,10 @@ def run_ours(args):
         st.lib().st_set_stream(h.handle, torch.cuda.current_stream(dev).cuda_stream)
     timer = DeviceTimer(torch, h.stream(), dev)
     k = 0
+    # the clock sampler starts before the warm-up: nvidia-smi's start-up must not overlap
+    # the timed region
+    clk = ClockSampler(local).__enter__()
+    time.sleep(1.5)
     for _ in range(args.warmup):
         h.step(dt, fs(k))
         if src_view is not None:
@@ -260,14 +281,17 @@ def run_ours(args):
     h.profile(True)
     h.profile_read("step", reset=True)
     launches0 = h.launch_count()
-    with ClockSampler(local) as clk:
-        timer.start()
-        for _ in range(args.steps):
-            h.step(dt, fs(k))
-            if src_view is not None:
-                pg.all_reduce(src_view)
-            k += 1
-        ms = timer.stop()
+    w0 = time.time()
+    timer.start()
+    for _ in range(args.steps):
+        h.step(dt, fs(k))
+        if src_view is not None:
+            pg.all_reduce(src_view)
+        k += 1
+    ms = timer.stop()
+    w1 = time.time()
+    time.sleep(0.3)
+    clk.__exit__(None, None, None)
     launches = h.launch_count() - launches0
     nstep, step_ms = h.profile_read("step")
     nfin, fin_ms = h.profile_read("finalize")
@@ -279,7 +303,7 @@ def run_ours(args):
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms = float(t.item())
-    clocks = clk.summary()
+    clocks = clk.summary(w0, w1)
     ms_per_step = ms / args.steps
     value = ws * npcl * args.steps / (ms / 1e3)
 
