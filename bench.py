@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--accuracy-steps", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-extras", action="store_true", help="only the headline timing")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip the configuration-4 adjoint timing")
+    ap.add_argument("--no-clouds", dest="clouds", action="store_false",
+                    help="skip the configuration-3 multi-cloud timing")
     return ap.parse_args()
 
 
@@ -370,6 +374,14 @@ def run_ours(args):
                "path": "st_evolve_cloud: U (float32 [nCells][3], pinned) H2D, step, source "
                        "(float32 UTrans, pinned) D2H; fixed fluid scale"}
 
+    # ---- 64 clouds in one launch, graph replay, autotuned ----
+    if not args.no_extras and rank == 0 and args.clouds:
+        extras["clouds"] = run_clouds(st, torch, local, dev)
+
+    # ---- adjoint of the time-averaged source ----
+    if not args.no_extras and rank == 0 and args.adjoint:
+        extras["adjoint"] = run_adjoint(st, local)
+
     # ---- CPU baseline: the oracle on this host's cores (bounded sample) ----
     cpu = None
     if not args.no_extras and rank == 0 and args.cpu_seconds > 0:
@@ -399,6 +411,104 @@ def run_ours(args):
     }
     line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+def run_clouds(st, torch, local, dev):
+    """Configuration 3: 64 clouds with log-uniform sizes on a 64^3 mesh, each with its own
+    source, one persistent launch per step; block size and re-sort interval from the
+    autotuner; the step sequence replayed from a captured CUDA graph."""
+    c = workload.CONFIGS["c3_clouds_64"]
+    sizes, dmed = workload.cloud_sizes(c)
+    n = c["n"]
+    U = workload.tgv_field(n, dtype=np.float32)
+    prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                    drag_model="schiller_naumann", precision="mixed", n_substeps=1,
+                    n_clouds=c["nclouds"], sort_interval=20)
+    total = int(sizes.sum())
+    with st.ParcelTracker(prm, st.mesh_desc(n, 0.0, workload.L_BOX), local) as h:
+        for k in range(c["nclouds"]):
+            xyz, uvw, d = workload.parcels(int(sizes[k]), 1000 + k, d_median=float(dmed[k]))
+            h.set_parcels(xyz, uvw, d, cloud=k)
+        h.set_fluid_velocity(U)
+        tune = h.autotune(workload.DT, trial_steps=40)
+        si = tune["sort_interval"]
+        chunk = 2 * si if si else 20
+        timer = DeviceTimer(torch, h.stream(), dev)
+        # plain launches
+        for _ in range(3):
+            h.step(workload.DT)
+        h.synchronize()
+        steps = (c["steps"] // chunk) * chunk
+        timer.start()
+        for _ in range(steps):
+            h.step(workload.DT)
+        ms_plain = timer.stop()
+        # captured graph (capture right after a re-sort: run up to the next one first)
+        h.synchronize()
+        extra = (si - (3 + steps) % si) % si if si else 0
+        for _ in range(extra):
+            h.step(workload.DT)
+        h.graph_capture(chunk, workload.DT)
+        h.graph_launch()
+        h.synchronize()
+        timer.start()
+        for _ in range(steps // chunk):
+            h.graph_launch()
+        ms_graph = timer.stop()
+        h.synchronize()
+    return {"workload": "BASELINE config 3: 64 clouds, sizes log-uniform in [1e3, 2e6] (seed 2), "
+                        "median diameter per cloud uniform in [5, 50] um, 64^3 mesh, one "
+                        "source per cloud, mixed precision, one launch per step",
+            "parcels": total, "steps": steps, "autotune": tune,
+            "particle_steps_per_s_graph": total * steps / (ms_graph / 1e3),
+            "particle_steps_per_s_launches": total * steps / (ms_plain / 1e3),
+            "ms_per_step_graph": ms_graph / steps, "ms_per_step_launches": ms_plain / steps}
+
+
+def run_adjoint(st, device):
+    """Forward (objective) and pull-back (gradient) times of configuration 4: J = |Sbar -
+    S*|^2 over 200 steps, 1e6 parcels, 128^3 cells, checkpoints every 20 steps."""
+    c = workload.CONFIGS["c4_adjoint_128"]
+    n, npcl, T, C = c["n"], c["nparcels"], c["steps"], c["checkpoint"]
+    xyz, uvw, d = workload.parcels(npcl, c["seed"])
+    U = workload.tgv_field(n, dtype=np.float32)
+    mesh = st.mesh_desc(n, 0.0, workload.L_BOX)
+
+    def prm(alpha=1.0, s=1.0):
+        return st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                         drag_model="schiller_naumann", precision="mixed", n_substeps=1,
+                         drag_multiplier=alpha, diameter_scale=s, sort_interval=20)
+
+    with st.ParcelTracker(prm(c["target_alpha"], c["target_dscale"]), mesh, device) as ht:
+        ht.set_parcels(xyz, uvw, d)
+        ht.set_fluid_velocity(U)
+        target = ht.mean_source_forward(T, C, workload.DT)
+    with st.ParcelTracker(prm(), mesh, device) as h:
+        h.set_parcels(xyz, uvw, d)
+        h.set_fluid_velocity(U)
+        h.mean_source_forward(T, C, workload.DT)  # warm-up
+        h.mean_source_pullback(np.zeros((n ** 3, 3)), T, C, workload.DT, want_v0=False)
+        h.profile(True)
+        h.profile_read("adj_forward", reset=True)
+        reps = 3
+        for _ in range(reps):
+            S = h.mean_source_forward(T, C, workload.DT)
+            r = S - target
+            J = float(np.sum(r * r))
+            da, ds, dv0 = h.mean_source_pullback(2.0 * r, T, C, workload.DT)
+        nf, fwd_ms = h.profile_read("adj_forward")
+        nb, bwd_ms = h.profile_read("adj_reverse")
+        h.profile(False)
+    fwd = fwd_ms / reps
+    bwd = bwd_ms / reps
+    return {"workload": "BASELINE config 4: 128^3 hex, 1e6 parcels, 200 steps, checkpoints every "
+                        "20 steps, mixed precision, J = |mean source - target|^2, target from "
+                        "drag x1.1 and diameters x0.95",
+            "forward_ms": round(fwd, 3), "pullback_ms": round(bwd, 3),
+            "adjoint_over_forward": round(bwd / fwd, 3),
+            "forward_particle_steps_per_s": npcl * T / (fwd / 1e3),
+            "objective": J, "dJ_ddrag_multiplier": da, "dJ_ddiameter_scale": ds,
+            "dJ_dv0_l2": float(np.linalg.norm(dv0))}
 
 
 def cpu_rate(n, xyz, uvw, d, U, budget_s, threads=None):

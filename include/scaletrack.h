@@ -136,9 +136,33 @@ ST_API int st_synchronize(st_handle* h);
 ST_API void* st_get_stream(st_handle* h);
 ST_API int st_set_stream(st_handle* h, void* stream);
 
+/* ---- CUDA-graph replay and autotuning ---------------------------------------------- */
+/* Captures n_steps calls of st_step (dt, fluid_scale[k] or 1) into a CUDA graph on the
+ * handle's stream; st_graph_launch replays them (asynchronously), which removes the host
+ * launch cost of a multi-cloud step sequence.  With re-sorting on, capture right after set-up
+ * or a re-sort and a multiple of 2 x sort_interval steps, so every replay starts from the same
+ * buffers.  st_set_parcels and st_autotune release the graph. */
+ST_API int st_graph_capture(st_handle* h, int n_steps, double dt, const double* fluid_scale);
+ST_API int st_graph_launch(st_handle* h);
+ST_API int st_graph_release(st_handle* h);
+
+typedef struct st_tune_result {
+    int32_t block_size;   /* threads per block of the step kernel */
+    int32_t grid_blocks;  /* persistent grid: SMs x resident blocks at that size */
+    int32_t sort_interval;
+    int32_t pad;
+    double ms_per_step;   /* measured, including the amortised re-sort */
+} st_tune_result;
+/* Times trial_steps steps for every block size in {128, 256} and re-sort interval in
+ * {never, 10, 20, 40} on a copy of the handle (the caller's parcels do not advance) and keeps
+ * the fastest.  The results of a step do not depend on either choice: parcel order never
+ * changes positions, velocities or the fixed-point source. */
+ST_API int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out);
+
 /* ---- instrumentation --------------------------------------------------------------- */
 enum { ST_KERNEL_STEP = 0, ST_KERNEL_FINALIZE = 1, ST_KERNEL_SORT = 2, ST_KERNEL_PROBE = 3,
-       ST_KERNEL_OTHER = 4, ST_KERNEL_KINDS = 5 };
+       ST_KERNEL_OTHER = 4, ST_KERNEL_ADJ_FORWARD = 5, ST_KERNEL_ADJ_REVERSE = 6,
+       ST_KERNEL_KINDS = 7 };
 /* Record CUDA events around every kernel the library launches (on the launching stream). */
 ST_API int st_profile_enable(st_handle* h, int on);
 /* Launch count and summed device time (ms) of one kernel kind since the last reset;
@@ -146,6 +170,31 @@ ST_API int st_profile_enable(st_handle* h, int on);
 ST_API int st_profile_read(st_handle* h, int kind, int64_t* launches, double* ms, int reset);
 /* Total number of kernels the library launched on this handle. */
 ST_API int64_t st_launch_count(st_handle* h);
+
+/* ---- adjoint of the time-averaged source (no counterpart in the reference) ---------- */
+/* The differentiable map is Sbar = (1/T) sum_{n<T} S_n over T steps of one cloud starting
+ * from its current state (which is not modified), Schiller-Naumann drag, one substep,
+ * mixed or FP64 precision.  Cell ownership and wall-bounce decisions are frozen at the
+ * forward pass.  This is the backend of a Julia ChainRules rrule: the forward call is the
+ * primal, the pull-back call the backward closure. */
+typedef struct st_adjoint_desc {
+    int32_t n_steps;             /* T >= 1 */
+    int32_t checkpoint_interval; /* C >= 1: (x, v) is stored every C steps and the C steps
+                                    after a checkpoint are recomputed in the pull-back */
+    double dt;                   /* time step (one substep) */
+    const double* fluid_scale;   /* [T] factor on U per step (host), or NULL for 1 */
+} st_adjoint_desc;
+/* Runs the forward pass, keeps its checkpoints in the handle and writes Sbar (host
+ * [nCells][3], FP64, deterministic fixed-point reduction with one scale for the run). */
+ST_API int st_mean_source_forward(st_handle* h, int cloud, const st_adjoint_desc* desc,
+                                  double* mean_source);
+/* Pull-back of the last st_mean_source_forward with the same desc: given the cotangent
+ * dJ/dSbar (host [nCells][3]) returns dJ/d(drag_multiplier), dJ/d(diameter_scale) and
+ * dJ/dv0 (host [3][n], order of st_set_parcels; may be NULL).  Velocity cotangents are in
+ * the velocity precision, parameter sums in FP64 (reproducible reduction order). */
+ST_API int st_mean_source_pullback(st_handle* h, int cloud, const st_adjoint_desc* desc,
+                                   const double* cotangent, double* d_drag_multiplier,
+                                   double* d_diameter_scale, double* d_velocity0);
 
 /* ---- shims with the reference's names and semantics -------------------------------- */
 /* Creates (or replaces) the process-wide default handle used by the two calls below, on

@@ -17,6 +17,7 @@
 #endif
 
 #include "step_oracle.hpp"
+#include "adjoint_oracle.hpp"
 
 using namespace st_oracle;
 
@@ -288,6 +289,154 @@ int oracle_num_threads(void)
 #else
     return 1;
 #endif
+}
+
+}  // extern "C"
+
+namespace {
+
+template <class P, class V>
+int adjoint_run(const oracle_cfg* cfg, int64_t np, const double* xyz, const double* uvw,
+                const double* d, const double* U, int T, double dt, const double* fscale,
+                const double* cotangent, const double* target, int mean_limbs,
+                double* mean_src, double* J_out, double* dalpha, double* dscale, double* dv0,
+                int32_t* fz_cell, uint8_t* fz_bounce, int replay)
+{
+    if (cfg->n_substeps != 1 || cfg->drag != DRAG_SN_EXPLICIT) return -2;
+    Params<P, V> pr = make_params<P, V>(cfg->n, cfg->origin, cfg->ending, cfg->mu_c, cfg->rho_c,
+                                        cfg->rho_d, cfg->drag, 1, cfg->drag_multiplier,
+                                        cfg->diameter_scale);
+    const int64_t nC = pr.mesh.nCells;
+    const P dtP = (P)dt;
+    const V dtV = (V)dtP;
+    const bool want_grad = dalpha || dscale || dv0;
+    std::vector<Frozen> fz((size_t)T * np);
+    if (replay)
+        for (int64_t k = 0; k < (int64_t)T * np; ++k) fz[k] = Frozen{fz_cell[k], fz_bounce[k]};
+    std::vector<V> vrec(want_grad ? (size_t)T * np * 3 : 0);
+    /* fixed-point model of the mean source (constant scale over the T steps) */
+    const int limbs = mean_limbs == 2 ? 2 : 1;
+    const int64_t nbound = std::max<int64_t>(2, np * (int64_t)T);
+    const int H = quant_headroom(limbs, nbound);
+    int emax = EXP_NONE;
+    for (int64_t i = 0; i < np; ++i) {  /* probe: largest deposit of the first step */
+        P pos[3] = {(P)xyz[i], (P)xyz[np + i], (P)xyz[2 * np + i]};
+        V vel[3] = {(V)uvw[i], (V)uvw[np + i], (V)uvw[2 * np + i]};
+        Frozen f = replay ? fz[i] : Frozen{0, 0};
+        StepLocal<V> o;
+        if (!adj_forward_step<P, V>(pr, dtP, dtV, U, fscale ? (V)fscale[0] : (V)1, pos, vel,
+                                    (V)d[i], f, replay != 0, o))
+            return -1;
+        for (int c = 0; c < 3; ++c) {
+            double dv = (double)o.dep[c];
+            if (dv != 0.0 && std::isfinite(dv)) emax = std::max(emax, exp_of(dv));
+        }
+    }
+    const int L = (emax == EXP_NONE) ? -H : emax - H;
+    std::vector<int64_t> q1(limbs == 1 ? 3 * nC : 0, 0), hi(limbs == 2 ? 3 * nC : 0, 0);
+    std::vector<uint64_t> lo(limbs == 2 ? 3 * nC : 0, 0);
+    int64_t ovf = 0;
+    for (int64_t i = 0; i < np; ++i) {
+        P pos[3] = {(P)xyz[i], (P)xyz[np + i], (P)xyz[2 * np + i]};
+        V vel[3] = {(V)uvw[i], (V)uvw[np + i], (V)uvw[2 * np + i]};
+        for (int n = 0; n < T; ++n) {
+            if (want_grad)
+                for (int c = 0; c < 3; ++c) vrec[((size_t)n * np + i) * 3 + c] = vel[c];
+            Frozen& f = fz[(size_t)n * np + i];
+            StepLocal<V> o;
+            if (!adj_forward_step<P, V>(pr, dtP, dtV, U, fscale ? (V)fscale[n] : (V)1, pos,
+                                        vel, (V)d[i], f, replay != 0, o))
+                return -1;
+            for (int c = 0; c < 3; ++c) {
+                double dv = (double)o.dep[c];
+                if (dv == 0.0) continue;
+                if (!std::isfinite(dv) || exp_of(dv) - L > H + QUANT_GROWTH_BITS) { ++ovf; continue; }
+                int64_t q = std::llrint(ldexp2(dv, -L));
+                const int64_t j = 3 * (int64_t)f.cell + c;
+                if (limbs == 1) q1[j] = (int64_t)((uint64_t)q1[j] + (uint64_t)q);
+                else { hi[j] += q >> 32; lo[j] += (uint64_t)q & 0xffffffffULL; }
+            }
+        }
+    }
+    std::vector<double> Sbar(3 * nC);
+    for (int64_t j = 0; j < 3 * nC; ++j) {
+        double v;
+        if (limbs == 1) {
+            v = (double)q1[j];
+        } else {
+            int64_t h = hi[j] + (int64_t)(lo[j] >> 32);
+            v = (double)h * 4294967296.0 + (double)(lo[j] & 0xffffffffULL);
+        }
+        Sbar[j] = ldexp2(v, L) / (double)T;
+    }
+    if (mean_src) std::memcpy(mean_src, Sbar.data(), sizeof(double) * 3 * nC);
+    double J = 0.0;
+    std::vector<double> G(3 * nC, 0.0);
+    for (int64_t j = 0; j < 3 * nC; ++j) {
+        double yb;
+        if (cotangent) {
+            yb = cotangent[j];
+        } else {
+            const double r = Sbar[j] - (target ? target[j] : 0.0);
+            J += r * r;
+            yb = 2.0 * r;
+        }
+        G[j] = yb / (double)T;
+    }
+    if (J_out) *J_out = J;
+    if (!replay && fz_cell)
+        for (int64_t k = 0; k < (int64_t)T * np; ++k) {
+            fz_cell[k] = fz[k].cell;
+            fz_bounce[k] = fz[k].bounce;
+        }
+    if (!want_grad) return ovf ? 2 : 0;
+    double da = 0.0, ds = 0.0;
+    for (int64_t i = 0; i < np; ++i) {
+        V a[3] = {(V)0, (V)0, (V)0};
+        for (int n = T - 1; n >= 0; --n) {
+            const Frozen& f = fz[(size_t)n * np + i];
+            V vel[3];
+            for (int c = 0; c < 3; ++c) vel[c] = vrec[((size_t)n * np + i) * 3 + c];
+            V Gc[3];
+            for (int c = 0; c < 3; ++c) Gc[c] = (V)G[3 * (int64_t)f.cell + c];
+            adj_reverse_step<P, V>(pr, dtP, dtV, U, fscale ? (V)fscale[n] : (V)1, vel, (V)d[i],
+                                   f, Gc, a, da, ds);
+        }
+        if (dv0)
+            for (int c = 0; c < 3; ++c) dv0[c * np + i] = (double)a[c];
+    }
+    if (dalpha) *dalpha = da;
+    if (dscale) *dscale = ds;
+    return ovf ? 2 : 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+/* Mean-source objective and its adjoint (SN drag, one substep), see adjoint_oracle.hpp.
+ *  cotangent: dJ/dSbar [nCells][3], or NULL: J = sum (Sbar - target)^2 (target NULL = 0)
+ *  mean_limbs: fixed-point model of the mean source (1 or 2 limbs, constant scale)
+ *  fz_cell/fz_bounce [T][np]: frozen ownership, written (replay = 0) or read (replay = 1)
+ * Returns 0, 2 (deposit out of range), -1 (parcel outside the mesh), -2 (unsupported). */
+int oracle_adjoint(const oracle_cfg* cfg, int64_t np, const double* xyz, const double* uvw,
+                   const double* d, const double* U, int T, double dt, const double* fscale,
+                   const double* cotangent, const double* target, int mean_limbs,
+                   double* mean_src, double* J_out, double* dalpha, double* dscale, double* dv0,
+                   int32_t* fz_cell, uint8_t* fz_bounce, int replay)
+{
+    switch (cfg->precision) {
+    case 1:
+        return adjoint_run<double, float>(cfg, np, xyz, uvw, d, U, T, dt, fscale, cotangent,
+                                          target, mean_limbs, mean_src, J_out, dalpha, dscale,
+                                          dv0, fz_cell, fz_bounce, replay);
+    case 2:
+        return adjoint_run<double, double>(cfg, np, xyz, uvw, d, U, T, dt, fscale, cotangent,
+                                           target, mean_limbs, mean_src, J_out, dalpha, dscale,
+                                           dv0, fz_cell, fz_bounce, replay);
+    default:
+        return -2;
+    }
 }
 
 }  // extern "C"

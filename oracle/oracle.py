@@ -60,6 +60,13 @@ def lib():
         L.oracle_pow0687.argtypes = [ctypes.c_int64, P(ctypes.c_double), P(ctypes.c_double)]
         L.oracle_pow0687f.argtypes = [ctypes.c_int64, P(ctypes.c_float), P(ctypes.c_float)]
         L.oracle_num_threads.restype = ctypes.c_int
+        L.oracle_adjoint.argtypes = [
+            P(OracleCfg), ctypes.c_int64, P(ctypes.c_double), P(ctypes.c_double),
+            P(ctypes.c_double), P(ctypes.c_double), ctypes.c_int, ctypes.c_double,
+            P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double), ctypes.c_int,
+            P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double),
+            P(ctypes.c_double), P(ctypes.c_int32), P(ctypes.c_uint8), ctypes.c_int]
+        L.oracle_adjoint.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -145,3 +152,43 @@ def pow0687f(x):
 
 def num_threads():
     return lib().oracle_num_threads()
+
+
+def adjoint(cfg, xyz, uvw, d, U, T, dt, fscale=None, cotangent=None, target=None,
+            mean_limbs=1, grad=True, frozen=None):
+    """Mean-source objective (and its adjoint when grad=True) with frozen ownership.
+
+    frozen=None records the ownership of this run; frozen=(cells, bounce) replays it.
+    Returns dict(mean_src, J, dalpha, dscale, dv0 [3, np], frozen=(cells, bounce), status)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    uvw = np.ascontiguousarray(uvw, dtype=np.float64)
+    d = np.ascontiguousarray(d, dtype=np.float64)
+    U = np.ascontiguousarray(U, dtype=np.float64).reshape(-1)
+    npcl = d.shape[0]
+    ncells = int(cfg.n[0]) * int(cfg.n[1]) * int(cfg.n[2])
+    fs = None if fscale is None else np.ascontiguousarray(fscale, dtype=np.float64)
+    cot = None if cotangent is None else np.ascontiguousarray(cotangent, dtype=np.float64).reshape(-1)
+    tgt = None if target is None else np.ascontiguousarray(target, dtype=np.float64).reshape(-1)
+    mean = np.zeros(3 * ncells)
+    J = np.zeros(1)
+    da = np.zeros(1)
+    ds = np.zeros(1)
+    dv0 = np.zeros((3, npcl)) if grad else None
+    replay = frozen is not None
+    if replay:
+        cells = np.ascontiguousarray(frozen[0], dtype=np.int32)
+        bounce = np.ascontiguousarray(frozen[1], dtype=np.uint8)
+    else:
+        cells = np.zeros(T * npcl, dtype=np.int32)
+        bounce = np.zeros(T * npcl, dtype=np.uint8)
+    st = lib().oracle_adjoint(ctypes.byref(cfg), npcl, _ptr(xyz, ctypes.c_double),
+                              _ptr(uvw, ctypes.c_double), _ptr(d, ctypes.c_double),
+                              _ptr(U, ctypes.c_double), T, dt, _ptr(fs, ctypes.c_double),
+                              _ptr(cot, ctypes.c_double), _ptr(tgt, ctypes.c_double), mean_limbs,
+                              _ptr(mean, ctypes.c_double), _ptr(J, ctypes.c_double),
+                              _ptr(da, ctypes.c_double) if grad else None,
+                              _ptr(ds, ctypes.c_double) if grad else None,
+                              _ptr(dv0, ctypes.c_double), _ptr(cells, ctypes.c_int32),
+                              _ptr(bounce, ctypes.c_uint8), 1 if replay else 0)
+    return dict(mean_src=mean.reshape(ncells, 3), J=float(J[0]), dalpha=float(da[0]),
+                dscale=float(ds[0]), dv0=dv0, frozen=(cells, bounce), status=st)

@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 #include <map>
+#include <algorithm>
 
 #include <cuda_runtime.h>
 
@@ -84,6 +85,31 @@ struct ProfRec {
     cudaEvent_t a, b;
 };
 
+/* Device memory of the mean-source adjoint: checkpoints of the last forward pass, the
+ * records of one segment, the cotangent and the per-block parameter partials. */
+struct AdjTape {
+    bool valid = false;
+    int cloud = -1;
+    int T = 0, C = 0, nseg = 0, grid = 0, limbs = 1;
+    int64_t n = 0;
+    double dt = 0.0;
+    std::vector<double> fs;     /* host copy of the per-step factors of the forward pass */
+    size_t bytes = 0;
+    void* mem = nullptr;        /* one allocation, carved below */
+    void* ck_x = nullptr;
+    void* ck_v = nullptr;
+    void* rec_v = nullptr;
+    int32_t* rec_c = nullptr;
+    uint8_t* rec_b = nullptr;
+    double* G = nullptr;
+    void* adj_v = nullptr;
+    double* partials = nullptr;
+    void* fsd = nullptr;
+    double* mean = nullptr;
+    CloudCtl* ctl = nullptr;
+    unsigned long long* acc = nullptr;
+};
+
 struct st_handle {
     st_params p;
     st_mesh_desc m;
@@ -118,10 +144,19 @@ struct st_handle {
     bool prof = false;
     std::vector<ProfRec> recs;
     std::vector<cudaEvent_t> pool;
-    int64_t prof_launches[ST_KERNEL_KINDS] = {0, 0, 0, 0, 0};
-    double prof_ms[ST_KERNEL_KINDS] = {0, 0, 0, 0, 0};
+    int64_t prof_launches[ST_KERNEL_KINDS] = {};
+    double prof_ms[ST_KERNEL_KINDS] = {};
     void* dstage = nullptr;
     size_t stage_bytes = 0;
+    AdjTape adj;
+    /* CUDA-graph replay of a step sequence */
+    bool capturing = false;
+    int cap_parity = 0;          /* which of the two descriptor arrays the captured step uses */
+    void* dclouds2 = nullptr;    /* descriptors for the current and the re-sorted buffers */
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int graph_steps = 0;
+    int64_t graph_launches = 0;
 };
 
 namespace {
@@ -323,6 +358,7 @@ int do_sort_all(st_handle* h)
     }
     h->clouds_dirty = true;
     h->steps_since_sort = 0;
+    if (h->capturing) h->cap_parity ^= 1;
     return ST_OK;
 }
 
@@ -330,7 +366,7 @@ template <class P, class V>
 int do_step(st_handle* h, double dt, double fscale)
 {
     int rc;
-    if (h->clouds_dirty && (rc = upload_clouds<P, V>(h)) != ST_OK) return rc;
+    if (!h->capturing && h->clouds_dirty && (rc = upload_clouds<P, V>(h)) != ST_OK) return rc;
     StepArgs<P, V> a;
     a.mesh = mesh_k<P>(h);
     a.phys = phys_k<V>(h);
@@ -339,7 +375,9 @@ int do_step(st_handle* h, double dt, double fscale)
     a.fscale = (V)fscale;
     a.nclouds = h->p.n_clouds;
     a.U = (const V*)h->dU;
-    a.clouds = (const CloudK<P, V>*)h->dclouds;
+    a.clouds = h->capturing
+                   ? (const CloudK<P, V>*)h->dclouds2 + (size_t)h->cap_parity * h->p.n_clouds
+                   : (const CloudK<P, V>*)h->dclouds;
     a.ctl = h->dctl;
     a.total_tiles = h->total_tiles;
     if (a.total_tiles == 0) return ST_OK;
@@ -562,6 +600,323 @@ void free_cloud(CloudBufs& c)
 }  // namespace
 
 /* ------------------------------------------------------------------------------------ */
+/* graph capture and autotuning                                                         */
+/* ------------------------------------------------------------------------------------ */
+namespace {
+
+/* Descriptor arrays for the current buffers [0] and for the buffers after one re-sort [1]
+ * (clouds of more than one parcel swap buffers), so that a captured sequence can switch
+ * between them without host copies. */
+template <class P, class V>
+int upload_clouds_pair(st_handle* h)
+{
+    int rc;
+    if ((rc = upload_clouds<P, V>(h))) return rc;
+    const int nc = h->p.n_clouds;
+    std::vector<CloudK<P, V>> v(2 * nc);
+    memcpy(v.data(), h->hclouds.data(), sizeof(CloudK<P, V>) * nc);
+    for (int c = 0; c < nc; ++c) {
+        CloudBufs& b = h->clouds[c];
+        CloudK<P, V> k = v[c];
+        if (b.n > 1) {
+            const int o = 1 - b.cur;
+            k.x = (P*)b.x[o]; k.y = (P*)b.y[o]; k.z = (P*)b.z[o];
+            k.u = (V*)b.u[o]; k.v = (V*)b.v[o]; k.w = (V*)b.w[o]; k.d = (const V*)b.d[o];
+        }
+        v[nc + c] = k;
+    }
+    if (!h->dclouds2) CK(cudaMalloc(&h->dclouds2, 2 * 256 * (size_t)nc));
+    CK(cudaMemcpyAsync(h->dclouds2, v.data(), sizeof(CloudK<P, V>) * 2 * nc,
+                       cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ST_OK;
+}
+
+void release_graph(st_handle* h)
+{
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->gexec = nullptr;
+    h->graph = nullptr;
+    h->graph_steps = 0;
+}
+
+template <class P, class V>
+int graph_capture(st_handle* h, int n, double dt, const double* fs)
+{
+    int rc;
+    release_graph(h);
+    CK(cudaStreamSynchronize(h->stream));
+    const bool det = (h->dep == DEP_DET1 || h->dep == DEP_DET2);
+    if (det && (h->need_probe || dt != h->last_dt)) {
+        /* the first-step scale comes from a read-only probe, run outside the graph */
+        if ((rc = upload_clouds<P, V>(h))) return rc;
+        StepArgs<P, V> a;
+        a.mesh = mesh_k<P>(h);
+        a.phys = phys_k<V>(h);
+        a.dtP = (P)dt / (P)h->p.n_substeps;
+        a.dtV = (V)a.dtP;
+        a.fscale = (V)(fs ? fs[0] : 1.0);
+        a.nclouds = h->p.n_clouds;
+        a.U = (const V*)h->dU;
+        a.clouds = (const CloudK<P, V>*)h->dclouds;
+        a.ctl = h->dctl;
+        a.total_tiles = h->total_tiles;
+        if (a.total_tiles > 0) {
+            CK(launch_step<P, V>(a, DEP_PROBE, h->grid, h->block, h->stream));
+            CK(launch_set_scale(h->dctl, h->p.n_clouds, h->stream));
+            h->launches += 2;
+        }
+        h->need_probe = false;
+        h->last_dt = dt;
+    }
+    if ((rc = upload_clouds_pair<P, V>(h))) return rc;
+    std::vector<int> cur(h->clouds.size());
+    for (size_t c = 0; c < h->clouds.size(); ++c) cur[c] = h->clouds[c].cur;
+    const int64_t steps0 = h->steps, launches0 = h->launches;
+    const int since0 = h->steps_since_sort;
+    const bool prof = h->prof;
+    h->prof = false;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    h->capturing = true;
+    h->cap_parity = 0;
+    for (int k = 0; k < n && rc == ST_OK; ++k) rc = do_step<P, V>(h, dt, fs ? fs[k] : 1.0);
+    h->capturing = false;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->prof = prof;
+    const int64_t per = h->launches - launches0;
+    for (size_t c = 0; c < h->clouds.size(); ++c) h->clouds[c].cur = cur[c];
+    h->steps = steps0;
+    h->steps_since_sort = since0;
+    h->launches = launches0;
+    h->clouds_dirty = true;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(ST_ERR_CUDA, "stream capture: %s", cudaGetErrorString(e));
+    h->graph = g;
+    if ((e = cudaGraphInstantiate(&h->gexec, g, 0)) != cudaSuccess) {
+        release_graph(h);
+        return fail(ST_ERR_CUDA, "graph instantiation: %s", cudaGetErrorString(e));
+    }
+    h->graph_steps = n;
+    h->graph_launches = per;
+    return ST_OK;
+}
+
+int occupancy_grid(st_handle* h, int block)
+{
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+    int occ = h->p.precision == ST_PREC_FP32
+                  ? step_max_active_blocks<float, float>(h->dep, block)
+                  : (h->p.precision == ST_PREC_MIXED
+                         ? step_max_active_blocks<double, float>(h->dep, block)
+                         : step_max_active_blocks<double, double>(h->dep, block));
+    return nsm * (occ < 1 ? 1 : occ);
+}
+
+}  // namespace
+
+/* ------------------------------------------------------------------------------------ */
+/* adjoint of the time-averaged source                                                  */
+/* ------------------------------------------------------------------------------------ */
+namespace {
+
+int adj_check(st_handle* h, int cloud, const st_adjoint_desc* d)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    if (!d) return fail(ST_ERR_INVALID_ARGUMENT, "null adjoint descriptor");
+    if (h->p.precision == ST_PREC_FP32 || h->p.drag_model != ST_DRAG_SCHILLER_NAUMANN ||
+        h->p.n_substeps != 1)
+        return fail(ST_ERR_INVALID_ARGUMENT,
+                    "the adjoint supports Schiller-Naumann drag, one substep and mixed or FP64 "
+                    "precision");
+    if (d->n_steps < 1 || d->checkpoint_interval < 1)
+        return fail(ST_ERR_INVALID_ARGUMENT, "n_steps and checkpoint_interval must be >= 1");
+    if (!(d->dt > 0) || !(d->dt < 1e300)) return fail(ST_ERR_INVALID_ARGUMENT, "dt must be positive");
+    if (!(h->p.drag_multiplier > 0) || !(h->p.diameter_scale > 0))
+        return fail(ST_ERR_INVALID_ARGUMENT, "drag_multiplier and diameter_scale must be positive");
+    return ST_OK;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+template <class P, class V>
+int adj_prepare(st_handle* h, int cloud, const st_adjoint_desc* d)
+{
+    AdjTape& t = h->adj;
+    const int64_t n = h->clouds[cloud].n;
+    const int T = d->n_steps, C = d->checkpoint_interval;
+    const int nseg = (T + C - 1) / C;
+    const int grid = (int)((n + 255) / 256);
+    const int limbs = sizeof(V) == 8 ? 2 : 1;
+    size_t off = 0;
+    auto carve = [&](size_t b) { size_t o = off; off += align256(b); return o; };
+    const size_t o_ckx = carve((size_t)nseg * 3 * n * sizeof(P));
+    const size_t o_ckv = carve((size_t)nseg * 3 * n * sizeof(V));
+    const size_t o_rv = carve((size_t)C * 3 * n * sizeof(V));
+    const size_t o_rc = carve((size_t)C * n * sizeof(int32_t));
+    const size_t o_rb = carve((size_t)C * n);
+    const size_t o_G = carve((size_t)h->stride * sizeof(double));
+    const size_t o_av = carve((size_t)3 * n * sizeof(V));
+    const size_t o_pa = carve((size_t)nseg * (grid > 0 ? grid : 1) * 2 * sizeof(double));
+    const size_t o_fs = carve((size_t)T * sizeof(V));
+    const size_t o_mean = carve((size_t)h->stride * sizeof(double));
+    const size_t o_ctl = carve(sizeof(CloudCtl));
+    const size_t o_acc = carve((size_t)h->stride * limbs * 8);
+    if (off > t.bytes) {
+        if (t.mem) cudaFree(t.mem);
+        t.mem = nullptr;
+        t.bytes = 0;
+        CK(cudaMalloc(&t.mem, off));
+        t.bytes = off;
+    }
+    char* b = static_cast<char*>(t.mem);
+    t.ck_x = b + o_ckx; t.ck_v = b + o_ckv; t.rec_v = b + o_rv;
+    t.rec_c = reinterpret_cast<int32_t*>(b + o_rc);
+    t.rec_b = reinterpret_cast<uint8_t*>(b + o_rb);
+    t.G = reinterpret_cast<double*>(b + o_G);
+    t.adj_v = b + o_av;
+    t.partials = reinterpret_cast<double*>(b + o_pa);
+    t.fsd = b + o_fs;
+    t.mean = reinterpret_cast<double*>(b + o_mean);
+    t.ctl = reinterpret_cast<CloudCtl*>(b + o_ctl);
+    t.acc = reinterpret_cast<unsigned long long*>(b + o_acc);
+    t.cloud = cloud; t.T = T; t.C = C; t.nseg = nseg; t.grid = grid; t.limbs = limbs;
+    t.n = n; t.dt = d->dt;
+    t.fs.assign(T, 1.0);
+    if (d->fluid_scale)
+        for (int k = 0; k < T; ++k) t.fs[k] = d->fluid_scale[k];
+    std::vector<V> fsv(T);
+    for (int k = 0; k < T; ++k) fsv[k] = (V)t.fs[k];
+    CK(cudaMemcpyAsync(t.fsd, fsv.data(), T * sizeof(V), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ST_OK;
+}
+
+template <class P, class V>
+AdjArgs<P, V> adj_args(st_handle* h)
+{
+    AdjTape& t = h->adj;
+    CloudBufs& c = h->clouds[t.cloud];
+    AdjArgs<P, V> a;
+    a.mesh = mesh_k<P>(h);
+    a.phys = phys_k<V>(h);
+    a.dtP = (P)t.dt;
+    a.dtV = (V)a.dtP;
+    a.n = t.n; a.T = t.T; a.C = t.C; a.limbs = t.limbs;
+    a.x = (const P*)c.x[c.cur]; a.y = (const P*)c.y[c.cur]; a.z = (const P*)c.z[c.cur];
+    a.u = (const V*)c.u[c.cur]; a.v = (const V*)c.v[c.cur]; a.w = (const V*)c.w[c.cur];
+    a.d = (const V*)c.d[c.cur];
+    a.U = (const V*)h->dU;
+    a.fs = (const V*)t.fsd;
+    a.acc = t.acc; a.ctl = t.ctl;
+    a.ck_x = (P*)t.ck_x; a.ck_v = (V*)t.ck_v;
+    a.rec_v = (V*)t.rec_v; a.rec_c = t.rec_c; a.rec_b = t.rec_b;
+    a.G = t.G; a.adj_v = (V*)t.adj_v; a.partials = t.partials;
+    return a;
+}
+
+template <class P, class V>
+int adj_forward(st_handle* h, int cloud, const st_adjoint_desc* d, double* mean_out)
+{
+    int rc;
+    h->adj.valid = false;
+    if ((rc = adj_prepare<P, V>(h, cloud, d))) return rc;
+    AdjTape& t = h->adj;
+    CloudCtl c0;
+    memset(&c0, 0, sizeof c0);
+    c0.emax = EXP_NONE;
+    int64_t bound = t.n * (int64_t)t.T;
+    if (bound < 2) bound = 2;
+    c0.H = t.limbs == 1 ? 62 - QUANT_GROWTH_BITS - quant_nbits(bound) : 62 - QUANT_GROWTH_BITS;
+    CK(cudaMemcpyAsync(t.ctl, &c0, sizeof c0, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(t.acc, 0, (size_t)h->stride * t.limbs * 8, h->stream));
+    AdjArgs<P, V> a = adj_args<P, V>(h);
+    {
+        ProfScope ps(h, ST_KERNEL_ADJ_FORWARD);
+        CK(launch_adj_forward<P, V>(a, true, h->stream));
+        CK(launch_adj_scale(t.ctl, h->stream));
+        CK(launch_adj_forward<P, V>(a, false, h->stream));
+        CK(launch_adj_mean(t.acc, t.ctl, t.limbs, t.T, t.mean, h->ncells * 3, h->stream));
+        h->launches += 4;
+    }
+    CloudCtl out;
+    CK(cudaMemcpyAsync(&out, t.ctl, sizeof out, cudaMemcpyDeviceToHost, h->stream));
+    if (mean_out)
+        CK(cudaMemcpyAsync(mean_out, t.mean, h->ncells * 3 * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (out.lost) return fail(ST_ERR_PARCEL_OUTSIDE, "parcel(s) left the mesh in the forward pass");
+    if (out.overflow)
+        return fail(ST_ERR_SOURCE_RANGE, "mean-source deposit(s) exceeded the fixed-point range");
+    t.valid = true;
+    return ST_OK;
+}
+
+template <class P, class V>
+int adj_pullback(st_handle* h, int cloud, const st_adjoint_desc* d, const double* cot,
+                 double* dalpha, double* dscale, double* dv0)
+{
+    AdjTape& t = h->adj;
+    bool same = t.valid && t.cloud == cloud && t.T == d->n_steps &&
+                t.C == d->checkpoint_interval && t.dt == d->dt && t.n == h->clouds[cloud].n;
+    for (int k = 0; same && k < t.T; ++k)
+        same = t.fs[k] == (d->fluid_scale ? d->fluid_scale[k] : 1.0);
+    if (!same)
+        return fail(ST_ERR_INVALID_ARGUMENT,
+                    "st_mean_source_pullback needs a preceding st_mean_source_forward with the "
+                    "same cloud and descriptor");
+    const int64_t ncomp = h->ncells * 3;
+    std::vector<double> G(ncomp);
+    for (int64_t j = 0; j < ncomp; ++j) G[j] = cot[j] / (double)t.T;
+    CK(cudaMemcpyAsync(t.G, G.data(), ncomp * sizeof(double), cudaMemcpyHostToDevice,
+                       h->stream));
+    CK(cudaMemsetAsync(t.adj_v, 0, (size_t)3 * t.n * sizeof(V), h->stream));
+    AdjArgs<P, V> a = adj_args<P, V>(h);
+    {
+        ProfScope ps(h, ST_KERNEL_ADJ_REVERSE);
+        for (int seg = t.nseg - 1; seg >= 0; --seg) {
+            const int len = std::min(t.C, t.T - seg * t.C);
+            CK(launch_adj_reverse<P, V>(a, seg, len, t.grid, h->stream));
+            h->launches += 1;
+        }
+    }
+    std::vector<double> parts((size_t)t.nseg * t.grid * 2);
+    if (!parts.empty())
+        CK(cudaMemcpyAsync(parts.data(), t.partials, parts.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream));
+    std::vector<V> av(dv0 ? (size_t)3 * t.n : 0);
+    std::vector<int32_t> id(dv0 ? t.n : 0);
+    CloudBufs& c = h->clouds[cloud];
+    if (dv0 && t.n > 0) {
+        CK(cudaMemcpyAsync(av.data(), t.adj_v, av.size() * sizeof(V), cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaMemcpyAsync(id.data(), c.id[c.cur], id.size() * sizeof(int32_t),
+                           cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    double sa = 0.0, ss = 0.0;  /* fixed order: segment, then block */
+    for (size_t k = 0; k < parts.size(); k += 2) {
+        sa += parts[k];
+        ss += parts[k + 1];
+    }
+    if (dalpha) *dalpha = sa;
+    if (dscale) *dscale = ss;
+    if (dv0)
+        for (int comp = 0; comp < 3; ++comp)
+            for (int64_t j = 0; j < t.n; ++j)
+                dv0[comp * t.n + id[j]] = (double)av[comp * t.n + j];
+    return ST_OK;
+}
+
+}  // namespace
+
+/* ------------------------------------------------------------------------------------ */
 /* public API                                                                           */
 /* ------------------------------------------------------------------------------------ */
 extern "C" {
@@ -709,8 +1064,10 @@ int st_destroy(st_handle* h)
     DeviceGuard g(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& c : h->clouds) free_cloud(c);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
     void* arrs[] = {h->dU, h->dsrc, h->dacc, h->dctl, h->dcounter, h->dcount, h->dclouds,
-                    h->dstage};
+                    h->dstage, h->adj.mem, h->dclouds2};
     for (void* p : arrs)
         if (p) cudaFree(p);
     for (auto& r : h->recs) {
@@ -762,6 +1119,7 @@ int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
         return fail(ST_ERR_INVALID_ARGUMENT, "null parcel array");
     DeviceGuard g(h->device);
     CK(cudaStreamSynchronize(h->stream));
+    release_graph(h);
     rc = DISPATCH(h, do_set_parcels, h, cloud, n, xyz, uvw, d);
     if (rc) return rc;
     return update_headroom(h);
@@ -936,6 +1294,142 @@ int st_profile_read(st_handle* h, int kind, int64_t* launches, double* ms, int r
 }
 
 int64_t st_launch_count(st_handle* h) { return h ? h->launches : -1; }
+
+int st_mean_source_forward(st_handle* h, int cloud, const st_adjoint_desc* desc,
+                           double* mean_source)
+{
+    int rc;
+    if ((rc = adj_check(h, cloud, desc))) return rc;
+    DeviceGuard g(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    return h->p.precision == ST_PREC_MIXED ? adj_forward<double, float>(h, cloud, desc, mean_source)
+                                           : adj_forward<double, double>(h, cloud, desc, mean_source);
+}
+
+int st_mean_source_pullback(st_handle* h, int cloud, const st_adjoint_desc* desc,
+                            const double* cotangent, double* d_drag_multiplier,
+                            double* d_diameter_scale, double* d_velocity0)
+{
+    int rc;
+    if ((rc = adj_check(h, cloud, desc))) return rc;
+    if (!cotangent) return fail(ST_ERR_INVALID_ARGUMENT, "null cotangent");
+    DeviceGuard g(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    return h->p.precision == ST_PREC_MIXED
+               ? adj_pullback<double, float>(h, cloud, desc, cotangent, d_drag_multiplier,
+                                             d_diameter_scale, d_velocity0)
+               : adj_pullback<double, double>(h, cloud, desc, cotangent, d_drag_multiplier,
+                                              d_diameter_scale, d_velocity0);
+}
+
+int st_graph_capture(st_handle* h, int n_steps, double dt, const double* fluid_scale)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (n_steps < 1) return fail(ST_ERR_INVALID_ARGUMENT, "n_steps must be >= 1");
+    if (!(dt > 0) || !(dt < 1e300)) return fail(ST_ERR_INVALID_ARGUMENT, "dt must be positive");
+    if (h->p.sort_interval > 0 &&
+        (h->steps_since_sort != 0 || n_steps % (2 * h->p.sort_interval) != 0))
+        return fail(ST_ERR_INVALID_ARGUMENT,
+                    "with re-sorting, capture right after a re-sort (or set-up) and a multiple "
+                    "of 2 x sort_interval steps, so that every replay starts from the same "
+                    "buffers");
+    DeviceGuard g(h->device);
+    return DISPATCH(h, graph_capture, h, n_steps, dt, fluid_scale);
+}
+
+int st_graph_launch(st_handle* h)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (!h->gexec) return fail(ST_ERR_INVALID_ARGUMENT, "no captured graph");
+    DeviceGuard g(h->device);
+    CK(cudaGraphLaunch(h->gexec, h->stream));
+    h->steps += h->graph_steps;
+    h->launches += h->graph_launches;
+    return ST_OK;
+}
+
+int st_graph_release(st_handle* h)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    DeviceGuard g(h->device);
+    cudaStreamSynchronize(h->stream);
+    release_graph(h);
+    return ST_OK;
+}
+
+int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (trial_steps < 4) return fail(ST_ERR_INVALID_ARGUMENT, "trial_steps must be >= 4");
+    if (!(dt > 0) || !(dt < 1e300)) return fail(ST_ERR_INVALID_ARGUMENT, "dt must be positive");
+    DeviceGuard g(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    release_graph(h);
+    /* trials run on a copy of the handle so that the caller's state does not advance */
+    st_handle* t = nullptr;
+    if ((rc = st_create(&h->p, &h->m, h->device, &t))) return rc;
+    for (int c = 0; c < h->p.n_clouds && rc == ST_OK; ++c) {
+        const int64_t n = h->clouds[c].n;
+        std::vector<double> xyz(3 * n), uvw(3 * n), d(n);
+        if (n > 0 && (rc = st_get_parcels(h, c, xyz.data(), uvw.data(), d.data()))) break;
+        rc = st_set_parcels(t, c, n, xyz.data(), uvw.data(), d.data());
+    }
+    if (rc == ST_OK) {
+        cudaError_t e = cudaMemcpy(t->dU, h->dU, h->ncells * 3 * h->vsz, cudaMemcpyDeviceToDevice);
+        if (e != cudaSuccess) rc = fail(ST_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e));
+    }
+    const int blocks[] = {128, 256};
+    const int sorts[] = {0, 10, 20, 40};
+    st_tune_result best;
+    best.block_size = h->block;
+    best.grid_blocks = h->grid;
+    best.sort_interval = h->p.sort_interval;
+    best.ms_per_step = 1e300;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int bi = 0; bi < 2 && rc == ST_OK; ++bi) {
+        for (int si = 0; si < 4 && rc == ST_OK; ++si) {
+            if (sorts[si] > trial_steps) continue;
+            t->block = blocks[bi];
+            t->grid = occupancy_grid(t, blocks[bi]);
+            t->p.sort_interval = sorts[si];
+            t->steps_since_sort = 0;
+            if ((rc = DISPATCH(t, do_sort_all, t))) break;  /* every trial starts sorted */
+            for (int k = 0; k < 2 && rc == ST_OK; ++k) rc = st_step(t, dt, 1.0);
+            cudaEventRecord(e0, t->stream);
+            for (int k = 0; k < trial_steps && rc == ST_OK; ++k) rc = st_step(t, dt, 1.0);
+            cudaEventRecord(e1, t->stream);
+            if (rc) break;
+            if ((rc = st_synchronize(t))) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const double per = ms / trial_steps;
+            if (per < best.ms_per_step) {
+                best.block_size = blocks[bi];
+                best.grid_blocks = t->grid;
+                best.sort_interval = sorts[si];
+                best.ms_per_step = per;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st_destroy(t);
+    if (rc) return rc;
+    h->block = best.block_size;
+    h->grid = best.grid_blocks;
+    h->p.block_size = best.block_size;
+    h->p.grid_blocks = best.grid_blocks;
+    h->p.sort_interval = best.sort_interval;
+    h->steps_since_sort = 0;
+    if (out) *out = best;
+    return ST_OK;
+}
 
 /* ------------------------------------------------------------------------------------ */
 /* reference-compatible shims                                                           */

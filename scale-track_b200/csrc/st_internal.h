@@ -90,6 +90,47 @@ struct StepArgs {
     int64_t total_tiles;        /* warp tiles (32 parcels) over all clouds */
 };
 
+/* Arguments of the adjoint kernels (st_adjoint.cu). */
+template <class P, class V>
+struct AdjArgs {
+    MeshK<P> mesh;
+    PhysK<V> phys;
+    P dtP;
+    V dtV;
+    int64_t n;                  /* parcels */
+    int T;                      /* steps */
+    int C;                      /* checkpoint interval */
+    int limbs;                  /* fixed-point limbs of the mean source */
+    const P* x;
+    const P* y;
+    const P* z;
+    const V* u;
+    const V* v;
+    const V* w;
+    const V* d;
+    const V* U;                 /* [nCells*3] */
+    const V* fs;                /* [T] fluid factor per step */
+    unsigned long long* acc;    /* [ncomp*limbs] mean-source accumulator */
+    CloudCtl* ctl;              /* scale and counters of the adjoint run */
+    P* ck_x;                    /* checkpoints [nseg][3][n] */
+    V* ck_v;
+    V* rec_v;                   /* forward records of one segment [C][3][n] */
+    int32_t* rec_c;             /* [C][n] */
+    uint8_t* rec_b;             /* [C][n] */
+    const double* G;            /* dJ/dS_n per cell component [ncomp] */
+    V* adj_v;                   /* velocity cotangent [3][n] */
+    double* partials;           /* [nseg][grid][2] parameter partials */
+};
+
+template <class P, class V>
+cudaError_t launch_adj_forward(const AdjArgs<P, V>& a, bool probe, cudaStream_t s);
+template <class P, class V>
+cudaError_t launch_adj_reverse(const AdjArgs<P, V>& a, int seg, int len, int grid,
+                               cudaStream_t s);
+cudaError_t launch_adj_scale(CloudCtl* ctl, cudaStream_t s);
+cudaError_t launch_adj_mean(const unsigned long long* acc, const CloudCtl* ctl, int limbs,
+                            int T, double* mean, int64_t ncomp, cudaStream_t s);
+
 /* Sets the thread-local message returned by st_last_error (st_abi.cu). */
 void st_set_last_error(const char* msg);
 

@@ -61,8 +61,12 @@ __global__ void k_sort_keys(const P* __restrict__ x, const P* __restrict__ y,
     }
 }
 
+/* Permutes the SoA arrays into sorted order.  Each thread handles GATHER_ILP outputs and
+ * issues all their (scattered) loads before any store, so that many reads are in flight. */
+constexpr int GATHER_ILP = 4;
+
 template <class P, class V>
-__global__ void k_gather(const uint32_t* __restrict__ perm, int64_t n,
+__global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ perm, int64_t n,
                          const P* __restrict__ x0, const P* __restrict__ y0,
                          const P* __restrict__ z0, const V* __restrict__ u0,
                          const V* __restrict__ v0, const V* __restrict__ w0,
@@ -71,17 +75,46 @@ __global__ void k_gather(const uint32_t* __restrict__ perm, int64_t n,
                          V* __restrict__ u1, V* __restrict__ v1, V* __restrict__ w1,
                          V* __restrict__ d1, int32_t* __restrict__ id1)
 {
-    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
-         p += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t s = perm[p];
-        x1[p] = x0[s];
-        y1[p] = y0[s];
-        z1[p] = z0[s];
-        u1[p] = u0[s];
-        v1[p] = v0[s];
-        w1[p] = w0[s];
-        d1[p] = d0[s];
-        id1[p] = id0[s];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * GATHER_ILP;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x * GATHER_ILP + threadIdx.x; base < n;
+         base += stride) {
+        int64_t src[GATHER_ILP];
+        P x[GATHER_ILP], y[GATHER_ILP], z[GATHER_ILP];
+        V u[GATHER_ILP], v[GATHER_ILP], w[GATHER_ILP], dd[GATHER_ILP];
+        int32_t id[GATHER_ILP];
+#pragma unroll
+        for (int k = 0; k < GATHER_ILP; ++k) {
+            const int64_t p = base + (int64_t)k * blockDim.x;
+            src[k] = p < n ? (int64_t)__ldcs(perm + p) : -1;
+        }
+#pragma unroll
+        for (int k = 0; k < GATHER_ILP; ++k) {
+            if (src[k] >= 0) {
+                const int64_t s = src[k];
+                x[k] = __ldg(x0 + s);
+                y[k] = __ldg(y0 + s);
+                z[k] = __ldg(z0 + s);
+                u[k] = __ldg(u0 + s);
+                v[k] = __ldg(v0 + s);
+                w[k] = __ldg(w0 + s);
+                dd[k] = __ldg(d0 + s);
+                id[k] = __ldg(id0 + s);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < GATHER_ILP; ++k) {
+            const int64_t p = base + (int64_t)k * blockDim.x;
+            if (src[k] >= 0) {
+                __stcs(x1 + p, x[k]);
+                __stcs(y1 + p, y[k]);
+                __stcs(z1 + p, z[k]);
+                __stcs(u1 + p, u[k]);
+                __stcs(v1 + p, v[k]);
+                __stcs(w1 + p, w[k]);
+                __stcs(d1 + p, dd[k]);
+                __stcs(id1 + p, id[k]);
+            }
+        }
     }
 }
 
@@ -177,7 +210,9 @@ cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& me
     e = cub::DeviceRadixSort::SortPairs(b.temp, bytes, b.keys[0], b.keys[1], b.perm[0],
                                         b.perm[1], (int)n, 0, key_bits, s);
     if (e != cudaSuccess) return e;
-    k_gather<P, V><<<grid_for(n), 256, 0, s>>>(b.perm[1], n, b.x[cur], b.y[cur], b.z[cur],
+    int64_t gblocks = (n + 256 * GATHER_ILP - 1) / (256 * GATHER_ILP);
+    if (gblocks > 148 * 64) gblocks = 148 * 64;
+    k_gather<P, V><<<(int)gblocks, 256, 0, s>>>(b.perm[1], n, b.x[cur], b.y[cur], b.z[cur],
                                                b.u[cur], b.v[cur], b.w[cur], b.d[cur],
                                                b.id[cur], b.x[o], b.y[o], b.z[o], b.u[o],
                                                b.v[o], b.w[o], b.d[o], b.id[o]);

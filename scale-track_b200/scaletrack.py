@@ -28,7 +28,8 @@ ST_ERR_OUT_OF_MEMORY = 6
 DRAG = {"stokes_implicit": 0, "schiller_naumann": 1, "sn_explicit": 1}
 PRECISION = {"fp32": 0, "mixed": 1, "fp64": 2}
 DEPOSIT = {"deterministic": 0, "atomic": 1}
-KERNEL_KINDS = {"step": 0, "finalize": 1, "sort": 2, "probe": 3, "other": 4}
+KERNEL_KINDS = {"step": 0, "finalize": 1, "sort": 2, "probe": 3, "other": 4,
+                "adj_forward": 5, "adj_reverse": 6}
 
 # every symbol include/scaletrack.h declares
 EXPORTS = [
@@ -38,7 +39,8 @@ EXPORTS = [
     "st_source_device", "st_synchronize", "st_get_stream", "st_set_stream",
     "st_profile_enable", "st_profile_read", "st_launch_count", "st_setup", "st_default_handle",
     "st_allocate_array", "st_evolve_cloud", "st_finalize", "st_step_noalloc",
-    "st_noalloc_max_cells",
+    "st_noalloc_max_cells", "st_mean_source_forward", "st_mean_source_pullback",
+    "st_graph_capture", "st_graph_launch", "st_graph_release", "st_autotune",
 ]
 
 
@@ -62,6 +64,17 @@ class Params(ctypes.Structure):
         ("block_size", ctypes.c_int32), ("grid_blocks", ctypes.c_int32),
         ("drag_multiplier", ctypes.c_double), ("diameter_scale", ctypes.c_double),
     ]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("block_size", ctypes.c_int32), ("grid_blocks", ctypes.c_int32),
+                ("sort_interval", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("ms_per_step", ctypes.c_double)]
+
+
+class AdjointDesc(ctypes.Structure):
+    _fields_ = [("n_steps", ctypes.c_int32), ("checkpoint_interval", ctypes.c_int32),
+                ("dt", ctypes.c_double), ("fluid_scale", ctypes.POINTER(ctypes.c_double))]
 
 
 _lib = None
@@ -111,6 +124,16 @@ def lib():
         "st_step_noalloc": ([P(Params), P(MeshDesc), ctypes.c_int64] + [ctypes.c_void_p] * 9 +
                             [ctypes.c_double, ctypes.c_double, ctypes.c_void_p], ctypes.c_int),
         "st_noalloc_max_cells": ([], ctypes.c_int64),
+        "st_graph_capture": ([c_h, ctypes.c_int, ctypes.c_double, ctypes.c_void_p],
+                             ctypes.c_int),
+        "st_graph_launch": ([c_h], ctypes.c_int),
+        "st_graph_release": ([c_h], ctypes.c_int),
+        "st_autotune": ([c_h, ctypes.c_double, ctypes.c_int, P(TuneResult)], ctypes.c_int),
+        "st_mean_source_forward": ([c_h, ctypes.c_int, P(AdjointDesc), ctypes.c_void_p],
+                                   ctypes.c_int),
+        "st_mean_source_pullback": ([c_h, ctypes.c_int, P(AdjointDesc), ctypes.c_void_p,
+                                     P(ctypes.c_double), P(ctypes.c_double), ctypes.c_void_p],
+                                    ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -266,6 +289,51 @@ class ParcelTracker:
 
     def launch_count(self):
         return int(lib().st_launch_count(self._h))
+
+    def graph_capture(self, n_steps, dt, fluid_scale=None):
+        fs = None if fluid_scale is None else np.ascontiguousarray(fluid_scale, dtype=np.float64)
+        _check(lib().st_graph_capture(self._h, n_steps, dt, _dptr(fs)))
+
+    def graph_launch(self):
+        _check(lib().st_graph_launch(self._h))
+
+    def graph_release(self):
+        _check(lib().st_graph_release(self._h))
+
+    def autotune(self, dt, trial_steps=40):
+        r = TuneResult()
+        _check(lib().st_autotune(self._h, dt, trial_steps, ctypes.byref(r)))
+        return dict(block_size=r.block_size, grid_blocks=r.grid_blocks,
+                    sort_interval=r.sort_interval, ms_per_step=r.ms_per_step)
+
+    def _adj_desc(self, n_steps, checkpoint_interval, dt, fluid_scale):
+        fs = None
+        if fluid_scale is not None:
+            fs = np.ascontiguousarray(fluid_scale, dtype=np.float64)
+            assert fs.shape == (n_steps,)
+        desc = AdjointDesc(n_steps, checkpoint_interval, dt,
+                           None if fs is None else fs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return desc, fs
+
+    def mean_source_forward(self, n_steps, checkpoint_interval, dt, fluid_scale=None, cloud=0):
+        """Sbar = (1/T) sum of the per-step sources over T steps from the current state (the
+        state is not modified); keeps the checkpoints for mean_source_pullback."""
+        desc, keep = self._adj_desc(n_steps, checkpoint_interval, dt, fluid_scale)
+        S = np.empty((self.ncells, 3))
+        _check(lib().st_mean_source_forward(self._h, cloud, ctypes.byref(desc), _dptr(S)))
+        return S
+
+    def mean_source_pullback(self, cotangent, n_steps, checkpoint_interval, dt,
+                             fluid_scale=None, cloud=0, want_v0=True):
+        """Pull-back of the last mean_source_forward: (dJ/dalpha, dJ/ds, dJ/dv0 [3, n])."""
+        desc, keep = self._adj_desc(n_steps, checkpoint_interval, dt, fluid_scale)
+        cot = np.ascontiguousarray(cotangent, dtype=np.float64).reshape(self.ncells, 3)
+        da = ctypes.c_double()
+        ds = ctypes.c_double()
+        dv0 = np.empty((3, self.num_parcels(cloud))) if want_v0 else None
+        _check(lib().st_mean_source_pullback(self._h, cloud, ctypes.byref(desc), _dptr(cot),
+                                             ctypes.byref(da), ctypes.byref(ds), _dptr(dv0)))
+        return float(da.value), float(ds.value), dv0
 
 
 # ---------------------------------------------------------------------------------------

@@ -29,6 +29,15 @@ CONFIGS = {
     # time-varying field
     "c1_mixed_128": dict(n=128, nparcels=10_000_000, seed=0, precision="mixed", steps=500,
                          U0=1.0, time_varying=True, sort_interval=20),
+    # 64 clouds, sizes log-uniform in [1e3, 2e6] (seed 2), per-cloud median diameter uniform
+    # in [5, 50] um, one shared 64^3 mesh, own source per cloud, 100 steps
+    "c3_clouds_64": dict(n=64, nclouds=64, seed=2, precision="mixed", steps=100,
+                         size_min=1_000, size_max=2_000_000, dmed_min=5e-6, dmed_max=50e-6),
+    # adjoint: 128^3 hex, 1e6 parcels, 200 steps, checkpoints every 20 steps; the target
+    # source comes from a forward run with drag multiplier 1.1 and diameters x 0.95
+    "c4_adjoint_128": dict(n=128, nparcels=1_000_000, seed=3, precision="mixed", steps=200,
+                           checkpoint=20, U0=1.0, time_varying=False, target_alpha=1.1,
+                           target_dscale=0.95),
 }
 
 
@@ -60,6 +69,15 @@ def parcels(nparcels, seed, L=L_BOX, d_median=20e-6, sigma=0.3, dtype_v=np.float
     d = (d_median * np.exp(sigma * rng.standard_normal(nparcels))).astype(dtype_v)
     uvw = np.zeros((3, nparcels), dtype=np.float64)
     return xyz, uvw, d.astype(np.float64)
+
+
+def cloud_sizes(cfg):
+    """Cloud sizes log-uniform in [size_min, size_max] and per-cloud median diameters."""
+    rng = np.random.default_rng(cfg["seed"])
+    sizes = np.exp(rng.uniform(np.log(cfg["size_min"]), np.log(cfg["size_max"]),
+                               cfg["nclouds"])).astype(np.int64)
+    dmed = rng.uniform(cfg["dmed_min"], cfg["dmed_max"], cfg["nclouds"])
+    return sizes, dmed
 
 
 def fluid_scale(step, dt=DT, time_varying=True):
