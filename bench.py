@@ -422,8 +422,8 @@ def run_clouds(st, torch, local, dev):
     n = c["n"]
     U = workload.tgv_field(n, dtype=np.float32)
     prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
-                    drag_model="schiller_naumann", precision="mixed", n_substeps=1,
-                    n_clouds=c["nclouds"], sort_interval=20)
+                    drag_model="schiller_naumann", precision="mixed",
+                    n_substeps=c["substeps"], n_clouds=c["nclouds"], sort_interval=20)
     total = int(sizes.sum())
     with st.ParcelTracker(prm, st.mesh_desc(n, 0.0, workload.L_BOX), local) as h:
         for k in range(c["nclouds"]):
@@ -458,7 +458,8 @@ def run_clouds(st, torch, local, dev):
         h.synchronize()
     return {"workload": "BASELINE config 3: 64 clouds, sizes log-uniform in [1e3, 2e6] (seed 2), "
                         "median diameter per cloud uniform in [5, 50] um, 64^3 mesh, one "
-                        "source per cloud, mixed precision, one launch per step",
+                        "source per cloud, mixed precision, 10 substeps inside one launch per "
+                        "step",
             "parcels": total, "steps": steps, "autotune": tune,
             "particle_steps_per_s_graph": total * steps / (ms_graph / 1e3),
             "particle_steps_per_s_launches": total * steps / (ms_plain / 1e3),

@@ -30,8 +30,10 @@ CONFIGS = {
     "c1_mixed_128": dict(n=128, nparcels=10_000_000, seed=0, precision="mixed", steps=500,
                          U0=1.0, time_varying=True, sort_interval=20),
     # 64 clouds, sizes log-uniform in [1e3, 2e6] (seed 2), per-cloud median diameter uniform
-    # in [5, 50] um, one shared 64^3 mesh, own source per cloud, 100 steps
-    "c3_clouds_64": dict(n=64, nclouds=64, seed=2, precision="mixed", steps=100,
+    # in [5, 50] um, one shared 64^3 mesh, own source per cloud, 100 steps.  Ten substeps of
+    # dt/10 (the reference's nSteps): a 2 um parcel has tau_p ~ 1.2e-5 s, and explicit Euler
+    # needs dt_sub / tau_p < 2
+    "c3_clouds_64": dict(n=64, nclouds=64, seed=2, precision="mixed", steps=100, substeps=10,
                          size_min=1_000, size_max=2_000_000, dmed_min=5e-6, dmed_max=50e-6),
     # adjoint: 128^3 hex, 1e6 parcels, 200 steps, checkpoints every 20 steps; the target
     # source comes from a forward run with drag multiplier 1.1 and diameters x 0.95

@@ -25,9 +25,9 @@ def clouds(k=5, seed=2):
     return out
 
 
-def params(k, sort_interval=0):
+def params(k, sort_interval=0, nsub=10):
     return st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
-                     drag_model="schiller_naumann", precision="mixed", n_substeps=1,
+                     drag_model="schiller_naumann", precision="mixed", n_substeps=nsub,
                      n_clouds=k, sort_interval=sort_interval)
 
 
@@ -68,7 +68,7 @@ def test_multi_cloud_against_oracle_per_cloud():
     U = workload.tgv_field(N, dtype=np.float32)
     g = run(6, cl, U, 4, graph=True)
     cfg = oracle.make_cfg(N, 0.0, workload.L_BOX, workload.MU_F, workload.RHO_F,
-                          workload.RHO_P, drag="sn_explicit", precision="mixed", n_substeps=1)
+                          workload.RHO_P, drag="sn_explicit", precision="mixed", n_substeps=10)
     for c, (xyz, uvw, d) in enumerate(cl):
         r = oracle.run(cfg, xyz, uvw, d, U.astype(np.float64), 4, workload.DT)
         assert np.array_equal(g[c][0], r["xyz"])
