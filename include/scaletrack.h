@@ -136,6 +136,40 @@ ST_API int st_synchronize(st_handle* h);
 ST_API void* st_get_stream(st_handle* h);
 ST_API int st_set_stream(st_handle* h, void* stream);
 
+/* ---- unstructured tetrahedral meshes (no counterpart in the reference) -------------- */
+/* A conforming tet mesh filling the box [origin, ending] (planar walls).  Face f of a tet is
+ * the face opposite its local vertex f; neighbors[4t + f] is the tet across it, or -1 on the
+ * boundary.  Parcels carry their owning tet; after each position update a greedy walk moves
+ * across the face with the largest positive signed distance (planes in FP64 from the face's
+ * vertices taken in increasing id order, ties to the face opposite the smaller vertex id)
+ * until the position is inside.  A position outside the box keeps its old
+ * coordinate on that axis and mirrors the old velocity component, as on cuboid meshes
+ * (A:1313-1329).  Deposits go to the tet of the last velocity sample.  Mixed and FP64
+ * precision only (positions in FP64). */
+typedef struct st_tet_mesh_desc {
+    int64_t n_vertices;
+    const double* vertices;    /* [n_vertices][3] (host) */
+    int64_t n_tets;
+    const int32_t* tets;       /* [n_tets][4] vertex ids (host) */
+    const int32_t* neighbors;  /* [n_tets][4] tet across face f, -1 on the boundary (host) */
+    double origin[3];          /* box walls */
+    double ending[3];
+    int32_t hop_limit;         /* walk hops per substep before a parcel counts as lost; 0 = 64 */
+    int32_t pad;
+} st_tet_mesh_desc;
+/* Like st_create for a tet mesh; cells are tets (st_num_cells = n_tets, U and the source
+ * are [n_tets][3]).  The mesh arrays are copied to the device. */
+ST_API int st_create_tet(const st_params* p, const st_tet_mesh_desc* mesh, int device,
+                         st_handle** out);
+/* Like st_set_parcels, with a starting tet per parcel (`hint`, [n], may be NULL for tet 0)
+ * from which the walk looks for the owning tet.  st_set_parcels on a tet handle walks from
+ * tet 0. */
+ST_API int st_set_parcels_tet(st_handle* h, int cloud, int64_t n, const double* xyz,
+                              const double* uvw, const double* d, const int32_t* hint);
+/* Walk lengths of every substep since the last reset: out[k] = substeps whose walk took k
+ * hops (k < 7), out[7] = 7 or more.  Synchronises the stream. */
+ST_API int st_tet_hop_histogram(st_handle* h, uint64_t out[8], int reset);
+
 /* ---- CUDA-graph replay and autotuning ---------------------------------------------- */
 /* Captures n_steps calls of st_step (dt, fluid_scale[k] or 1) into a CUDA graph on the
  * handle's stream; st_graph_launch replays them (asynchronously), which removes the host

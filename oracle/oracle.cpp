@@ -18,6 +18,7 @@
 
 #include "step_oracle.hpp"
 #include "adjoint_oracle.hpp"
+#include "tet_oracle.hpp"
 
 using namespace st_oracle;
 
@@ -437,6 +438,141 @@ int oracle_adjoint(const oracle_cfg* cfg, int64_t np, const double* xyz, const d
     default:
         return -2;
     }
+}
+
+}  // extern "C"
+
+namespace {
+
+template <class V>
+int tet_run(const oracle_cfg* cfg, const TetMesh& mesh, int64_t np, double* xyz, double* uvw,
+            const double* d, int32_t* cells, const double* U, int nsteps, double dt,
+            const double* fscale, double* src_seq, double* src_quant, int32_t* scale_io,
+            int64_t* stats, int64_t* hop_hist, int hop_limit)
+{
+    Params<double, V> pr = make_params<double, V>(cfg->n, cfg->origin, cfg->ending, cfg->mu_c,
+                                                  cfg->rho_c, cfg->rho_d, cfg->drag,
+                                                  cfg->n_substeps, cfg->drag_multiplier,
+                                                  cfg->diameter_scale);
+    const int64_t nC = mesh.nt;
+    const double dtP = dt / (double)cfg->n_substeps;
+    const V dtV = (V)dtP;
+    const bool quant = src_quant != nullptr;
+    const int limbs = cfg->quant_limbs == 2 ? 2 : 1;
+    std::vector<int64_t> q1(limbs == 1 && quant ? 3 * nC : 0), hi(limbs == 2 && quant ? 3 * nC : 0);
+    std::vector<uint64_t> lo(limbs == 2 && quant ? 3 * nC : 0);
+    std::vector<double> seq(src_seq ? 3 * nC : 0);
+    const int H = quant_headroom(limbs, std::max<int64_t>(2, np * (int64_t)cfg->n_substeps));
+    int L = scale_io ? *scale_io : INT_MIN;
+    int64_t lost = 0, ovf = 0;
+    std::vector<double> P(3 * np);
+    std::vector<V> Vv(3 * np), D(np);
+    for (int64_t i = 0; i < np; ++i) {
+        for (int c = 0; c < 3; ++c) {
+            P[3 * i + c] = xyz[c * np + i];
+            Vv[3 * i + c] = (V)uvw[c * np + i];
+        }
+        D[i] = (V)d[i];
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        const V fs = fscale ? (V)fscale[s] : (V)1;
+        if (quant && L == INT_MIN) {
+            Acc pa;
+            pa.limbs = limbs; pa.L = 0; pa.H = 1 << 20;
+            AccSink<V> sk(&pa, true);
+            for (int64_t i = 0; i < np; ++i) {
+                double x[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
+                V v[3] = {Vv[3 * i], Vv[3 * i + 1], Vv[3 * i + 2]};
+                int32_t c = cells[i];
+                evolve_parcel_tet<V>(mesh, pr, dtP, dtV, U, fs, x, v, c, D[i], hop_limit, sk,
+                                     nullptr);
+            }
+            L = (sk.emax == EXP_NONE) ? -H : sk.emax - H;
+        }
+        Acc acc;
+        acc.limbs = limbs; acc.L = L; acc.H = H;
+        if (src_seq) { std::fill(seq.begin(), seq.end(), 0.0); acc.seq = seq.data(); }
+        if (quant) {
+            if (limbs == 1) { std::fill(q1.begin(), q1.end(), 0); acc.q1 = q1.data(); }
+            else {
+                std::fill(hi.begin(), hi.end(), 0); std::fill(lo.begin(), lo.end(), 0);
+                acc.hi = hi.data(); acc.lo = lo.data();
+            }
+        }
+        AccSink<V> sk(&acc, quant);
+        for (int64_t i = 0; i < np; ++i) {
+            if (!evolve_parcel_tet<V>(mesh, pr, dtP, dtV, U, fs, &P[3 * i], &Vv[3 * i], cells[i],
+                                      D[i], hop_limit, sk, hop_hist))
+                ++lost;
+        }
+        ovf += sk.overflow;
+        if (s == nsteps - 1 && quant) {
+            for (int64_t j = 0; j < 3 * nC; ++j) {
+                double v;
+                if (limbs == 1) v = (double)q1[j];
+                else {
+                    int64_t h = hi[j] + (int64_t)(lo[j] >> 32);
+                    v = (double)h * 4294967296.0 + (double)(lo[j] & 0xffffffffULL);
+                }
+                src_quant[j] = ldexp2(v, L);
+            }
+        }
+        if (quant && sk.emax != EXP_NONE) L = sk.emax - H;
+    }
+    if (src_seq) std::memcpy(src_seq, seq.data(), sizeof(double) * 3 * nC);
+    if (scale_io) *scale_io = L;
+    for (int64_t i = 0; i < np; ++i)
+        for (int c = 0; c < 3; ++c) {
+            xyz[c * np + i] = P[3 * i + c];
+            uvw[c * np + i] = (double)Vv[3 * i + c];
+        }
+    if (stats) { stats[0] = lost; stats[1] = ovf; stats[2] = H; }
+    return (lost ? 1 : 0) | (ovf ? 2 : 0);
+}
+
+}  // namespace
+
+extern "C" {
+
+/* Steps on a tetrahedral mesh (face walk).  cells [np]: tet of each parcel, in/out.
+ * box from cfg->origin/ending; precision 1 (mixed) or 2 (FP64).  hop_hist[8]: histogram
+ * of walk lengths (hops per substep, last bin 7+), or NULL.  Returns as oracle_run. */
+int oracle_tet_run(const oracle_cfg* cfg, int64_t nv, const double* verts, int64_t nt,
+                   const int32_t* tets, const int32_t* nbr, int64_t np, double* xyz,
+                   double* uvw, const double* d, int32_t* cells, const double* U, int nsteps,
+                   double dt, const double* fscale, double* src_seq, double* src_quant,
+                   int32_t* scale_io, int64_t* stats, int64_t* hop_hist, int hop_limit)
+{
+    std::vector<int32_t> ct(4 * nt), cn(4 * nt);
+    canonical_tets(nt, tets, nbr, ct.data(), cn.data());
+    TetMesh m;
+    m.nv = nv; m.nt = nt; m.verts = verts; m.tets = ct.data(); m.nbr = cn.data();
+    for (int a = 0; a < 3; ++a) { m.origin[a] = cfg->origin[a]; m.ending[a] = cfg->ending[a]; }
+    if (cfg->precision == 1)
+        return tet_run<float>(cfg, m, np, xyz, uvw, d, cells, U, nsteps, dt, fscale, src_seq,
+                              src_quant, scale_io, stats, hop_hist, hop_limit);
+    if (cfg->precision == 2)
+        return tet_run<double>(cfg, m, np, xyz, uvw, d, cells, U, nsteps, dt, fscale, src_seq,
+                               src_quant, scale_io, stats, hop_hist, hop_limit);
+    return -2;
+}
+
+/* Walk from start[i] to the tet containing xyz[:, i]; status[i] as WALK_*. */
+int oracle_tet_locate(int64_t nv, const double* verts, int64_t nt, const int32_t* tets,
+                      const int32_t* nbr, int64_t np, const double* xyz, const int32_t* start,
+                      int32_t* cells, int32_t* status, int hop_limit)
+{
+    std::vector<int32_t> ct(4 * nt), cn(4 * nt);
+    canonical_tets(nt, tets, nbr, ct.data(), cn.data());
+    TetMesh m;
+    m.nv = nv; m.nt = nt; m.verts = verts; m.tets = ct.data(); m.nbr = cn.data();
+    for (int64_t i = 0; i < np; ++i) {
+        double x[3] = {xyz[i], xyz[np + i], xyz[2 * np + i]};
+        int st = 0, hops = 0;
+        cells[i] = tet_walk(m, start[i], x, hop_limit, st, hops);
+        status[i] = st;
+    }
+    return 0;
 }
 
 }  // extern "C"

@@ -67,6 +67,17 @@ def lib():
             P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double),
             P(ctypes.c_double), P(ctypes.c_int32), P(ctypes.c_uint8), ctypes.c_int]
         L.oracle_adjoint.restype = ctypes.c_int
+        L.oracle_tet_run.argtypes = [
+            P(OracleCfg), ctypes.c_int64, P(ctypes.c_double), ctypes.c_int64, P(ctypes.c_int32),
+            P(ctypes.c_int32), ctypes.c_int64, P(ctypes.c_double), P(ctypes.c_double),
+            P(ctypes.c_double), P(ctypes.c_int32), P(ctypes.c_double), ctypes.c_int,
+            ctypes.c_double, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double),
+            P(ctypes.c_int32), P(ctypes.c_int64), P(ctypes.c_int64), ctypes.c_int]
+        L.oracle_tet_run.restype = ctypes.c_int
+        L.oracle_tet_locate.argtypes = [
+            ctypes.c_int64, P(ctypes.c_double), ctypes.c_int64, P(ctypes.c_int32),
+            P(ctypes.c_int32), ctypes.c_int64, P(ctypes.c_double), P(ctypes.c_int32),
+            P(ctypes.c_int32), P(ctypes.c_int32), ctypes.c_int]
         _lib = L
     return _lib
 
@@ -192,3 +203,53 @@ def adjoint(cfg, xyz, uvw, d, U, T, dt, fscale=None, cotangent=None, target=None
                               _ptr(bounce, ctypes.c_uint8), 1 if replay else 0)
     return dict(mean_src=mean.reshape(ncells, 3), J=float(J[0]), dalpha=float(da[0]),
                 dscale=float(ds[0]), dv0=dv0, frozen=(cells, bounce), status=st)
+
+
+def tet_run(cfg, mesh, xyz, uvw, d, cells, U, nsteps, dt, fscale=None, want_seq=True,
+            want_quant=True, scale=INT_MIN, hop_limit=64):
+    """Steps on a tet mesh (verts, tets, nbrs); cells [np] start tets.  Returns dict(xyz, uvw,
+    cells, src_seq, src_quant, scale, lost, overflow, hop_hist, status)."""
+    verts, tets, nbrs = (np.ascontiguousarray(mesh[0], dtype=np.float64),
+                         np.ascontiguousarray(mesh[1], dtype=np.int32),
+                         np.ascontiguousarray(mesh[2], dtype=np.int32))
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+    uvw = np.ascontiguousarray(uvw, dtype=np.float64).copy()
+    d = np.ascontiguousarray(d, dtype=np.float64)
+    cells = np.ascontiguousarray(cells, dtype=np.int32).copy()
+    U = np.ascontiguousarray(U, dtype=np.float64).reshape(-1)
+    nt = tets.shape[0]
+    fs = None if fscale is None else np.ascontiguousarray(fscale, dtype=np.float64)
+    src_seq = np.zeros(3 * nt) if want_seq else None
+    src_q = np.zeros(3 * nt) if want_quant else None
+    sc = np.array([scale], dtype=np.int32)
+    stats = np.zeros(3, dtype=np.int64)
+    hist = np.zeros(8, dtype=np.int64)
+    st = lib().oracle_tet_run(ctypes.byref(cfg), verts.shape[0], _ptr(verts, ctypes.c_double),
+                              nt, _ptr(tets, ctypes.c_int32), _ptr(nbrs, ctypes.c_int32),
+                              d.shape[0], _ptr(xyz, ctypes.c_double), _ptr(uvw, ctypes.c_double),
+                              _ptr(d, ctypes.c_double), _ptr(cells, ctypes.c_int32),
+                              _ptr(U, ctypes.c_double), nsteps, dt, _ptr(fs, ctypes.c_double),
+                              _ptr(src_seq, ctypes.c_double), _ptr(src_q, ctypes.c_double),
+                              _ptr(sc, ctypes.c_int32), _ptr(stats, ctypes.c_int64),
+                              _ptr(hist, ctypes.c_int64), hop_limit)
+    return dict(xyz=xyz, uvw=uvw, cells=cells,
+                src_seq=None if src_seq is None else src_seq.reshape(nt, 3),
+                src_quant=None if src_q is None else src_q.reshape(nt, 3), scale=int(sc[0]),
+                lost=int(stats[0]), overflow=int(stats[1]), hop_hist=hist, status=st)
+
+
+def tet_locate(mesh, xyz, start, hop_limit=1024):
+    verts, tets, nbrs = (np.ascontiguousarray(mesh[0], dtype=np.float64),
+                         np.ascontiguousarray(mesh[1], dtype=np.int32),
+                         np.ascontiguousarray(mesh[2], dtype=np.int32))
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    start = np.ascontiguousarray(start, dtype=np.int32)
+    npcl = xyz.shape[1]
+    cells = np.zeros(npcl, dtype=np.int32)
+    status = np.zeros(npcl, dtype=np.int32)
+    lib().oracle_tet_locate(verts.shape[0], _ptr(verts, ctypes.c_double), tets.shape[0],
+                            _ptr(tets, ctypes.c_int32), _ptr(nbrs, ctypes.c_int32), npcl,
+                            _ptr(xyz, ctypes.c_double), _ptr(start, ctypes.c_int32),
+                            _ptr(cells, ctypes.c_int32), _ptr(status, ctypes.c_int32),
+                            hop_limit)
+    return cells, status

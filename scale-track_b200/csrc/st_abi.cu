@@ -25,6 +25,7 @@
 #include <vector>
 #include <map>
 #include <algorithm>
+#include <type_traits>
 
 #include <cuda_runtime.h>
 
@@ -73,6 +74,7 @@ struct CloudBufs {
     void* w[2] = {nullptr, nullptr};
     void* d[2] = {nullptr, nullptr};
     int32_t* id[2] = {nullptr, nullptr};
+    int32_t* cell[2] = {nullptr, nullptr};  /* owning tet (tet meshes) */
     uint32_t* keys[2] = {nullptr, nullptr};
     uint32_t* perm[2] = {nullptr, nullptr};
     void* temp = nullptr;
@@ -149,6 +151,13 @@ struct st_handle {
     void* dstage = nullptr;
     size_t stage_bytes = 0;
     AdjTape adj;
+    /* unstructured tetrahedral mesh */
+    bool tet = false;
+    TetMeshK tmesh = {};
+    double* d_verts = nullptr;
+    int32_t* d_tets = nullptr;
+    int32_t* d_nbr = nullptr;
+    unsigned long long* d_hops = nullptr;   /* walk-length histogram [8] */
     /* CUDA-graph replay of a step sequence */
     bool capturing = false;
     int cap_parity = 0;          /* which of the two descriptor arrays the captured step uses */
@@ -302,6 +311,7 @@ SortBufs<P, V> sort_bufs(CloudBufs& c)
         b.w[k] = (V*)c.w[k];
         b.d[k] = (V*)c.d[k];
         b.id[k] = c.id[k];
+        b.cell[k] = c.cell[k];
         b.keys[k] = c.keys[k];
         b.perm[k] = c.perm[k];
     }
@@ -330,6 +340,7 @@ int upload_clouds(st_handle* h)
         k.tile0 = tiles;
         k.acc = h->dacc + (int64_t)c * h->stride * h->limbs;
         k.src = h->dsrc + (int64_t)c * h->stride;
+        k.cell = b.cell[b.cur];
         tiles += (b.n + WARP_TILE - 1) / WARP_TILE;
     }
     h->total_tiles = tiles;
@@ -362,10 +373,16 @@ int do_sort_all(st_handle* h)
     return ST_OK;
 }
 
+template <class V>
+int do_step_tet(st_handle* h, double dt, double fscale);
+
 template <class P, class V>
 int do_step(st_handle* h, double dt, double fscale)
 {
     int rc;
+    if constexpr (std::is_same<P, double>::value) {
+        if (h->tet) return do_step_tet<V>(h, dt, fscale);
+    }
     if (!h->capturing && h->clouds_dirty && (rc = upload_clouds<P, V>(h)) != ST_OK) return rc;
     StepArgs<P, V> a;
     a.mesh = mesh_k<P>(h);
@@ -432,9 +449,80 @@ int do_step(st_handle* h, double dt, double fscale)
     return ST_OK;
 }
 
+/* The step on a tetrahedral mesh: same launch sequence as do_step with the face-walk
+ * kernel (st_tet.cu). */
+template <class V>
+int do_step_tet(st_handle* h, double dt, double fscale)
+{
+    int rc;
+    if (!h->capturing && h->clouds_dirty && (rc = upload_clouds<double, V>(h)) != ST_OK) return rc;
+    TetStepArgs<V> a;
+    a.mesh = h->tmesh;
+    a.phys = phys_k<V>(h);
+    a.dtP = dt / (double)h->p.n_substeps;
+    a.dtV = (V)a.dtP;
+    a.fscale = (V)fscale;
+    a.nclouds = h->p.n_clouds;
+    a.U = (const V*)h->dU;
+    a.clouds = h->capturing
+                   ? (const CloudK<double, V>*)h->dclouds2 + (size_t)h->cap_parity * h->p.n_clouds
+                   : (const CloudK<double, V>*)h->dclouds;
+    a.ctl = h->dctl;
+    a.total_tiles = h->total_tiles;
+    a.hop_hist = h->d_hops;
+    if (a.total_tiles == 0) return ST_OK;
+    int grid = h->grid;
+    const int64_t need = (a.total_tiles + h->block / 32 - 1) / (h->block / 32);
+    if (grid > need) grid = (int)need;
+    if (grid < 1) grid = 1;
+    const bool det = (h->dep == DEP_DET1 || h->dep == DEP_DET2);
+    if (det && (h->need_probe || dt != h->last_dt)) {
+        {
+            ProfScope ps(h, ST_KERNEL_PROBE);
+            CK(launch_step_tet<V>(a, DEP_PROBE, grid, h->block, h->stream));
+        }
+        {
+            ProfScope ps(h, ST_KERNEL_OTHER);
+            CK(launch_set_scale(h->dctl, h->p.n_clouds, h->stream));
+        }
+        h->launches += 2;
+        h->need_probe = false;
+    }
+    h->last_dt = dt;
+    if (!det) {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        CK(launch_zero_f64(h->dsrc, (int64_t)h->p.n_clouds * h->stride, h->stream));
+        h->launches += 1;
+    }
+    {
+        ProfScope ps(h, ST_KERNEL_STEP);
+        CK(launch_step_tet<V>(a, h->dep, grid, h->block, h->stream));
+        h->launches += 1;
+    }
+    if (det) {
+        int64_t gx = (h->stride / COMP_ALIGN + 255) / 256;
+        int64_t cap = (148 * 8 + h->p.n_clouds - 1) / h->p.n_clouds;
+        if (gx > cap) gx = cap;
+        if (gx < 1) gx = 1;
+        {
+            ProfScope ps(h, ST_KERNEL_FINALIZE);
+            CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter,
+                               h->p.n_clouds, h->stride, (int)gx, h->stream));
+            h->launches += 1;
+        }
+        CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * h->p.n_clouds * h->limbs * 8,
+                           h->stream));
+    }
+    h->steps += 1;
+    h->steps_since_sort += 1;
+    if (h->p.sort_interval > 0 && h->steps_since_sort >= h->p.sort_interval)
+        return do_sort_all<double, V>(h);
+    return ST_OK;
+}
+
 template <class P, class V>
 int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
-                   const double* d)
+                   const double* d, const int32_t* hint)
 {
     CloudBufs& c = h->clouds[cloud];
     if (n > c.cap) {
@@ -448,8 +536,11 @@ int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
             if (c.id[k]) cudaFree(c.id[k]);
             if (c.keys[k]) cudaFree(c.keys[k]);
             if (c.perm[k]) cudaFree(c.perm[k]);
+            if (c.cell[k]) cudaFree(c.cell[k]);
             c.id[k] = nullptr;
+            c.cell[k] = nullptr;
             c.keys[k] = c.perm[k] = nullptr;
+            if (h->tet) CK(cudaMalloc(&c.cell[k], (size_t)n * sizeof(int32_t)));
             CK(cudaMalloc(&c.id[k], (size_t)n * sizeof(int32_t)));
             CK(cudaMalloc(&c.keys[k], (size_t)n * sizeof(uint32_t)));
             CK(cudaMalloc(&c.perm[k], (size_t)n * sizeof(uint32_t)));
@@ -469,19 +560,35 @@ int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
         for (int a = 0; a < 3; ++a) {
             for (int64_t i = 0; i < n; ++i) hp[i] = (P)xyz[a * n + i];
             void* dst = a == 0 ? c.x[0] : (a == 1 ? c.y[0] : c.z[0]);
-            CK(cudaMemcpy(dst, hp.data(), n * sizeof(P), cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync(dst, hp.data(), n * sizeof(P), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));   /* hp is reused */
         }
         for (int a = 0; a < 4; ++a) {
             const double* srcp = a < 3 ? uvw + a * n : d;
             for (int64_t i = 0; i < n; ++i) hv[i] = (V)srcp[i];
             void* dst = a == 0 ? c.u[0] : (a == 1 ? c.v[0] : (a == 2 ? c.w[0] : c.d[0]));
-            CK(cudaMemcpy(dst, hv.data(), n * sizeof(V), cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync(dst, hv.data(), n * sizeof(V), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));   /* hv is reused */
         }
         for (int64_t i = 0; i < n; ++i) hid[i] = (int32_t)i;
-        CK(cudaMemcpy(c.id[0], hid.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        /* every upload is ordered on the handle's stream: a plain cudaMemcpy runs on the
+         * legacy stream, which the handle's non-blocking stream does not wait for */
+        CK(cudaMemcpyAsync(c.id[0], hid.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice,
+                           h->stream));
         /* every parcel must start inside the mesh: the reference would index out of bounds */
         CK(cudaMemsetAsync(h->dcount, 0, sizeof(unsigned long long), h->stream));
-        {
+        if (h->tet) {
+            /* walk from the caller's hint to the owning tet */
+            CK(cudaMemcpyAsync(c.cell[1], hint, n * sizeof(int32_t), cudaMemcpyHostToDevice,
+                               h->stream));
+            ProfScope ps(h, ST_KERNEL_OTHER);
+            TetMeshK lm = h->tmesh;
+            lm.hop_limit = 1 << 20;   /* bounded: a walk that cycles counts as outside */
+            CK(launch_tet_locate(lm, (const double*)c.x[0], (const double*)c.y[0],
+                                 (const double*)c.z[0], c.cell[1], n, c.cell[0], h->dcount,
+                                 h->stream));
+            h->launches += 1;
+        } else {
             ProfScope ps(h, ST_KERNEL_OTHER);
             CK(cells_cloud<P>((const P*)c.x[0], (const P*)c.y[0], (const P*)c.z[0], nullptr, n,
                               mesh_k<P>(h), (int32_t*)c.keys[0], h->dcount, h->stream));
@@ -554,7 +661,11 @@ int do_get_cells(st_handle* h, int cloud, int32_t* cells)
     const int64_t n = c.n;
     if (n == 0) return ST_OK;
     /* the sort key buffer is free between steps */
-    {
+    if (h->tet) {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        CK(cells_unpermute(c.id[c.cur], c.cell[c.cur], n, (int32_t*)c.keys[0], h->stream));
+        h->launches += 1;
+    } else {
         ProfScope ps(h, ST_KERNEL_OTHER);
         CK(cells_cloud<P>((const P*)c.x[c.cur], (const P*)c.y[c.cur], (const P*)c.z[c.cur],
                           c.id[c.cur], n, mesh_k<P>(h), (int32_t*)c.keys[0], nullptr, h->stream));
@@ -589,7 +700,7 @@ void free_cloud(CloudBufs& c)
 {
     for (int k = 0; k < 2; ++k) {
         void* arrs[] = {c.x[k], c.y[k], c.z[k], c.u[k], c.v[k], c.w[k], c.d[k],
-                        c.id[k], c.keys[k], c.perm[k]};
+                        c.id[k], c.keys[k], c.perm[k], c.cell[k]};
         for (void* p : arrs)
             if (p) cudaFree(p);
     }
@@ -622,6 +733,7 @@ int upload_clouds_pair(st_handle* h)
             const int o = 1 - b.cur;
             k.x = (P*)b.x[o]; k.y = (P*)b.y[o]; k.z = (P*)b.z[o];
             k.u = (V*)b.u[o]; k.v = (V*)b.v[o]; k.w = (V*)b.w[o]; k.d = (const V*)b.d[o];
+            k.cell = b.cell[o];
         }
         v[nc + c] = k;
     }
@@ -730,6 +842,7 @@ int adj_check(st_handle* h, int cloud, const st_adjoint_desc* d)
     int rc;
     if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
     if (!d) return fail(ST_ERR_INVALID_ARGUMENT, "null adjoint descriptor");
+    if (h->tet) return fail(ST_ERR_INVALID_ARGUMENT, "the adjoint supports cuboid meshes only");
     if (h->p.precision == ST_PREC_FP32 || h->p.drag_model != ST_DRAG_SCHILLER_NAUMANN ||
         h->p.n_substeps != 1)
         return fail(ST_ERR_INVALID_ARGUMENT,
@@ -944,19 +1057,9 @@ void st_params_default(st_params* p)
     p->diameter_scale = 1.0;
 }
 
-int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle** out)
+static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells,
+                       const st_tet_mesh_desc* tm, int device, st_handle** out)
 {
-    if (!p || !m || !out) return fail(ST_ERR_INVALID_ARGUMENT, "null argument to st_create");
-    *out = nullptr;
-    for (int a = 0; a < 3; ++a) {
-        if (m->n[a] < 1) return fail(ST_ERR_INVALID_ARGUMENT, "mesh n[%d] = %d < 1", a, m->n[a]);
-        if (!(m->ending[a] > m->origin[a]))
-            return fail(ST_ERR_INVALID_ARGUMENT, "mesh ending[%d] must exceed origin[%d]", a, a);
-    }
-    const int64_t ncells = (int64_t)m->n[0] * m->n[1] * m->n[2];
-    if (ncells > INT32_MAX)
-        return fail(ST_ERR_INVALID_ARGUMENT, "mesh has %lld cells; at most 2^31-1 supported",
-                    (long long)ncells);
     if (p->precision < ST_PREC_FP32 || p->precision > ST_PREC_FP64)
         return fail(ST_ERR_INVALID_ARGUMENT, "unknown precision %d", p->precision);
     if (p->drag_model != ST_DRAG_STOKES_IMPLICIT && p->drag_model != ST_DRAG_SCHILLER_NAUMANN)
@@ -977,11 +1080,14 @@ int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle**
         return fail(ST_ERR_CUDA, "no CUDA device available (the library has no CPU path)");
     if (device < 0 || device >= ndev)
         return fail(ST_ERR_INVALID_ARGUMENT, "device %d out of range [0, %d)", device, ndev);
+    if (tm && p->precision == ST_PREC_FP32)
+        return fail(ST_ERR_INVALID_ARGUMENT, "tet meshes need mixed or FP64 precision");
     DeviceGuard g(device);
 
     st_handle* h = new st_handle();
     h->p = *p;
     h->m = *m;
+    h->tet = tm != nullptr;
     h->device = device;
     h->ncells = ncells;
     h->stride = (ncells * 3 + COMP_ALIGN - 1) / COMP_ALIGN * COMP_ALIGN;
@@ -997,7 +1103,7 @@ int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle**
         h->dep = DEP_DET1;
         h->limbs = 1;
     }
-    h->morton = m->n[0] <= 1024 && m->n[1] <= 1024 && m->n[2] <= 1024;
+    h->morton = !h->tet && m->n[0] <= 1024 && m->n[1] <= 1024 && m->n[2] <= 1024;
     if (h->morton) {
         int b = 1;
         int nmax = std::max(m->n[0], std::max(m->n[1], m->n[2]));
@@ -1043,19 +1149,120 @@ int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle**
             c.lost = 0;
             c.overflow = 0;
         }
-        if ((e = cudaMemcpy(h->dctl, ctl.data(), sizeof(CloudCtl) * p->n_clouds,
-                            cudaMemcpyHostToDevice)) != cudaSuccess)
+        if ((e = cudaMemcpyAsync(h->dctl, ctl.data(), sizeof(CloudCtl) * p->n_clouds,
+                                 cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
             return bail(fail(ST_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e)));
+    }
+    if (h->tet) {
+        const size_t nv = (size_t)tm->n_vertices, nt = (size_t)tm->n_tets;
+        if ((e = cudaMalloc((void**)&h->d_verts, nv * 3 * sizeof(double))) != cudaSuccess ||
+            (e = cudaMalloc((void**)&h->d_tets, nt * 4 * sizeof(int32_t))) != cudaSuccess ||
+            (e = cudaMalloc((void**)&h->d_nbr, nt * 4 * sizeof(int32_t))) != cudaSuccess ||
+            (e = cudaMalloc((void**)&h->d_hops, 8 * sizeof(unsigned long long))) != cudaSuccess)
+            return bail(fail(e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA,
+                             "device allocation: %s", cudaGetErrorString(e)));
+        if ((e = cudaMemcpyAsync(h->d_verts, tm->vertices, nv * 3 * sizeof(double),
+                                 cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(h->d_tets, tm->tets, nt * 4 * sizeof(int32_t),
+                                 cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(h->d_nbr, tm->neighbors, nt * 4 * sizeof(int32_t),
+                                 cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+            (e = cudaMemsetAsync(h->d_hops, 0, 8 * sizeof(unsigned long long), h->stream)) !=
+                cudaSuccess ||
+            (e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
+            return bail(fail(ST_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e)));
+        TetMeshK& k = h->tmesh;
+        k.verts = h->d_verts;
+        k.tets = h->d_tets;
+        k.nbr = h->d_nbr;
+        k.nt = (int64_t)nt;
+        for (int a = 0; a < 3; ++a) {
+            k.origin[a] = tm->origin[a];
+            k.ending[a] = tm->ending[a];
+        }
+        k.hop_limit = tm->hop_limit > 0 ? tm->hop_limit : 64;
+        k.pad = 0;
     }
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    int occ = DISPATCH(h, step_max_active_blocks, h->dep, h->block);
+    int occ = h->tet ? (p->precision == ST_PREC_FP64
+                            ? step_tet_max_active_blocks<double>(h->dep, h->block)
+                            : step_tet_max_active_blocks<float>(h->dep, h->block))
+                     : DISPATCH(h, step_max_active_blocks, h->dep, h->block);
     if (occ < 1) occ = 1;
     h->grid = p->grid_blocks > 0 ? p->grid_blocks : nsm * occ;
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
         return bail(fail(ST_ERR_CUDA, "set-up: %s", cudaGetErrorString(e)));
     *out = h;
     return ST_OK;
+}
+
+int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle** out)
+{
+    if (!p || !m || !out) return fail(ST_ERR_INVALID_ARGUMENT, "null argument to st_create");
+    *out = nullptr;
+    for (int a = 0; a < 3; ++a) {
+        if (m->n[a] < 1) return fail(ST_ERR_INVALID_ARGUMENT, "mesh n[%d] = %d < 1", a, m->n[a]);
+        if (!(m->ending[a] > m->origin[a]))
+            return fail(ST_ERR_INVALID_ARGUMENT, "mesh ending[%d] must exceed origin[%d]", a, a);
+    }
+    const int64_t ncells = (int64_t)m->n[0] * m->n[1] * m->n[2];
+    if (ncells > INT32_MAX)
+        return fail(ST_ERR_INVALID_ARGUMENT, "mesh has %lld cells; at most 2^31-1 supported",
+                    (long long)ncells);
+    return create_impl(p, m, ncells, nullptr, device, out);
+}
+
+int st_create_tet(const st_params* p, const st_tet_mesh_desc* tm, int device, st_handle** out)
+{
+    if (!p || !tm || !out) return fail(ST_ERR_INVALID_ARGUMENT, "null argument to st_create_tet");
+    *out = nullptr;
+    if (tm->n_vertices < 4 || tm->n_tets < 1 || tm->n_tets > INT32_MAX / 4 ||
+        tm->n_vertices > INT32_MAX)
+        return fail(ST_ERR_INVALID_ARGUMENT, "tet mesh sizes out of range (%lld vertices, %lld tets)",
+                    (long long)tm->n_vertices, (long long)tm->n_tets);
+    if (!tm->vertices || !tm->tets || !tm->neighbors)
+        return fail(ST_ERR_INVALID_ARGUMENT, "null tet mesh array");
+    if (tm->hop_limit < 0) return fail(ST_ERR_INVALID_ARGUMENT, "hop_limit must be >= 0");
+    st_mesh_desc m;
+    memset(&m, 0, sizeof m);
+    for (int a = 0; a < 3; ++a) {
+        if (!(tm->ending[a] > tm->origin[a]))
+            return fail(ST_ERR_INVALID_ARGUMENT, "mesh ending[%d] must exceed origin[%d]", a, a);
+        m.origin[a] = tm->origin[a];
+        m.ending[a] = tm->ending[a];
+        m.n[a] = 1;
+    }
+    /* every index the kernels follow must stay inside the arrays */
+    const int64_t nt = tm->n_tets, nv = tm->n_vertices;
+    for (int64_t i = 0; i < 4 * nt; ++i) {
+        if (tm->tets[i] < 0 || tm->tets[i] >= nv)
+            return fail(ST_ERR_INVALID_ARGUMENT, "tet %lld has vertex id %d out of range",
+                        (long long)(i / 4), tm->tets[i]);
+        if (tm->neighbors[i] < -1 || tm->neighbors[i] >= nt)
+            return fail(ST_ERR_INVALID_ARGUMENT, "tet %lld has neighbour %d out of range",
+                        (long long)(i / 4), tm->neighbors[i]);
+    }
+    /* canonical order: vertex ids increasing within each tet, neighbours permuted with them,
+     * so both tets of a shared face build its plane from the same vertices in the same order */
+    std::vector<int32_t> ct((size_t)nt * 4), cn((size_t)nt * 4);
+    for (int64_t t = 0; t < nt; ++t) {
+        int idx[4] = {0, 1, 2, 3};
+        const int32_t* v = tm->tets + 4 * t;
+        std::sort(idx, idx + 4, [v](int a, int b) { return v[a] < v[b]; });
+        for (int k = 0; k < 4; ++k) {
+            ct[4 * t + k] = v[idx[k]];
+            cn[4 * t + k] = tm->neighbors[4 * t + idx[k]];
+        }
+        if (ct[4 * t] == ct[4 * t + 1] || ct[4 * t + 1] == ct[4 * t + 2] ||
+            ct[4 * t + 2] == ct[4 * t + 3])
+            return fail(ST_ERR_INVALID_ARGUMENT, "tet %lld repeats a vertex", (long long)t);
+    }
+    st_tet_mesh_desc c = *tm;
+    c.tets = ct.data();
+    c.neighbors = cn.data();
+    return create_impl(p, &m, nt, &c, device, out);
 }
 
 int st_destroy(st_handle* h)
@@ -1067,7 +1274,8 @@ int st_destroy(st_handle* h)
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
     void* arrs[] = {h->dU, h->dsrc, h->dacc, h->dctl, h->dcounter, h->dcount, h->dclouds,
-                    h->dstage, h->adj.mem, h->dclouds2};
+                    h->dstage, h->adj.mem, h->dclouds2, h->d_verts, h->d_tets, h->d_nbr,
+                    h->d_hops};
     for (void* p : arrs)
         if (p) cudaFree(p);
     for (auto& r : h->recs) {
@@ -1108,8 +1316,39 @@ static int update_headroom(st_handle* h)
     return ST_OK;
 }
 
+static int set_parcels_impl(st_handle* h, int cloud, int64_t n, const double* xyz,
+                            const double* uvw, const double* d, const int32_t* hint);
+
 int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
                    const double* d)
+{
+    return set_parcels_impl(h, cloud, n, xyz, uvw, d, nullptr);
+}
+
+int st_set_parcels_tet(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
+                       const double* d, const int32_t* hint)
+{
+    if (h && !h->tet) return fail(ST_ERR_INVALID_ARGUMENT, "st_set_parcels_tet on a cuboid mesh");
+    return set_parcels_impl(h, cloud, n, xyz, uvw, d, hint);
+}
+
+int st_tet_hop_histogram(st_handle* h, uint64_t out[8], int reset)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (!h->tet) return fail(ST_ERR_INVALID_ARGUMENT, "st_tet_hop_histogram on a cuboid mesh");
+    DeviceGuard g(h->device);
+    unsigned long long v[8];
+    CK(cudaMemcpyAsync(v, h->d_hops, sizeof v, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (out)
+        for (int k = 0; k < 8; ++k) out[k] = v[k];
+    if (reset) CK(cudaMemsetAsync(h->d_hops, 0, sizeof v, h->stream));
+    return ST_OK;
+}
+
+static int set_parcels_impl(st_handle* h, int cloud, int64_t n, const double* xyz,
+                            const double* uvw, const double* d, const int32_t* hint)
 {
     int rc;
     if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
@@ -1120,7 +1359,12 @@ int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
     DeviceGuard g(h->device);
     CK(cudaStreamSynchronize(h->stream));
     release_graph(h);
-    rc = DISPATCH(h, do_set_parcels, h, cloud, n, xyz, uvw, d);
+    std::vector<int32_t> zeros;
+    if (h->tet && !hint && n > 0) {
+        zeros.assign((size_t)n, 0);
+        hint = zeros.data();
+    }
+    rc = DISPATCH(h, do_set_parcels, h, cloud, n, xyz, uvw, d, hint);
     if (rc) return rc;
     return update_headroom(h);
 }
@@ -1365,6 +1609,7 @@ int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out)
     int rc;
     if ((rc = check_handle(h))) return rc;
     if (trial_steps < 4) return fail(ST_ERR_INVALID_ARGUMENT, "trial_steps must be >= 4");
+    if (h->tet) return fail(ST_ERR_INVALID_ARGUMENT, "st_autotune supports cuboid meshes only");
     if (!(dt > 0) || !(dt < 1e300)) return fail(ST_ERR_INVALID_ARGUMENT, "dt must be positive");
     DeviceGuard g(h->device);
     CK(cudaStreamSynchronize(h->stream));
@@ -1379,7 +1624,8 @@ int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out)
         rc = st_set_parcels(t, c, n, xyz.data(), uvw.data(), d.data());
     }
     if (rc == ST_OK) {
-        cudaError_t e = cudaMemcpy(t->dU, h->dU, h->ncells * 3 * h->vsz, cudaMemcpyDeviceToDevice);
+        cudaError_t e = cudaMemcpyAsync(t->dU, h->dU, h->ncells * 3 * h->vsz,
+                                        cudaMemcpyDeviceToDevice, t->stream);
         if (e != cudaSuccess) rc = fail(ST_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e));
     }
     const int blocks[] = {128, 256};

@@ -74,6 +74,7 @@ struct CloudK {
     int64_t tile0;              /* first warp tile (WARP_TILE parcels) of this cloud */
     unsigned long long* acc;    /* [stride*limbs], stride = nCells*3 padded to COMP_ALIGN */
     double* src;                /* [stride] */
+    int32_t* cell;              /* owning tet per parcel (tet meshes), else nullptr */
 };
 
 template <class P, class V>
@@ -89,6 +90,44 @@ struct StepArgs {
     CloudCtl* ctl;              /* [nclouds] */
     int64_t total_tiles;        /* warp tiles (32 parcels) over all clouds */
 };
+
+/* Unstructured tetrahedral mesh (st_tet.cu). */
+struct TetMeshK {
+    const double* verts;        /* [nv][3] */
+    const int32_t* tets;        /* [nt][4] vertex indices */
+    const int32_t* nbr;         /* [nt][4] tet across the face opposite local vertex k, or -1 */
+    int64_t nt;
+    double origin[3];           /* box of the walls */
+    double ending[3];
+    int32_t hop_limit;          /* face-walk hops per substep before a parcel counts as lost */
+    int32_t pad;
+};
+
+template <class V>
+struct TetStepArgs {
+    TetMeshK mesh;
+    PhysK<V> phys;
+    double dtP;
+    V dtV;
+    V fscale;
+    int32_t nclouds;
+    const V* U;                          /* [nt*3] */
+    const CloudK<double, V>* clouds;
+    CloudCtl* ctl;
+    int64_t total_tiles;                 /* warp tiles of WARP_TILE parcels */
+    unsigned long long* hop_hist;        /* [8] walk lengths per substep, or nullptr */
+};
+
+template <class V>
+cudaError_t launch_step_tet(const TetStepArgs<V>& a, int dep, int grid, int block,
+                            cudaStream_t s);
+template <class V>
+int step_tet_max_active_blocks(int dep, int block);
+/* Walks every parcel from hint[i] to the tet that contains it (hop limit of the mesh);
+ * cells[i] = tet or -1, and `outside` counts failures. */
+cudaError_t launch_tet_locate(const TetMeshK& m, const double* x, const double* y,
+                              const double* z, const int32_t* hint, int64_t n, int32_t* cells,
+                              unsigned long long* outside, cudaStream_t s);
 
 /* Arguments of the adjoint kernels (st_adjoint.cu). */
 template <class P, class V>
@@ -159,6 +198,7 @@ struct SortBufs {
     V* w[2];
     V* d[2];
     int32_t* id[2];
+    int32_t* cell[2];       /* tet meshes: owning tet, sorted along; nullptr on hex meshes */
     uint32_t* keys[2];
     uint32_t* perm[2];
     void* temp;
@@ -171,6 +211,8 @@ cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& me
                        bool morton, cudaStream_t s, int* launches);
 template <class P, class V>
 cudaError_t unpermute_cloud(SortBufs<P, V>& b, int cur, int64_t n, cudaStream_t s);
+cudaError_t cells_unpermute(const int32_t* id, const int32_t* cell, int64_t n, int32_t* out,
+                            cudaStream_t s);
 template <class P>
 cudaError_t cells_cloud(const P* x, const P* y, const P* z, const int32_t* id, int64_t n,
                         const MeshK<P>& mesh, int32_t* cells_out, unsigned long long* outside,

@@ -23,33 +23,13 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "st_internal.h"
-#include "st_pow.h"
+#include "st_device.cuh"
 
 namespace st {
-
-#define FULL_MASK 0xffffffffu
 
 /* ------------------------------------------------------------------------------------ */
 /* relocation                                                                           */
 /* ------------------------------------------------------------------------------------ */
-
-__device__ __forceinline__ float st_floor(float v) { return floorf(v); }
-__device__ __forceinline__ double st_floor(double v) { return floor(v); }
-__device__ __forceinline__ float st_sqrt(float v) { return __fsqrt_rn(v); }
-__device__ __forceinline__ double st_sqrt(double v) { return __dsqrt_rn(v); }
-
-/* floor(label, v) (A:668-670); values outside int32 mark the parcel as lost. */
-template <class P>
-__device__ __forceinline__ int32_t floor_label(P v, bool& bad)
-{
-    P f = st_floor(v);
-    if (!(f >= (P)-2147483648.0 && f < (P)2147483648.0)) {
-        bad = true;
-        return 0;
-    }
-    return (int32_t)f;
-}
 
 struct LocK {
     int32_t I, J, K;
@@ -92,136 +72,6 @@ __device__ __forceinline__ LocK locate(const MeshK<P>& m, P x, P y, P z, bool& b
 }
 
 /* ------------------------------------------------------------------------------------ */
-/* fixed-point deposit                                                                  */
-/* ------------------------------------------------------------------------------------ */
-
-/* smallest e with |a| < 2^e, for finite a != 0 (the frexp exponent) */
-__device__ __forceinline__ int exp_of(double a)
-{
-    uint64_t b = (uint64_t)__double_as_longlong(a) & 0x7fffffffffffffffULL;
-    int be = (int)(b >> 52);
-    if (be == 0) {
-        double s = __longlong_as_double((long long)b) * 18014398509481984.0; /* 2^54 */
-        be = (int)(((uint64_t)__double_as_longlong(s)) >> 52) - 54;
-    }
-    return be - 1022;
-}
-
-__device__ __forceinline__ double ldexp2(double x, int k)
-{
-    int k1 = k / 2;
-    int k2 = k - k1;
-    return (x * st_pow2i(k1)) * st_pow2i(k2);
-}
-
-/* largest finite |v| seen (probe pass) */
-template <class V>
-__device__ __forceinline__ void track_max(V v, double& amax)
-{
-    const double a = fabs((double)v);
-    if (a < __longlong_as_double(0x7ff0000000000000LL)) amax = fmax(amax, a);
-}
-
-/* Fixed-point parameters of one cloud for the current step: q = rint(dep * 2^-L), and a
- * deposit with |dep| >= 2^(cap+L) (i.e. frexp exponent - L > cap) does not fit.  Single
- * precision deposits are scaled in single precision when 2^-L and 2^(cap+L) are normal
- * floats: scaling by a power of two is exact, so the integer is the same as through FP64. */
-struct Quant {
-    double scale;   /* 2^-L, or 0 when 2^-L is not a normal double (then ldexp2 is used) */
-    double thr;     /* 2^(cap+L) */
-    float scale_f;  /* 2^-L as float, when `fast` */
-    float thr_f;    /* 2^(cap+L) as float, when `fast` */
-    int L;
-    bool fast;
-};
-
-__device__ __forceinline__ Quant make_quant(int L, int cap)
-{
-    Quant q;
-    q.L = L;
-    q.scale = (-L >= -1022 && -L <= 1023) ? st_pow2i(-L) : 0.0;
-    q.thr = ldexp2(1.0, cap + L);
-    q.fast = (-L >= -126 && -L <= 127) && (cap + L >= -126 && cap + L <= 127);
-    q.scale_f = q.fast ? st_pow2if(-L) : 0.0f;
-    q.thr_f = q.fast ? st_pow2if(cap + L) : 0.0f;
-    return q;
-}
-
-/* Quantises one deposit component: 0 for zero, non-finite or out-of-range values (the
- * latter two are counted in `ovf`).  `amax` tracks the largest finite |dep| for the next
- * step's scale (max is order-independent, so the scale is reproducible). */
-__device__ __forceinline__ long long quantize(double dv, const Quant& qp, double& amax,
-                                              unsigned& ovf)
-{
-    const double a = fabs(dv);
-    if (a == 0.0) return 0;
-    if (a < __longlong_as_double(0x7ff0000000000000LL)) amax = fmax(amax, a);
-    if (!(a < qp.thr)) {
-        ++ovf;
-        return 0;
-    }
-    const double x = qp.scale != 0.0 ? dv * qp.scale : ldexp2(dv, -qp.L);
-    return __double2ll_rn(x);
-}
-
-__device__ __forceinline__ long long quantize(float dv, const Quant& qp, double& amax,
-                                              unsigned& ovf)
-{
-    if (!qp.fast) return quantize((double)dv, qp, amax, ovf);
-    const float a = fabsf(dv);
-    if (a == 0.0f) return 0;
-    if (a < __int_as_float(0x7f800000)) amax = fmax(amax, (double)a);
-    if (!(a < qp.thr_f)) {
-        ++ovf;
-        return 0;
-    }
-    return __float2ll_rn(dv * qp.scale_f);
-}
-
-template <int DEP, class V>
-__device__ __forceinline__ void deposit_direct(const V dep[3], int64_t cell0,
-                                               unsigned long long* acc, double* src,
-                                               const Quant& qp, double& amax, unsigned& ovf)
-{
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        if (DEP == DEP_ATOMIC) {
-            if (dep[c] != (V)0) atomicAdd(src + 3 * cell0 + c, (double)dep[c]);
-        } else {
-            long long q = quantize(dep[c], qp, amax, ovf);
-            if (DEP == DEP_DET1) {
-                if (q) atomicAdd(acc + 3 * cell0 + c, (unsigned long long)q);
-            } else if (DEP == DEP_DET2) {
-                if (q) {
-                    atomicAdd(acc + 2 * (3 * cell0 + c), (unsigned long long)(q >> 32));
-                    atomicAdd(acc + 2 * (3 * cell0 + c) + 1,
-                              (unsigned long long)q & 0xffffffffULL);
-                }
-            }
-        }
-    }
-}
-
-#ifndef ST_SCAN_STEPS
-#define ST_SCAN_STEPS 2
-#endif
-constexpr int SCAN_STEPS = ST_SCAN_STEPS;   /* 0..5 */
-constexpr int SPAN = 1 << SCAN_STEPS;        /* lanes summed per emitted chunk */
-
-/* Inclusive scan over the lane's run of equal keys, limited to SPAN lanes (runs are
- * contiguous lane ranges). */
-template <class T>
-__device__ __forceinline__ T seg_scan(T v, int lane, int segstart)
-{
-#pragma unroll
-    for (int off = 1; off < SPAN; off <<= 1) {
-        T t = __shfl_up_sync(FULL_MASK, v, off);
-        if (lane - off >= segstart) v += t;
-    }
-    return v;
-}
-
-/* ------------------------------------------------------------------------------------ */
 /* the step kernel                                                                      */
 /* ------------------------------------------------------------------------------------ */
 
@@ -239,11 +89,6 @@ __device__ __forceinline__ int find_cloud(const StepArgs<P, V>& a, int64_t tile)
     }
     return lo;
 }
-
-template <class T>
-__device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
-template <class T>
-__device__ __forceinline__ void st_stream(T* p, T v) { __stcs(p, v); }
 
 /* One parcel through all substeps (A:1271-1365) after its start cell has been located and
  * the cell velocity gathered.  pos/vel are updated in place; the final deposit is returned
@@ -386,91 +231,6 @@ __device__ __forceinline__ void evolve_one(const StepArgs<P, V>& a, P pos[3], V 
         vel[k] = velNew[k];
         dep[k] = mB * (state0[k] - velNew[k]);                                          /* A:1361 */
     }
-}
-
-/* Final deposits of 32 consecutive parcels (one per lane, key < 0 = none): runs of equal
- * cells are summed with a segmented warp scan and the last lane of each run adds the sum. */
-template <int DEP, class V>
-__device__ __forceinline__ void deposit_warp(int32_t key, const V dep[3],
-                                             unsigned long long* acc, double* src,
-                                             const Quant& qp, int lane, double& amax,
-                                             unsigned& ovf)
-{
-    if (DEP == DEP_PROBE) {
-        if (key >= 0) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) track_max(dep[k], amax);
-        }
-        return;
-    }
-    if (DEP == DEP_ATOMIC) {
-        if (key >= 0) deposit_direct<DEP_ATOMIC, V>(dep, key, acc, src, qp, amax, ovf);
-        return;
-    }
-    long long q[3] = {0, 0, 0};
-    if (key >= 0) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) q[k] = quantize(dep[k], qp, amax, ovf);
-    }
-    const int prev = __shfl_up_sync(FULL_MASK, key, 1);
-    const bool head = (lane == 0) || (prev != key);
-    const unsigned heads = __ballot_sync(FULL_MASK, head);
-    const int segstart = 31 - __clz(heads & (FULL_MASK >> (31 - lane)));
-    const bool tail = (lane == 31) || ((heads >> (lane + 1)) & 1u);
-    /* A scan of SCAN_STEPS steps sums runs in chunks of SPAN lanes: lane j holds the sum of
-     * [max(run start, j - SPAN + 1), j]; the run's last lane and every SPAN-th lane before it
-     * add their chunk, which covers the run exactly once. */
-    const unsigned tails = __ballot_sync(FULL_MASK, tail);
-    const int tailpos = lane + __ffs(tails >> lane) - 1;
-    const bool emit = ((tailpos - lane) & (SPAN - 1)) == 0;
-    if (DEP == DEP_DET1) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) q[k] = seg_scan(q[k], lane, segstart);
-        if (emit && key >= 0) {
-            unsigned long long* p = acc + 3 * (int64_t)key;
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-                if (q[k]) atomicAdd(p + k, (unsigned long long)q[k]);
-        }
-    } else {
-        long long hi[3];
-        unsigned long long lo[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            hi[k] = seg_scan(q[k] >> 32, lane, segstart);
-            lo[k] = seg_scan((unsigned long long)q[k] & 0xffffffffULL, lane, segstart);
-        }
-        if (emit && key >= 0) {
-            unsigned long long* p = acc + 6 * (int64_t)key;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                if (hi[k]) atomicAdd(p + 2 * k, (unsigned long long)hi[k]);
-                if (lo[k]) atomicAdd(p + 2 * k + 1, lo[k]);
-            }
-        }
-    }
-}
-
-/* Warp-aggregated bookkeeping for one cloud: largest deposit exponent, lost parcels and
- * range errors.  Called when a warp moves on to another cloud and at the end. */
-template <int DEP>
-__device__ __forceinline__ void flush_ctl(CloudCtl* ctl, int lane, double& amax, unsigned& ovf,
-                                          unsigned& lost)
-{
-    if (DEP != DEP_ATOMIC) {
-        const int e = amax > 0.0 ? exp_of(amax) : EXP_NONE;
-        const int wmax = __reduce_max_sync(FULL_MASK, e);
-        if (lane == 0 && wmax != EXP_NONE) atomicMax(&ctl->emax, wmax);
-    }
-    const unsigned nlost = __reduce_add_sync(FULL_MASK, lost);
-    const unsigned novf = __reduce_add_sync(FULL_MASK, ovf);
-    if (lane == 0) {
-        if (nlost) atomicAdd(&ctl->lost, (unsigned long long)nlost);
-        if (novf && DEP != DEP_PROBE) atomicAdd(&ctl->overflow, (unsigned long long)novf);
-    }
-    amax = 0.0;
-    ovf = 0;
-    lost = 0;
 }
 
 /* The step kernel.  A warp owns a tile of SLICES x 32 consecutive parcels (lane l holds

@@ -65,6 +65,26 @@ __global__ void k_sort_keys(const P* __restrict__ x, const P* __restrict__ y,
  * issues all their (scattered) loads before any store, so that many reads are in flight. */
 constexpr int GATHER_ILP = 4;
 
+/* tet meshes: the key is the owning tet (tets are numbered with spatial locality) */
+__global__ void k_sort_keys_cell(const int32_t* __restrict__ cell, int64_t n,
+                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ perm)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        keys[p] = (uint32_t)cell[p];
+        perm[p] = (uint32_t)p;
+    }
+}
+
+/* out[id[p]] = cell[p] */
+__global__ void k_cells_unpermute(const int32_t* __restrict__ id, const int32_t* __restrict__ cell,
+                                  int64_t n, int32_t* __restrict__ out)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x)
+        out[id[p]] = cell[p];
+}
+
 template <class P, class V>
 __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ perm, int64_t n,
                          const P* __restrict__ x0, const P* __restrict__ y0,
@@ -73,7 +93,8 @@ __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ per
                          const V* __restrict__ d0, const int32_t* __restrict__ id0,
                          P* __restrict__ x1, P* __restrict__ y1, P* __restrict__ z1,
                          V* __restrict__ u1, V* __restrict__ v1, V* __restrict__ w1,
-                         V* __restrict__ d1, int32_t* __restrict__ id1)
+                         V* __restrict__ d1, int32_t* __restrict__ id1,
+                         const int32_t* __restrict__ c0, int32_t* __restrict__ c1)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x * GATHER_ILP;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x * GATHER_ILP + threadIdx.x; base < n;
@@ -82,6 +103,7 @@ __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ per
         P x[GATHER_ILP], y[GATHER_ILP], z[GATHER_ILP];
         V u[GATHER_ILP], v[GATHER_ILP], w[GATHER_ILP], dd[GATHER_ILP];
         int32_t id[GATHER_ILP];
+        int32_t cc[GATHER_ILP];
 #pragma unroll
         for (int k = 0; k < GATHER_ILP; ++k) {
             const int64_t p = base + (int64_t)k * blockDim.x;
@@ -99,6 +121,7 @@ __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ per
                 w[k] = __ldg(w0 + s);
                 dd[k] = __ldg(d0 + s);
                 id[k] = __ldg(id0 + s);
+                if (c0) cc[k] = __ldg(c0 + s);
             }
         }
 #pragma unroll
@@ -113,6 +136,7 @@ __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ per
                 __stcs(w1 + p, w[k]);
                 __stcs(d1 + p, dd[k]);
                 __stcs(id1 + p, id[k]);
+                if (c1) __stcs(c1 + p, cc[k]);
             }
         }
     }
@@ -202,8 +226,11 @@ cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& me
 {
     if (n <= 1) return cudaSuccess;
     const int o = 1 - cur;
-    k_sort_keys<P><<<grid_for(n), 256, 0, s>>>(b.x[cur], b.y[cur], b.z[cur], n, mesh,
-                                               morton ? 1 : 0, b.keys[0], b.perm[0]);
+    if (b.cell[cur])
+        k_sort_keys_cell<<<grid_for(n), 256, 0, s>>>(b.cell[cur], n, b.keys[0], b.perm[0]);
+    else
+        k_sort_keys<P><<<grid_for(n), 256, 0, s>>>(b.x[cur], b.y[cur], b.z[cur], n, mesh,
+                                                   morton ? 1 : 0, b.keys[0], b.perm[0]);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     size_t bytes = b.temp_bytes;
@@ -215,7 +242,8 @@ cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& me
     k_gather<P, V><<<(int)gblocks, 256, 0, s>>>(b.perm[1], n, b.x[cur], b.y[cur], b.z[cur],
                                                b.u[cur], b.v[cur], b.w[cur], b.d[cur],
                                                b.id[cur], b.x[o], b.y[o], b.z[o], b.u[o],
-                                               b.v[o], b.w[o], b.d[o], b.id[o]);
+                                               b.v[o], b.w[o], b.d[o], b.id[o], b.cell[cur],
+                                               b.cell[o]);
     if (launches) *launches += 2;  /* our keys and gather kernels; CUB's own are not counted */
     return cudaGetLastError();
 }
@@ -239,6 +267,14 @@ cudaError_t cells_cloud(const P* x, const P* y, const P* z, const int32_t* id, i
 {
     if (n == 0) return cudaSuccess;
     k_cells<P><<<grid_for(n), 256, 0, s>>>(x, y, z, id, n, mesh, cells_out, outside);
+    return cudaGetLastError();
+}
+
+cudaError_t cells_unpermute(const int32_t* id, const int32_t* cell, int64_t n, int32_t* out,
+                            cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    k_cells_unpermute<<<grid_for(n), 256, 0, s>>>(id, cell, n, out);
     return cudaGetLastError();
 }
 

@@ -1,0 +1,300 @@
+/*
+ * st_tet.cu -- the parcel step on unstructured tetrahedral meshes with face-walk
+ * relocation (configuration 2: 96^3 jittered hexes split into 6 tets; no counterpart in the
+ * reference, whose cuboid mesh is located by floor, A:663-697).
+ *
+ * Each parcel carries its owning tet.  After the drag update and the position update, a new
+ * position outside the box keeps its old coordinate on that axis and mirrors the old
+ * velocity component (the reference's wall rule, A:1313-1329), then a greedy walk moves from
+ * the current tet across the face with the largest positive signed distance until the
+ * position is inside.  Face planes are computed at use in FP64 from the tet's four vertices
+ * (the 22 MB vertex array of configuration 2 stays in L2).  Each tet's vertex ids are stored
+ * in increasing order (st_create_tet sorts them and permutes the neighbours with them), and
+ *   face f opposite vertex f, (p, q, r) = the other vertices in increasing order,
+ *   n = (q - p) x (r - p), negated if n . (v_f - p) > 0; s_f(x) = n . (x - p); inside iff all
+ *   s_f <= 0; ties between faces go to the lowest index.
+ * The two tets of a shared face therefore compute the same plane bit for bit up to an exact
+ * negation: a point is never outside both, and no walk bounces between two tets.
+ * The same arithmetic, without fused multiply-adds, is in the CPU oracle, so owning tets agree
+ * bit for bit.  A walk that reaches a boundary face or exceeds the hop limit marks the parcel
+ * as lost (its state is left unchanged and the host reports it).  Deposits use the same
+ * deterministic fixed-point path as the hex kernels.
+ */
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "st_device.cuh"
+
+namespace st {
+
+enum { TWALK_OK = 0, TWALK_EXIT = 1, TWALK_HOPS = 2 };
+
+__device__ __forceinline__ void tet_signed(const TetMeshK& m, int32_t t, const double x[3],
+                                           double s[4])
+{
+    const int4 tv = __ldg(reinterpret_cast<const int4*>(m.tets) + t);
+    const int ids[4] = {tv.x, tv.y, tv.z, tv.w};
+    double v[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double* pv = m.verts + 3 * (int64_t)ids[k];
+        v[k][0] = __ldg(pv);
+        v[k][1] = __ldg(pv + 1);
+        v[k][2] = __ldg(pv + 2);
+    }
+    const int F[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        const double* p = v[F[f][0]];
+        const double* q = v[F[f][1]];
+        const double* r = v[F[f][2]];
+        const double a0 = q[0] - p[0], a1 = q[1] - p[1], a2 = q[2] - p[2];
+        const double b0 = r[0] - p[0], b1 = r[1] - p[1], b2 = r[2] - p[2];
+        double n0 = a1 * b2 - a2 * b1;
+        double n1 = a2 * b0 - a0 * b2;
+        double n2 = a0 * b1 - a1 * b0;
+        const double e = (n0 * (v[f][0] - p[0]) + n1 * (v[f][1] - p[1])) + n2 * (v[f][2] - p[2]);
+        if (e > 0.0) { n0 = -n0; n1 = -n1; n2 = -n2; }
+        s[f] = (n0 * (x[0] - p[0]) + n1 * (x[1] - p[1])) + n2 * (x[2] - p[2]);
+    }
+}
+
+/* Greedy walk; at most hop_limit moves (bounded loop). */
+__device__ __forceinline__ int32_t tet_walk(const TetMeshK& m, int32_t t, const double x[3],
+                                            int hop_limit, int& status, int& hops)
+{
+    hops = 0;
+    for (int it = 0; it <= hop_limit; ++it) {
+        double s[4];
+        tet_signed(m, t, x, s);
+        int fb = 0;
+        double smax = s[0];
+#pragma unroll
+        for (int f = 1; f < 4; ++f)
+            if (s[f] > smax) { smax = s[f]; fb = f; }
+        if (!(smax > 0.0)) {
+            status = TWALK_OK;
+            return t;
+        }
+        const int32_t nb = __ldg(m.nbr + 4 * (int64_t)t + fb);
+        if (nb < 0) {
+            status = TWALK_EXIT;
+            return t;
+        }
+        if (hops >= hop_limit) break;
+        t = nb;
+        ++hops;
+    }
+    status = TWALK_HOPS;
+    return t;
+}
+
+template <class V>
+__device__ __forceinline__ int tet_find_cloud(const TetStepArgs<V>& a, int64_t tile)
+{
+    int lo = 0, hi = a.nclouds - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&a.clouds[mid].tile0) <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class V>
+struct TetMinBlocks {
+    static constexpr int value = 2;
+};
+
+template <class V, int DEP>
+__global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const TetStepArgs<V> a)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    constexpr bool DET = (DEP == DEP_DET1 || DEP == DEP_DET2);
+    const PhysK<V>& ph = a.phys;
+    int cur_cloud = -1;
+    Quant qp = {0.0, 0.0, 0.0f, 0.0f, 0, false};
+    double amax = 0.0;
+    unsigned ovf = 0, nlost = 0;
+    unsigned hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+
+    for (int64_t tile = warp0; tile < a.total_tiles; tile += nwarps) {
+        const int c = (a.nclouds == 1) ? 0 : tet_find_cloud(a, tile);
+        if (c != cur_cloud) {
+            if (cur_cloud >= 0) flush_ctl<DEP>(a.ctl + cur_cloud, lane, amax, ovf, nlost);
+            cur_cloud = c;
+            if (DET) qp = make_quant(a.ctl[c].L, a.ctl[c].H + QUANT_GROWTH_BITS);
+        }
+        const CloudK<double, V>* cl = a.clouds + c;
+        const int64_t n = __ldg(&cl->n);
+        unsigned long long* const acc = DET ? cl->acc : nullptr;
+        double* const src = (DEP == DEP_ATOMIC) ? cl->src : nullptr;
+        for (int sl = 0; sl < WARP_TILE / 32; ++sl) {
+        const int64_t i = (tile - __ldg(&cl->tile0)) * WARP_TILE + 32 * sl + lane;
+        int32_t key = -1;
+        V dep[3] = {(V)0, (V)0, (V)0};
+        if (i < n) {
+            double pos[3] = {ld_stream(cl->x + i), ld_stream(cl->y + i), ld_stream(cl->z + i)};
+            V vel[3] = {ld_stream(cl->u + i), ld_stream(cl->v + i), ld_stream(cl->w + i)};
+            const V d = ld_stream(cl->d + i) * ph.dscale;
+            int32_t cur = ld_stream(cl->cell + i);
+            const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
+            const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
+            const V* Uc = a.U + 3 * (int64_t)cur;
+            V uc[3] = {__ldg(Uc) * a.fscale, __ldg(Uc + 1) * a.fscale, __ldg(Uc + 2) * a.fscale};
+            V state0[3] = {vel[0], vel[1], vel[2]};
+            double posNew[3] = {pos[0], pos[1], pos[2]};
+            V velNew[3] = {vel[0], vel[1], vel[2]};
+            int32_t tNew = cur;
+            bool lost = false;
+            for (int t = 1; t <= ph.nsub; ++t) {
+                if (ph.drag == 0) {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) velNew[k] = (vel[k] + f * uc[k]) / ((V)1 + f);
+                } else {
+                    V du[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) du[k] = uc[k] - vel[k];
+                    V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
+                    V Re = (mag * d) * ph.rnu;
+                    V pw;
+                    if (sizeof(V) == 4) pw = (V)st_pow0687f((float)Re);
+                    else pw = (V)st_pow0687((double)Re);
+                    V g = f * ((V)1 + (V)0.15 * pw);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) velNew[k] = vel[k] + g * du[k];
+                }
+#pragma unroll
+                for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (double)velNew[k] * a.dtP;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if (posNew[k] < a.mesh.origin[k] || posNew[k] > a.mesh.ending[k]) {
+                        posNew[k] = pos[k];
+                        velNew[k] = -vel[k];
+                        state0[k] -= (V)2 * vel[k];
+                    }
+                }
+                int status = TWALK_OK, hops = 0;
+                tNew = tet_walk(a.mesh, tNew, posNew, a.mesh.hop_limit, status, hops);
+                if (status != TWALK_OK) { lost = true; break; }
+                if (a.hop_hist && DEP != DEP_PROBE) {
+                    const int hb = hops < 7 ? hops : 7;
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) hist[k] += (hb == k);
+                }
+                if (t != ph.nsub && tNew != cur) {
+                    V di[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) di[k] = mB * (state0[k] - velNew[k]);
+                    if (DEP == DEP_PROBE) {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) track_max(di[k], amax);
+                    } else {
+                        deposit_direct<DEP, V>(di, (int64_t)cur, acc, src, qp, amax, ovf);
+                    }
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) state0[k] = velNew[k];
+                    const V* Un = a.U + 3 * (int64_t)tNew;
+                    uc[0] = __ldg(Un) * a.fscale;
+                    uc[1] = __ldg(Un + 1) * a.fscale;
+                    uc[2] = __ldg(Un + 2) * a.fscale;
+                    cur = tNew;
+                }
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { vel[k] = velNew[k]; pos[k] = posNew[k]; }
+            }
+            if (lost) {
+                ++nlost;
+            } else {
+                if (DEP != DEP_PROBE) {
+                    st_stream(cl->x + i, posNew[0]);
+                    st_stream(cl->y + i, posNew[1]);
+                    st_stream(cl->z + i, posNew[2]);
+                    st_stream(cl->u + i, velNew[0]);
+                    st_stream(cl->v + i, velNew[1]);
+                    st_stream(cl->w + i, velNew[2]);
+                    st_stream(cl->cell + i, tNew);
+                }
+                key = cur;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) dep[k] = mB * (state0[k] - velNew[k]);
+            }
+        }
+        deposit_warp<DEP, V>(key, dep, acc, src, qp, lane, amax, ovf);
+        }
+    }
+    if (cur_cloud >= 0) flush_ctl<DEP>(a.ctl + cur_cloud, lane, amax, ovf, nlost);
+    if (a.hop_hist && DEP != DEP_PROBE) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const unsigned v = __reduce_add_sync(FULL_MASK, hist[k]);
+            if (lane == 0 && v) atomicAdd(a.hop_hist + k, (unsigned long long)v);
+        }
+    }
+}
+
+template <class V>
+cudaError_t launch_step_tet(const TetStepArgs<V>& a, int dep, int grid, int block, cudaStream_t s)
+{
+    switch (dep) {
+    case DEP_DET1: k_step_tet<V, DEP_DET1><<<grid, block, 0, s>>>(a); break;
+    case DEP_DET2: k_step_tet<V, DEP_DET2><<<grid, block, 0, s>>>(a); break;
+    case DEP_ATOMIC: k_step_tet<V, DEP_ATOMIC><<<grid, block, 0, s>>>(a); break;
+    case DEP_PROBE: k_step_tet<V, DEP_PROBE><<<grid, block, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <class V>
+int step_tet_max_active_blocks(int dep, int block)
+{
+    int nb = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (dep) {
+    case DEP_DET1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_DET1>, block, 0); break;
+    case DEP_DET2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_DET2>, block, 0); break;
+    case DEP_ATOMIC: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_ATOMIC>, block, 0); break;
+    case DEP_PROBE: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_PROBE>, block, 0); break;
+    default: break;
+    }
+    return e == cudaSuccess ? nb : 0;
+}
+
+__global__ void k_tet_locate(const TetMeshK m, const double* __restrict__ x,
+                             const double* __restrict__ y, const double* __restrict__ z,
+                             const int32_t* __restrict__ hint, int64_t n,
+                             int32_t* __restrict__ cells, unsigned long long* outside)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double p[3] = {x[i], y[i], z[i]};
+        int32_t h = hint[i];
+        int status = TWALK_EXIT, hops = 0;
+        int32_t t = -1;
+        if (h >= 0 && h < m.nt) t = tet_walk(m, h, p, m.hop_limit, status, hops);
+        const bool ok = status == TWALK_OK;
+        cells[i] = ok ? t : -1;
+        if (!ok) atomicAdd(outside, 1ULL);
+    }
+}
+
+cudaError_t launch_tet_locate(const TetMeshK& m, const double* x, const double* y,
+                              const double* z, const int32_t* hint, int64_t n, int32_t* cells,
+                              unsigned long long* outside, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    int64_t g = (n + 255) / 256;
+    if (g > 148 * 16) g = 148 * 16;
+    k_tet_locate<<<(int)g, 256, 0, s>>>(m, x, y, z, hint, n, cells, outside);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_step_tet<float>(const TetStepArgs<float>&, int, int, int, cudaStream_t);
+template cudaError_t launch_step_tet<double>(const TetStepArgs<double>&, int, int, int, cudaStream_t);
+template int step_tet_max_active_blocks<float>(int, int);
+template int step_tet_max_active_blocks<double>(int, int);
+
+}  // namespace st

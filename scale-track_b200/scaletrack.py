@@ -41,6 +41,7 @@ EXPORTS = [
     "st_allocate_array", "st_evolve_cloud", "st_finalize", "st_step_noalloc",
     "st_noalloc_max_cells", "st_mean_source_forward", "st_mean_source_pullback",
     "st_graph_capture", "st_graph_launch", "st_graph_release", "st_autotune",
+    "st_create_tet", "st_set_parcels_tet", "st_tet_hop_histogram",
 ]
 
 
@@ -53,6 +54,14 @@ class ScaleTrackError(RuntimeError):
 class MeshDesc(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int32 * 3), ("origin", ctypes.c_double * 3),
                 ("ending", ctypes.c_double * 3)]
+
+
+class TetMeshDesc(ctypes.Structure):
+    _fields_ = [("n_vertices", ctypes.c_int64), ("vertices", ctypes.c_void_p),
+                ("n_tets", ctypes.c_int64), ("tets", ctypes.c_void_p),
+                ("neighbors", ctypes.c_void_p), ("origin", ctypes.c_double * 3),
+                ("ending", ctypes.c_double * 3), ("hop_limit", ctypes.c_int32),
+                ("pad", ctypes.c_int32)]
 
 
 class Params(ctypes.Structure):
@@ -129,6 +138,11 @@ def lib():
         "st_graph_launch": ([c_h], ctypes.c_int),
         "st_graph_release": ([c_h], ctypes.c_int),
         "st_autotune": ([c_h, ctypes.c_double, ctypes.c_int, P(TuneResult)], ctypes.c_int),
+        "st_create_tet": ([P(Params), P(TetMeshDesc), ctypes.c_int, P(c_h)], ctypes.c_int),
+        "st_set_parcels_tet": ([c_h, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                               ctypes.c_int),
+        "st_tet_hop_histogram": ([c_h, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
         "st_mean_source_forward": ([c_h, ctypes.c_int, P(AdjointDesc), ctypes.c_void_p],
                                    ctypes.c_int),
         "st_mean_source_pullback": ([c_h, ctypes.c_int, P(AdjointDesc), ctypes.c_void_p,
@@ -166,6 +180,28 @@ def mesh_desc(n, origin, ending):
     return m
 
 
+def tet_mesh_desc(vertices, tets, neighbors, origin, ending, hop_limit=0):
+    """Tetrahedral mesh filling the box [origin, ending]: vertices [nv][3] (FP64), tets and
+    neighbours [nt][4] (int32; neighbour across the face opposite local vertex f, -1 on
+    the boundary).  The returned descriptor keeps the arrays alive."""
+    verts = np.ascontiguousarray(vertices, dtype=np.float64)
+    tt = np.ascontiguousarray(tets, dtype=np.int32)
+    nb = np.ascontiguousarray(neighbors, dtype=np.int32)
+    assert verts.ndim == 2 and verts.shape[1] == 3
+    assert tt.shape == nb.shape and tt.ndim == 2 and tt.shape[1] == 4
+    m = TetMeshDesc()
+    m.n_vertices = verts.shape[0]
+    m.vertices = verts.ctypes.data
+    m.n_tets = tt.shape[0]
+    m.tets = tt.ctypes.data
+    m.neighbors = nb.ctypes.data
+    m.origin = (ctypes.c_double * 3)(*[float(x) for x in _vec3(origin)])
+    m.ending = (ctypes.c_double * 3)(*[float(x) for x in _vec3(ending)])
+    m.hop_limit = int(hop_limit)
+    m._keep = (verts, tt, nb)
+    return m
+
+
 def params(**kw):
     """st_params with the library defaults (the reference's setup.jl) overridden by kw.
     String values are accepted for drag_model, precision and deposit."""
@@ -195,8 +231,9 @@ class ParcelTracker:
         self._h = ctypes.c_void_p()
         self.params = prm
         self.mesh = mesh
-        _check(lib().st_create(ctypes.byref(prm), ctypes.byref(mesh), device,
-                               ctypes.byref(self._h)))
+        self.tet = isinstance(mesh, TetMeshDesc)
+        create = lib().st_create_tet if self.tet else lib().st_create
+        _check(create(ctypes.byref(prm), ctypes.byref(mesh), device, ctypes.byref(self._h)))
         self.ncells = int(lib().st_num_cells(self._h))
 
     def close(self):
@@ -220,13 +257,27 @@ class ParcelTracker:
     def handle(self):
         return self._h
 
-    def set_parcels(self, xyz, uvw, d, cloud=0):
+    def set_parcels(self, xyz, uvw, d, cloud=0, hint=None):
+        """hint: starting tet per parcel for the walk to the owning tet (tet meshes only)."""
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         uvw = np.ascontiguousarray(uvw, dtype=np.float64)
         d = np.ascontiguousarray(d, dtype=np.float64)
         n = d.shape[0]
         assert xyz.shape == (3, n) and uvw.shape == (3, n)
-        _check(lib().st_set_parcels(self._h, cloud, n, _dptr(xyz), _dptr(uvw), _dptr(d)))
+        if self.tet:
+            h = None if hint is None else np.ascontiguousarray(hint, dtype=np.int32)
+            assert h is None or h.shape == (n,)
+            _check(lib().st_set_parcels_tet(self._h, cloud, n, _dptr(xyz), _dptr(uvw),
+                                            _dptr(d), _dptr(h)))
+        else:
+            assert hint is None, "hint is for tet meshes"
+            _check(lib().st_set_parcels(self._h, cloud, n, _dptr(xyz), _dptr(uvw), _dptr(d)))
+
+    def hop_histogram(self, reset=False):
+        """Walk lengths per substep since the last reset: [k] = walks of k hops, [7] = 7+."""
+        out = np.zeros(8, dtype=np.uint64)
+        _check(lib().st_tet_hop_histogram(self._h, _dptr(out), int(reset)))
+        return out
 
     def num_parcels(self, cloud=0):
         return int(lib().st_num_parcels(self._h, cloud))

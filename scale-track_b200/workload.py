@@ -35,6 +35,10 @@ CONFIGS = {
     # needs dt_sub / tau_p < 2
     "c3_clouds_64": dict(n=64, nclouds=64, seed=2, precision="mixed", steps=100, substeps=10,
                          size_min=1_000, size_max=2_000_000, dmed_min=5e-6, dmed_max=50e-6),
+    # 96^3 hexes x 6 tets, vertices jittered +-0.15 h (seed 1), 2e7 parcels, U0 = 3 m/s,
+    # mixed precision, 200 steps, face-walk relocation
+    "c2_tets_96": dict(n=96, nparcels=20_000_000, seed=0, mesh_seed=1, jitter=0.15,
+                       precision="mixed", steps=200, U0=3.0, sort_interval=20),
     # adjoint: 128^3 hex, 1e6 parcels, 200 steps, checkpoints every 20 steps; the target
     # source comes from a forward run with drag multiplier 1.1 and diameters x 0.95
     "c4_adjoint_128": dict(n=128, nparcels=1_000_000, seed=3, precision="mixed", steps=200,
@@ -73,6 +77,96 @@ def parcels(nparcels, seed, L=L_BOX, d_median=20e-6, sigma=0.3, dtype_v=np.float
     return xyz, uvw, d.astype(np.float64)
 
 
+# Each hex (cube vertices numbered v0 = (0,0,0), v1 = (1,0,0), v2 = (1,1,0), v3 = (0,1,0),
+# v4..v7 the same at z = 1) splits into six tetrahedra around the diagonal v0-v6; the split is
+# conforming between neighbouring hexes and every tet is positively oriented.
+KUHN_TETS = ((0, 1, 2, 6), (0, 2, 3, 6), (0, 3, 7, 6), (0, 7, 4, 6), (0, 4, 5, 6), (0, 5, 1, 6))
+CUBE = ((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1))
+
+
+def _morton3(i, j, k):
+    def spread(v):
+        v = v.astype(np.uint64) & np.uint64(0x3FF)
+        v = (v | (v << np.uint64(16))) & np.uint64(0x030000FF)
+        v = (v | (v << np.uint64(8))) & np.uint64(0x0300F00F)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x030C30C3)
+        v = (v | (v << np.uint64(2))) & np.uint64(0x09249249)
+        return v
+    return spread(i) | (spread(j) << np.uint64(1)) | (spread(k) << np.uint64(2))
+
+
+def kuhn_tet_mesh(n, L=L_BOX, jitter=0.15, seed=1):
+    """n^3 hexes on [0, L]^3, each split into 6 tets; vertices jittered uniformly by +-jitter*h
+    (seeded), boundary vertices only tangentially so the walls stay planar.  Hexes are
+    numbered in Morton order and tet = 6 hex + s.  Returns (vertices [nv,3] float64,
+    tets [nt,4] int32, neighbours [nt,4] int32 (tet across the face opposite local vertex f,
+    -1 on the boundary), hex_ijk [nhex,3])."""
+    h = L / n
+    g = np.arange(n + 1)
+    vk, vj, vi = np.meshgrid(g, g, g, indexing="ij")
+    ijk = np.stack([vi.ravel(), vj.ravel(), vk.ravel()], axis=1)
+    verts = ijk.astype(np.float64) * h
+    rng = np.random.default_rng(seed)
+    jit = rng.uniform(-jitter * h, jitter * h, verts.shape)
+    jit[(ijk == 0) | (ijk == n)] = 0.0          # walls stay planar
+    verts = verts + jit
+    hk, hj, hi = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    hex_ijk = np.stack([hi.ravel(), hj.ravel(), hk.ravel()], axis=1)
+    order = np.argsort(_morton3(hex_ijk[:, 0], hex_ijk[:, 1], hex_ijk[:, 2]), kind="stable")
+    hex_ijk = hex_ijk[order]
+    nh = hex_ijk.shape[0]
+
+    def vid(o):
+        c = hex_ijk + np.array(CUBE[o])
+        return (c[:, 2] * (n + 1) + c[:, 1]) * (n + 1) + c[:, 0]
+
+    corner = np.stack([vid(o) for o in range(8)], axis=1)
+    tets = np.empty((nh, 6, 4), dtype=np.int32)
+    for s_, t in enumerate(KUHN_TETS):
+        tets[:, s_, :] = corner[:, list(t)]
+    tets = tets.reshape(-1, 4)
+    nt = tets.shape[0]
+    # neighbours by matching sorted face triples
+    faces = np.empty((nt, 4, 3), dtype=np.int64)
+    for f in range(4):
+        faces[:, f, :] = np.sort(np.delete(tets, f, axis=1), axis=1)
+    faces = faces.reshape(-1, 3)
+    key = (faces[:, 0] * (n + 1) ** 3 + faces[:, 1]) * (n + 1) ** 3 + faces[:, 2]
+    srt = np.argsort(key, kind="stable")
+    ks = key[srt]
+    nbr = -np.ones(nt * 4, dtype=np.int64)
+    same = ks[1:] == ks[:-1]
+    a, b = srt[:-1][same], srt[1:][same]
+    nbr[a] = b // 4
+    nbr[b] = a // 4
+    return verts, tets, nbr.reshape(nt, 4).astype(np.int32), hex_ijk
+
+
+def tet_centroids(verts, tets):
+    return verts[tets].mean(axis=1)
+
+
+def tgv_at(points, U0=1.0, L=L_BOX, dtype=np.float32):
+    """The Taylor-Green-like field evaluated at given points [m, 3] (tet centroids)."""
+    a, b, c = (np.pi * points[:, k] / L for k in range(3))
+    U = np.empty((points.shape[0], 3), dtype=np.float64)
+    U[:, 0] = U0 * np.sin(a) * np.cos(b) * np.cos(c)
+    U[:, 1] = -U0 * np.cos(a) * np.sin(b) * np.cos(c)
+    U[:, 2] = 0.0
+    return U.astype(dtype)
+
+
+def tet_hints(xyz, hex_ijk, n, L=L_BOX):
+    """A starting tet for each parcel: the first tet of the hex of the unjittered lattice."""
+    h = L / n
+    ijk = np.clip(np.floor(xyz / h).astype(np.int64), 0, n - 1)
+    rank = np.empty(n ** 3, dtype=np.int64)
+    lin = (hex_ijk[:, 2] * n + hex_ijk[:, 1]) * n + hex_ijk[:, 0]
+    rank[lin] = np.arange(hex_ijk.shape[0])
+    hx = rank[(ijk[2] * n + ijk[1]) * n + ijk[0]]
+    return (6 * hx).astype(np.int32)
+
+
 def cloud_sizes(cfg):
     """Cloud sizes log-uniform in [size_min, size_max] and per-cloud median diameters."""
     rng = np.random.default_rng(cfg["seed"])
@@ -97,6 +191,16 @@ def algorithmic_bytes(precision, nparcels, ncells):
     bp = {"mixed": 76, "fp64": 104, "fp32": 52}[precision]
     bc = {"mixed": 36, "fp64": 48, "fp32": 36}[precision]
     return nparcels * bp + ncells * bc
+
+
+def tet_step_kernel_bytes(precision, nparcels, ntets, nverts):
+    """Compulsory traffic of the tet step kernel: the parcel state as on cuboid meshes plus
+    the owning tet read and written (8 B), and once per step every tet's U (12 or 24 B),
+    vertex ids (16 B) and neighbours (16 B) and every vertex (24 B); with several parcels per
+    tet every tet is visited."""
+    bp = {"mixed": 76, "fp64": 104}[precision] + 8
+    bt = {"mixed": 12, "fp64": 24}[precision] + 32
+    return nparcels * bp + ntets * bt + nverts * 24
 
 
 def step_kernel_bytes(precision, nparcels, ncells):
