@@ -131,6 +131,7 @@ struct st_handle {
     unsigned long long* dcount = nullptr;  /* scratch counter (outside parcels) */
     void* dclouds = nullptr;
     std::vector<unsigned char> hclouds;      /* host image of the CloudK array */
+    std::vector<unsigned char> hclouds2;     /* host image of the two-parity pair (capture) */
     std::vector<CloudBufs> clouds;
     bool clouds_dirty = true;
     bool need_probe = true;
@@ -397,6 +398,13 @@ int do_step(st_handle* h, double dt, double fscale)
                    : (const CloudK<P, V>*)h->dclouds;
     a.ctl = h->dctl;
     a.total_tiles = h->total_tiles;
+    if (h->p.n_clouds == 1) {
+        const std::vector<unsigned char>& hc = h->capturing ? h->hclouds2 : h->hclouds;
+        const size_t off = h->capturing ? (size_t)h->cap_parity * sizeof(CloudK<P, V>) : 0;
+        memcpy(&a.one, hc.data() + off, sizeof(CloudK<P, V>));
+    } else {
+        memset(&a.one, 0, sizeof a.one);
+    }
     if (a.total_tiles == 0) return ST_OK;
     int grid = h->grid;
     const int64_t warps_per_block = h->block / 32;
@@ -737,6 +745,8 @@ int upload_clouds_pair(st_handle* h)
         }
         v[nc + c] = k;
     }
+    h->hclouds2.resize(sizeof(CloudK<P, V>) * 2 * nc);
+    memcpy(h->hclouds2.data(), v.data(), h->hclouds2.size());
     if (!h->dclouds2) CK(cudaMalloc(&h->dclouds2, 2 * 256 * (size_t)nc));
     CK(cudaMemcpyAsync(h->dclouds2, v.data(), sizeof(CloudK<P, V>) * 2 * nc,
                        cudaMemcpyHostToDevice, h->stream));
@@ -774,6 +784,7 @@ int graph_capture(st_handle* h, int n, double dt, const double* fs)
         a.clouds = (const CloudK<P, V>*)h->dclouds;
         a.ctl = h->dctl;
         a.total_tiles = h->total_tiles;
+        memcpy(&a.one, h->hclouds.data(), sizeof(CloudK<P, V>));
         if (a.total_tiles > 0) {
             CK(launch_step<P, V>(a, DEP_PROBE, h->grid, h->block, h->stream));
             CK(launch_set_scale(h->dctl, h->p.n_clouds, h->stream));

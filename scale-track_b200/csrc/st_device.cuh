@@ -23,16 +23,20 @@ __device__ __forceinline__ double st_floor(double v) { return floor(v); }
 __device__ __forceinline__ float st_sqrt(float v) { return __fsqrt_rn(v); }
 __device__ __forceinline__ double st_sqrt(double v) { return __dsqrt_rn(v); }
 
-/* floor(label, v) (A:668-670); values outside int32 mark the parcel as lost. */
+__device__ __forceinline__ int32_t st_floor_int(float v) { return __float2int_rd(v); }
+__device__ __forceinline__ int32_t st_floor_int(double v) { return __double2int_rd(v); }
+
+/* floor(label, v) (A:668-670); values outside int32 mark the parcel as lost.  floor(v) lies
+ * in [-2^31, 2^31) exactly when v does (both bounds are integers), so the range test is made
+ * on v and one round-down conversion gives the label. */
 template <class P>
 __device__ __forceinline__ int32_t floor_label(P v, bool& bad)
 {
-    P f = st_floor(v);
-    if (!(f >= (P)-2147483648.0 && f < (P)2147483648.0)) {
+    if (!(v >= (P)-2147483648.0 && v < (P)2147483648.0)) {
         bad = true;
         return 0;
     }
-    return (int32_t)f;
+    return st_floor_int(v);
 }
 
 /* ------------------------------------------------------------------------------------ */
@@ -58,11 +62,20 @@ __device__ __forceinline__ double ldexp2(double x, int k)
     return (x * st_pow2i(k1)) * st_pow2i(k2);
 }
 
-/* largest finite |v| seen (probe pass) */
+/* The running maximum of |deposit| is kept in the velocity precision (AmaxT<V>): every
+ * deposit is a V value, so the maximum is exact in V and needs no conversion per deposit. */
 template <class V>
-__device__ __forceinline__ void track_max(V v, double& amax)
+using AmaxT = V;
+
+/* largest finite |v| seen (probe pass) */
+__device__ __forceinline__ void track_max(float v, float& amax)
 {
-    const double a = fabs((double)v);
+    const float a = fabsf(v);
+    if (a < __int_as_float(0x7f800000)) amax = fmaxf(amax, a);
+}
+__device__ __forceinline__ void track_max(double v, double& amax)
+{
+    const double a = fabs(v);
     if (a < __longlong_as_double(0x7ff0000000000000LL)) amax = fmax(amax, a);
 }
 
@@ -94,12 +107,14 @@ __device__ __forceinline__ Quant make_quant(int L, int cap)
 /* Quantises one deposit component: 0 for zero, non-finite or out-of-range values (the
  * latter two are counted in `ovf`).  `amax` tracks the largest finite |dep| for the next
  * step's scale (max is order-independent, so the scale is reproducible). */
-__device__ __forceinline__ long long quantize(double dv, const Quant& qp, double& amax,
+template <class A>
+__device__ __forceinline__ long long quantize(double dv, const Quant& qp, A& amax,
                                               unsigned& ovf)
 {
     const double a = fabs(dv);
     if (a == 0.0) return 0;
-    if (a < __longlong_as_double(0x7ff0000000000000LL)) amax = fmax(amax, a);
+    /* exact for A = float: dv is then a float value */
+    if (a < __longlong_as_double(0x7ff0000000000000LL)) amax = (A)fmax((double)amax, a);
     if (!(a < qp.thr)) {
         ++ovf;
         return 0;
@@ -108,13 +123,13 @@ __device__ __forceinline__ long long quantize(double dv, const Quant& qp, double
     return __double2ll_rn(x);
 }
 
-__device__ __forceinline__ long long quantize(float dv, const Quant& qp, double& amax,
+__device__ __forceinline__ long long quantize(float dv, const Quant& qp, float& amax,
                                               unsigned& ovf)
 {
     if (!qp.fast) return quantize((double)dv, qp, amax, ovf);
     const float a = fabsf(dv);
     if (a == 0.0f) return 0;
-    if (a < __int_as_float(0x7f800000)) amax = fmax(amax, (double)a);
+    if (a < __int_as_float(0x7f800000)) amax = fmaxf(amax, a);
     if (!(a < qp.thr_f)) {
         ++ovf;
         return 0;
@@ -125,7 +140,7 @@ __device__ __forceinline__ long long quantize(float dv, const Quant& qp, double&
 template <int DEP, class V>
 __device__ __forceinline__ void deposit_direct(const V dep[3], int64_t cell0,
                                                unsigned long long* acc, double* src,
-                                               const Quant& qp, double& amax, unsigned& ovf)
+                                               const Quant& qp, AmaxT<V>& amax, unsigned& ovf)
 {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -175,7 +190,7 @@ __device__ __forceinline__ void st_stream(T* p, T v) { __stcs(p, v); }
 template <int DEP, class V>
 __device__ __forceinline__ void deposit_warp(int32_t key, const V dep[3],
                                              unsigned long long* acc, double* src,
-                                             const Quant& qp, int lane, double& amax,
+                                             const Quant& qp, int lane, AmaxT<V>& amax,
                                              unsigned& ovf)
 {
     if (DEP == DEP_PROBE) {
@@ -235,12 +250,12 @@ __device__ __forceinline__ void deposit_warp(int32_t key, const V dep[3],
 
 /* Warp-aggregated bookkeeping for one cloud: largest deposit exponent, lost parcels and
  * range errors.  Called when a warp moves on to another cloud and at the end. */
-template <int DEP>
-__device__ __forceinline__ void flush_ctl(CloudCtl* ctl, int lane, double& amax, unsigned& ovf,
+template <int DEP, class A>
+__device__ __forceinline__ void flush_ctl(CloudCtl* ctl, int lane, A& amax, unsigned& ovf,
                                           unsigned& lost)
 {
     if (DEP != DEP_ATOMIC) {
-        const int e = amax > 0.0 ? exp_of(amax) : EXP_NONE;
+        const int e = amax > (A)0 ? exp_of((double)amax) : EXP_NONE;
         const int wmax = __reduce_max_sync(FULL_MASK, e);
         if (lane == 0 && wmax != EXP_NONE) atomicMax(&ctl->emax, wmax);
     }
@@ -251,7 +266,7 @@ __device__ __forceinline__ void flush_ctl(CloudCtl* ctl, int lane, double& amax,
         if (nlost && DEP != DEP_PROBE) atomicAdd(&ctl->lost, (unsigned long long)nlost);
         if (novf && DEP != DEP_PROBE) atomicAdd(&ctl->overflow, (unsigned long long)novf);
     }
-    amax = 0.0;
+    amax = (A)0;
     ovf = 0;
     lost = 0;
 }

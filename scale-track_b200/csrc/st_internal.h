@@ -89,6 +89,7 @@ struct StepArgs {
     const CloudK<P, V>* clouds; /* [nclouds] device array */
     CloudCtl* ctl;              /* [nclouds] */
     int64_t total_tiles;        /* warp tiles (32 parcels) over all clouds */
+    CloudK<P, V> one;           /* with one cloud: its descriptor, read from parameter space */
 };
 
 /* Unstructured tetrahedral mesh (st_tet.cu). */

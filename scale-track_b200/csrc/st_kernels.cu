@@ -97,7 +97,7 @@ __device__ __forceinline__ int find_cloud(const StepArgs<P, V>& a, int64_t tile)
 template <class P, class V, int DEP>
 __device__ __forceinline__ void evolve_parcel(const StepArgs<P, V>& a, P pos[3], V vel[3], V d,
                                               int32_t posI, V uc[3], unsigned long long* acc,
-                                              double* src, const Quant& qp, double& amax,
+                                              double* src, const Quant& qp, AmaxT<V>& amax,
                                               unsigned& ovf, bool& lost, int32_t& key,
                                               V dep[3])
 {
@@ -252,7 +252,7 @@ struct MinBlocks {
     static constexpr int value = sizeof(V) == 8 ? ST_MIN_BLOCKS_FP64 : ST_MIN_BLOCKS;
 };
 
-template <class P, class V, int DEP, bool ONE>
+template <class P, class V, int DEP, bool ONE, bool SINGLE>
 __global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArgs<P, V> a)
 {
     const int lane = threadIdx.x & 31;
@@ -262,28 +262,29 @@ __global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArg
 
     int cur = -1;
     Quant qp = {0.0, 0.0, 0};
-    double amax = 0.0;
+    AmaxT<V> amax = (V)0;
     unsigned ovf = 0, nlost = 0;
 
     for (int64_t tile = warp0; tile < a.total_tiles; tile += nwarps) {
-        const int c = (a.nclouds == 1) ? 0 : find_cloud(a, tile);
+        const int c = SINGLE ? 0 : find_cloud(a, tile);
         if (c != cur) {
             if (cur >= 0) flush_ctl<DEP>(a.ctl + cur, lane, amax, ovf, nlost);
             cur = c;
             if (DET) qp = make_quant(a.ctl[c].L, a.ctl[c].H + QUANT_GROWTH_BITS);
         }
-        const CloudK<P, V>* cl = a.clouds + c;
-        const int64_t n = __ldg(&cl->n);
-        const int64_t base = (tile - __ldg(&cl->tile0)) * TILE + lane;
-        P* const xp = cl->x;
-        P* const yp = cl->y;
-        P* const zp = cl->z;
-        V* const up = cl->u;
-        V* const vp = cl->v;
-        V* const wp = cl->w;
-        const V* const dp = cl->d;
-        unsigned long long* const acc = DET ? cl->acc : nullptr;
-        double* const src = (DEP == DEP_ATOMIC) ? cl->src : nullptr;
+        /* one cloud: the descriptor comes from parameter space (no loads per tile) */
+        const CloudK<P, V>& cl = SINGLE ? a.one : a.clouds[c];
+        const int64_t n = cl.n;
+        const int64_t base = (tile - cl.tile0) * TILE + lane;
+        P* const xp = cl.x;
+        P* const yp = cl.y;
+        P* const zp = cl.z;
+        V* const up = cl.u;
+        V* const vp = cl.v;
+        V* const wp = cl.w;
+        const V* const dp = cl.d;
+        unsigned long long* const acc = DET ? cl.acc : nullptr;
+        double* const src = (DEP == DEP_ATOMIC) ? cl.src : nullptr;
 
         /* phase 1: every load of the tile in flight at once (streaming, evict-first) */
         P X[SLICES], Y[SLICES], Z[SLICES];
@@ -356,15 +357,15 @@ __global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArg
     if (cur >= 0) flush_ctl<DEP>(a.ctl + cur, lane, amax, ovf, nlost);
 }
 
-template <class P, class V, bool ONE>
+template <class P, class V, bool ONE, bool SINGLE>
 static cudaError_t launch_step_t(const StepArgs<P, V>& a, int dep, int grid, int block,
                                  cudaStream_t s)
 {
     switch (dep) {
-    case DEP_DET1: k_step<P, V, DEP_DET1, ONE><<<grid, block, 0, s>>>(a); break;
-    case DEP_DET2: k_step<P, V, DEP_DET2, ONE><<<grid, block, 0, s>>>(a); break;
-    case DEP_ATOMIC: k_step<P, V, DEP_ATOMIC, ONE><<<grid, block, 0, s>>>(a); break;
-    case DEP_PROBE: k_step<P, V, DEP_PROBE, ONE><<<grid, block, 0, s>>>(a); break;
+    case DEP_DET1: k_step<P, V, DEP_DET1, ONE, SINGLE><<<grid, block, 0, s>>>(a); break;
+    case DEP_DET2: k_step<P, V, DEP_DET2, ONE, SINGLE><<<grid, block, 0, s>>>(a); break;
+    case DEP_ATOMIC: k_step<P, V, DEP_ATOMIC, ONE, SINGLE><<<grid, block, 0, s>>>(a); break;
+    case DEP_PROBE: k_step<P, V, DEP_PROBE, ONE, SINGLE><<<grid, block, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -373,20 +374,23 @@ static cudaError_t launch_step_t(const StepArgs<P, V>& a, int dep, int grid, int
 template <class P, class V>
 cudaError_t launch_step(const StepArgs<P, V>& a, int dep, int grid, int block, cudaStream_t s)
 {
-    return a.phys.nsub == 1 ? launch_step_t<P, V, true>(a, dep, grid, block, s)
-                            : launch_step_t<P, V, false>(a, dep, grid, block, s);
+    if (a.nclouds == 1)
+        return a.phys.nsub == 1 ? launch_step_t<P, V, true, true>(a, dep, grid, block, s)
+                                : launch_step_t<P, V, false, true>(a, dep, grid, block, s);
+    return a.phys.nsub == 1 ? launch_step_t<P, V, true, false>(a, dep, grid, block, s)
+                            : launch_step_t<P, V, false, false>(a, dep, grid, block, s);
 }
 
-template <class P, class V, bool ONE>
+template <class P, class V, bool ONE, bool SINGLE>
 static int max_active_t(int dep, int block)
 {
     int nb = 0;
     cudaError_t e = cudaErrorInvalidValue;
     switch (dep) {
-    case DEP_DET1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_DET1, ONE>, block, 0); break;
-    case DEP_DET2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_DET2, ONE>, block, 0); break;
-    case DEP_ATOMIC: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_ATOMIC, ONE>, block, 0); break;
-    case DEP_PROBE: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_PROBE, ONE>, block, 0); break;
+    case DEP_DET1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_DET1, ONE, SINGLE>, block, 0); break;
+    case DEP_DET2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_DET2, ONE, SINGLE>, block, 0); break;
+    case DEP_ATOMIC: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_ATOMIC, ONE, SINGLE>, block, 0); break;
+    case DEP_PROBE: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step<P, V, DEP_PROBE, ONE, SINGLE>, block, 0); break;
     default: break;
     }
     return e == cudaSuccess ? nb : 0;
@@ -395,10 +399,13 @@ static int max_active_t(int dep, int block)
 template <class P, class V>
 int step_max_active_blocks(int dep, int block)
 {
-    /* both variants are compiled with the same launch bounds; take the smaller */
-    int a = max_active_t<P, V, true>(dep, block);
-    int b = max_active_t<P, V, false>(dep, block);
-    return a < b ? a : b;
+    /* all variants are compiled with the same launch bounds; take the smallest */
+    int m = max_active_t<P, V, true, true>(dep, block);
+    const int r[3] = {max_active_t<P, V, false, true>(dep, block),
+                      max_active_t<P, V, true, false>(dep, block),
+                      max_active_t<P, V, false, false>(dep, block)};
+    for (int v : r) m = v < m ? v : m;
+    return m;
 }
 
 template cudaError_t launch_step<float, float>(const StepArgs<float, float>&, int, int, int, cudaStream_t);

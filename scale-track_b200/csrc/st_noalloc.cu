@@ -188,6 +188,7 @@ ST_API int st_step_noalloc(const st_params* p, const st_mesh_desc* m, int64_t n,
     a.clouds = cloud;
     a.ctl = ctl;
     a.total_tiles = (n + WARP_TILE - 1) / WARP_TILE;
+    a.one = ck;
 
     cudaError_t e;
     if ((e = cudaMemsetAsync(acc, 0, (size_t)ncomp * sizeof(unsigned long long), s)) != cudaSuccess)

@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
     const PhysK<V>& ph = a.phys;
     int cur_cloud = -1;
     Quant qp = {0.0, 0.0, 0.0f, 0.0f, 0, false};
-    double amax = 0.0;
+    AmaxT<V> amax = (V)0;
     unsigned ovf = 0, nlost = 0;
     unsigned hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
