@@ -234,15 +234,15 @@ __device__ __forceinline__ void evolve_one(const StepArgs<P, V>& a, P pos[3], V 
 }
 
 /* The step kernel.  A warp owns a tile of SLICES x 32 consecutive parcels (lane l holds
- * parcels l, l+32, l+64, l+96 of the tile): all loads of the tile are issued first, then the
- * start cells are located and the cell velocities gathered for every slice, then each slice
- * is stepped, stored and its deposits reduced.  Tiles are distributed over the persistent
- * grid with a fixed stride; the clouds of a multi-cloud launch occupy consecutive tile
- * ranges. */
+ * parcels l, l+32, l+64, l+96 of the tile): all loads of the tile are issued one tile ahead
+ * (while the previous tile is stepped), then the start cells are located and the cell
+ * velocities gathered for every slice, then each slice is stepped, stored and its deposits
+ * reduced.  Tiles are distributed over the persistent grid with a fixed stride; the clouds
+ * of a multi-cloud launch occupy consecutive tile ranges. */
 /* Resident blocks of 256 threads per SM the compiler must allow (a register budget):
- * 4 (64 registers) for FP32 velocities, 3 (80 registers) for FP64, whose state is wider. */
+ * 3 (80 registers), which holds the two tiles of the software pipeline without spills. */
 #ifndef ST_MIN_BLOCKS
-#define ST_MIN_BLOCKS 4
+#define ST_MIN_BLOCKS 3
 #endif
 #ifndef ST_MIN_BLOCKS_FP64
 #define ST_MIN_BLOCKS_FP64 3
@@ -265,14 +265,42 @@ __global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArg
     AmaxT<V> amax = (V)0;
     unsigned ovf = 0, nlost = 0;
 
+    /* Software pipeline over the warp's tiles: the streaming loads of the next tile are
+     * issued before the current tile is stepped, so each warp keeps two tiles of parcel data
+     * in flight and the HBM latency overlaps the arithmetic. */
+    struct Raw {
+        P X[SLICES], Y[SLICES], Z[SLICES];
+        V Uv[SLICES], Vv[SLICES], Wv[SLICES], D[SLICES];
+    };
+    auto load = [&](int64_t t, Raw& r) {   /* every load of tile t (streaming, evict-first) */
+        const int cc = SINGLE ? 0 : find_cloud(a, t);
+        const CloudK<P, V>& cl = SINGLE ? a.one : a.clouds[cc];
+        const int64_t n = cl.n;
+        const int64_t base = (t - cl.tile0) * TILE + lane;
+#pragma unroll
+        for (int s = 0; s < SLICES; ++s) {
+            const int64_t i = base + 32 * s;
+            if (i < n) {
+                r.X[s] = ld_stream(cl.x + i);
+                r.Y[s] = ld_stream(cl.y + i);
+                r.Z[s] = ld_stream(cl.z + i);
+                r.Uv[s] = ld_stream(cl.u + i);
+                r.Vv[s] = ld_stream(cl.v + i);
+                r.Wv[s] = ld_stream(cl.w + i);
+                r.D[s] = ld_stream(cl.d + i);
+            }
+        }
+    };
+    Raw R, RN;
+    if (warp0 < a.total_tiles) load(warp0, R);
     for (int64_t tile = warp0; tile < a.total_tiles; tile += nwarps) {
+        if (tile + nwarps < a.total_tiles) load(tile + nwarps, RN);
         const int c = SINGLE ? 0 : find_cloud(a, tile);
         if (c != cur) {
             if (cur >= 0) flush_ctl<DEP>(a.ctl + cur, lane, amax, ovf, nlost);
             cur = c;
             if (DET) qp = make_quant(a.ctl[c].L, a.ctl[c].H + QUANT_GROWTH_BITS);
         }
-        /* one cloud: the descriptor comes from parameter space (no loads per tile) */
         const CloudK<P, V>& cl = SINGLE ? a.one : a.clouds[c];
         const int64_t n = cl.n;
         const int64_t base = (tile - cl.tile0) * TILE + lane;
@@ -282,26 +310,16 @@ __global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArg
         V* const up = cl.u;
         V* const vp = cl.v;
         V* const wp = cl.w;
-        const V* const dp = cl.d;
         unsigned long long* const acc = DET ? cl.acc : nullptr;
         double* const src = (DEP == DEP_ATOMIC) ? cl.src : nullptr;
-
-        /* phase 1: every load of the tile in flight at once (streaming, evict-first) */
         P X[SLICES], Y[SLICES], Z[SLICES];
         V Uv[SLICES], Vv[SLICES], Wv[SLICES], D[SLICES];
 #pragma unroll
         for (int s = 0; s < SLICES; ++s) {
-            const int64_t i = base + 32 * s;
-            if (i < n) {
-                X[s] = ld_stream(xp + i);
-                Y[s] = ld_stream(yp + i);
-                Z[s] = ld_stream(zp + i);
-                Uv[s] = ld_stream(up + i);
-                Vv[s] = ld_stream(vp + i);
-                Wv[s] = ld_stream(wp + i);
-                D[s] = ld_stream(dp + i);
-            }
+            X[s] = R.X[s]; Y[s] = R.Y[s]; Z[s] = R.Z[s];
+            Uv[s] = R.Uv[s]; Vv[s] = R.Vv[s]; Wv[s] = R.Wv[s]; D[s] = R.D[s];
         }
+        R = RN;
         /* phase 2: start cells (A:1286) and cell velocities (A:1288) */
         int32_t pI[SLICES];
         V uc[SLICES][3];

@@ -5,9 +5,10 @@
  * which cell it ends up in.  Cell indices must agree bit for bit between the CUDA kernels
  * and the CPU oracle, so the power function cannot come from two different math libraries
  * (CUDA's pow and glibc's pow differ in the last ulp for some arguments).  This header is
- * compiled unchanged by nvcc (device) and gcc (host) and uses only IEEE-754 +, -, *, /
- * (correctly rounded on both), integer bit manipulation and comparisons.  Both sides must be
- * built without contraction of a*b+c into fma: nvcc --fmad=false, gcc -ffp-contract=off.
+ * compiled unchanged by nvcc (device) and gcc (host) and uses only IEEE-754 +, -, *, / and
+ * explicit fma (correctly rounded on both), integer bit manipulation and comparisons.  Both
+ * sides must be built without implicit contraction of a*b+c into fma: nvcc --fmad=false,
+ * gcc -ffp-contract=off.
  *
  * Method (textbook, no library constants):
  *   pow(x, a) = exp(a ln x)
@@ -16,8 +17,9 @@
  *          remainder < 1e-18 relative).  See Abramowitz & Stegun 4.1.28 (ln((1+s)/(1-s))).
  *   exp y: Cody & Waite (1980) reduction y = k ln2 + r, |r| <= ln2/2, e^r by its Taylor series
  *          to r^14/14! (remainder < 5e-18), result scaled by 2^k through the exponent field.
- * Accuracy: a few ulp in double (st_pow0687) and 1 ulp in single (st_pow0687f), far below
- * what the drag model needs; the point is that host and device produce the same bits.
+ * Accuracy: a few ulp in double (st_pow0687) and 2 ulp in single (st_pow0687f, a separate
+ * polynomial method described at its definition), far below what the drag model needs; the
+ * point is that host and device produce the same bits.
  * Checked against libm pow by the CPU tests and host vs device bit-equality by the GPU
  * tests.
  */
@@ -30,6 +32,7 @@
 #define ST_HD __host__ __device__ __forceinline__
 #else
 #define ST_HD static inline
+#include <math.h>
 #include <string.h>
 #endif
 
@@ -162,21 +165,34 @@ ST_HD float st_pow2if(int k)
     return st_float_of((uint32_t)(k + 127) << 23);
 }
 
-/* x^0.687 for the FP32 and mixed drag (the drag is evaluated in FP32).  Same method as
- * st_pow0687 with float-sized series: ln m = 2s(1 + z/3 + ... + z^4/9) in float (remainder
- * < 3e-9), e^r to r^7/7! in float (remainder < 6e-9).  The exponent bookkeeping
- * y = 0.687 (e ln 2 + ln m) and the reduction r = y - k ln 2 are done in double: in float
- * their rounding would cost |y| ulp of the result.  At most 1 ulp from the correctly
- * rounded value over the physical range (the CPU tests check this against libm). */
+/* Fused multiply-add, correctly rounded on both sides (glibc's fmaf and the GPU's FFMA
+ * round once), so explicit fma calls give the same bits on host and device even though
+ * neither compiler may contract a*b+c on its own. */
+ST_HD float st_fmaf(float a, float b, float c)
+{
+#if defined(__CUDA_ARCH__)
+    return __fmaf_rn(a, b, c);
+#else
+    return fmaf(a, b, c);
+#endif
+}
+
+/* x^0.687 for the FP32 and mixed drag (the drag is evaluated in FP32).
+ *   x = 2^e m, m in [sqrt(1/2), sqrt(2)), t = m - 1 (exact);
+ *   687 e = 1000 k + r with integer k and 0 <= r < 1000, so 0.687 e = k + r/1000 exactly;
+ *   x^0.687 = (1 + t)^0.687 * 2^(r/1000) * 2^k,
+ * the first two factors by polynomials (degree 8 in t, degree 6 in r; coefficients fitted by
+ * least squares on Chebyshev nodes, pow_coeffs.py, approximation error below 0.05 ulp each)
+ * evaluated by Horner's rule with fma, the last by the exponent field.  All arithmetic is
+ * single precision or integer; nothing is converted to double.
+ * Within 2 ulp of the correctly rounded value for every normal and subnormal x (the CPU
+ * tests check this against a double-precision reference). */
 ST_HD float st_pow0687f(float x)
 {
-    const double LN2 = 0.69314718055994530942;
-    const double INV_LN2 = 1.44269504088896340736;
-    const float SQRT2 = 1.4142135f;
     if (!(x > 0.0f)) return x != x ? x : 0.0f;
-    if (x > 3.0e38f) return x;
-    int e = 0;
     uint32_t b = st_bits_of_f(x);
+    if ((b >> 23) == 0xff) return x;               /* +inf */
+    int e = 0;
     if ((b >> 23) == 0) {                          /* subnormal */
         x = x * 16777216.0f;                       /* 2^24, exact */
         e = -24;
@@ -184,33 +200,31 @@ ST_HD float st_pow0687f(float x)
     }
     e += (int)((b >> 23) & 0xff) - 127;
     float m = st_float_of((b & 0x007fffffu) | 0x3f800000u); /* [1,2) */
-    if (m > SQRT2) {
+    if (m > 1.41421356f) {
         m = m * 0.5f;
         e += 1;
     }
-    float s = (m - 1.0f) / (m + 1.0f);
-    float z = s * s;
-    float p = 1.0f / 9.0f;
-    p = p * z + 1.0f / 7.0f;
-    p = p * z + 1.0f / 5.0f;
-    p = p * z + 1.0f / 3.0f;
-    p = p * z + 1.0f;
-    float lnm = (2.0f * s) * p;
-    double y = 0.687 * ((double)e * LN2 + (double)lnm);
-    double t = y * INV_LN2;
-    int k = (int)(t >= 0.0 ? t + 0.5 : t - 0.5);
-    float r = (float)(y - (double)k * LN2);
-    float q = 1.0f / 5040.0f;
-    q = q * r + 1.0f / 720.0f;
-    q = q * r + 1.0f / 120.0f;
-    q = q * r + 1.0f / 24.0f;
-    q = q * r + 1.0f / 6.0f;
-    q = q * r + 0.5f;
-    q = q * r + 1.0f;
-    q = q * r + 1.0f;
-    int k1 = k / 2;
-    int k2 = k - k1;
-    return (q * st_pow2if(k1)) * st_pow2if(k2);
+    const float t = m - 1.0f;
+    float p = -0x1.921f0ep-8f;
+    p = st_fmaf(p, t, 0x1.68372ap-7f);
+    p = st_fmaf(p, t, -0x1.b6bb7ep-7f);
+    p = st_fmaf(p, t, 0x1.2657a8p-6f);
+    p = st_fmaf(p, t, -0x1.bd5c3ap-6f);
+    p = st_fmaf(p, t, 0x1.817e2ap-5f);
+    p = st_fmaf(p, t, -0x1.b862bep-4f);
+    p = st_fmaf(p, t, 0x1.5fbe76p-1f);
+    p = st_fmaf(p, t, 1.0f);
+    const int y = 687 * e;                         /* |y| <= 102363 */
+    const int k = y >= 0 ? y / 1000 : -((999 - y) / 1000);   /* floor(y / 1000) */
+    const float r = (float)(y - 1000 * k);         /* exact integer in [0, 1000) */
+    float q = 0x1.08638ep-72f;
+    q = st_fmaf(q, r, 0x1.6dafdep-60f);
+    q = st_fmaf(q, r, 0x1.5cea7ap-47f);
+    q = st_fmaf(q, r, 0x1.e8030ap-35f);
+    q = st_fmaf(q, r, 0x1.01f20ep-22f);
+    q = st_fmaf(q, r, 0x1.6b689cp-11f);
+    q = st_fmaf(q, r, 1.0f);
+    return (p * q) * st_pow2if(k);                 /* -103 <= k <= 87 */
 }
 
 #endif /* ST_POW_H */

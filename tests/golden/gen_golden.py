@@ -13,14 +13,15 @@ Reference file (A:): run/icoJuliaParcelFoam/cavity3D/asyncParallelTracking.jl
   Mesh construction (Float64 -> Float32) ..... A:237-268
 
 The Schiller-Naumann drag is project-defined (the reference only has Stokes drag); its
-power functions follow the same textbook algorithms as scale-track_b200/csrc/st_pow.h,
-restated here in Python floats (double) and numpy float32 scalars (single).
+power functions follow the same algorithms as scale-track_b200/csrc/st_pow.h, restated here
+in Python floats (double) and numpy float32 scalars with an exact-rational fma (single).
 
 Run:  python tests/golden/gen_golden.py      (rewrites the .npz files next to this script)
 """
 import math
 import os
 import struct
+from fractions import Fraction
 
 import numpy as np
 
@@ -98,47 +99,65 @@ def _ffrom(b):
     return np.array([b], dtype=np.uint32).view(np.float32)[0]
 
 
+def fmaf(a, b, c):
+    """Single-precision fused multiply-add, rounded once: a*b + c is formed exactly as a
+    rational number and rounded to the nearest binary32 value (ties to even)."""
+    v = Fraction(float(a)) * Fraction(float(b)) + Fraction(float(c))
+    if v == 0:
+        return F(0)
+    sign = -1 if v < 0 else 1
+    v = abs(v)
+    ex = v.numerator.bit_length() - v.denominator.bit_length()
+    if Fraction(2) ** ex > v:
+        ex -= 1                                   # now 2^ex <= v < 2^(ex+1)
+    quantum = Fraction(2) ** (max(ex, -126) - 23)
+    q = v / quantum
+    n = q.numerator // q.denominator
+    rem = q - n
+    if rem > Fraction(1, 2) or (rem == Fraction(1, 2) and n % 2 == 1):
+        n += 1
+    return F(sign * float(n * quantum))          # exact: n * quantum is a binary32 value
+
+
+# coefficients of st_pow0687f (printed by scale-track_b200/csrc/pow_coeffs.py)
+_PT = [float.fromhex(h) for h in ("0x1p+0", "0x1.5fbe76p-1", "-0x1.b862bep-4", "0x1.817e2ap-5",
+                                  "-0x1.bd5c3ap-6", "0x1.2657a8p-6", "-0x1.b6bb7ep-7",
+                                  "0x1.68372ap-7", "-0x1.921f0ep-8")]
+_PR = [float.fromhex(h) for h in ("0x1p+0", "0x1.6b689cp-11", "0x1.01f20ep-22",
+                                  "0x1.e8030ap-35", "0x1.5cea7ap-47", "0x1.6dafdep-60",
+                                  "0x1.08638ep-72")]
+
+
 def pow0687f(x):
-    """Single-precision x^0.687 (same algorithm as st_pow0687f): float series, double
-    exponent bookkeeping; numpy float32 scalars and Python floats."""
+    """Single-precision x^0.687 (same algorithm as st_pow0687f): x = 2^e m, t = m - 1,
+    687 e = 1000 k + r; (1+t)^0.687 and 2^(r/1000) by Horner with fma, times 2^k."""
     x = F(x)
     if not (x > F(0)):
         return x if x != x else F(0)
-    if x > F(3.0e38):
-        return x
-    LN2 = 0.69314718055994530942
-    INV_LN2 = 1.44269504088896340736
-    e = 0
     b = _fbits(x)
+    if (b >> 23) == 0xFF:
+        return x
+    e = 0
     if (b >> 23) == 0:
         x = F(x * F(16777216.0))
         e = -24
         b = _fbits(x)
     e += ((b >> 23) & 0xFF) - 127
     m = _ffrom((b & 0x007FFFFF) | 0x3F800000)
-    if m > F(1.4142135):
+    if m > F(1.41421356):
         m = F(m * F(0.5))
         e += 1
-    s = F(F(m - F(1)) / F(m + F(1)))
-    z = F(s * s)
-    p = F(F(1) / F(9))
-    for c in (7.0, 5.0, 3.0):
-        p = F(F(p * z) + F(F(1) / F(c)))
-    p = F(F(p * z) + F(1))
-    lnm = F(F(F(2) * s) * p)
-    y = 0.687 * (float(e) * LN2 + float(lnm))
-    t = y * INV_LN2
-    k = int(t + 0.5) if t >= 0.0 else -int(-t + 0.5)
-    r = F(y - float(k) * LN2)
-    q = F(F(1) / F(5040))
-    for c in (720.0, 120.0, 24.0, 6.0):
-        q = F(F(q * r) + F(F(1) / F(c)))
-    q = F(F(q * r) + F(0.5))
-    q = F(F(q * r) + F(1))
-    q = F(F(q * r) + F(1))
-    k1 = int(k / 2)
-    k2 = k - k1
-    return F(F(q * _ffrom((k1 + 127) << 23)) * _ffrom((k2 + 127) << 23))
+    t = F(m - F(1))
+    p = F(_PT[8])
+    for c in reversed(_PT[:8]):
+        p = fmaf(p, t, F(c))
+    y = 687 * e
+    k = y // 1000                                 # floor division
+    r = F(y - 1000 * k)
+    q = F(_PR[6])
+    for c in reversed(_PR[:6]):
+        q = fmaf(q, r, F(c))
+    return F(F(p * q) * _ffrom((k + 127) << 23))
 
 
 # ----------------------------------------------------------------------------- the step
