@@ -137,6 +137,35 @@ __device__ __forceinline__ long long quantize(float dv, const Quant& qp, float& 
     return __float2ll_rn(dv * qp.scale_f);
 }
 
+/* The three components of one deposit.  In single precision with the fast scale: when
+ * |d0| + |d1| + |d2| (rounded, which cannot fall below a power-of-two bound any single term
+ * reaches) is below the range bound, every component is finite and in range, and each is
+ * scaled and rounded directly, with the same integers and the same maximum as the
+ * per-component path; otherwise (and in double precision) each component goes through
+ * quantize, which counts what does not fit. */
+__device__ __forceinline__ void quantize3(const float d[3], const Quant& qp, float& amax,
+                                          unsigned& ovf, long long q[3])
+{
+    if (qp.fast) {
+        const float a0 = fabsf(d[0]), a1 = fabsf(d[1]), a2 = fabsf(d[2]);
+        if ((a0 + a1) + a2 < qp.thr_f) {
+            amax = fmaxf(amax, fmaxf(fmaxf(a0, a1), a2));
+#pragma unroll
+            for (int k = 0; k < 3; ++k) q[k] = __float2ll_rn(d[k] * qp.scale_f);
+            return;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) q[k] = quantize(d[k], qp, amax, ovf);
+}
+
+__device__ __forceinline__ void quantize3(const double d[3], const Quant& qp, double& amax,
+                                          unsigned& ovf, long long q[3])
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k) q[k] = quantize(d[k], qp, amax, ovf);
+}
+
 template <int DEP, class V>
 __device__ __forceinline__ void deposit_direct(const V dep[3], int64_t cell0,
                                                unsigned long long* acc, double* src,
@@ -205,10 +234,7 @@ __device__ __forceinline__ void deposit_warp(int32_t key, const V dep[3],
         return;
     }
     long long q[3] = {0, 0, 0};
-    if (key >= 0) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) q[k] = quantize(dep[k], qp, amax, ovf);
-    }
+    if (key >= 0) quantize3(dep, qp, amax, ovf, q);
     const int prev = __shfl_up_sync(FULL_MASK, key, 1);
     const bool head = (lane == 0) || (prev != key);
     const unsigned heads = __ballot_sync(FULL_MASK, head);
