@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--no-tets", dest="tets", action="store_false",
                     help="skip configuration 2 (tet mesh)")
     ap.add_argument("--tet-steps", type=int, default=workload.CONFIGS["c2_tets_96"]["steps"])
+    ap.add_argument("--tet-nparcels", type=int, default=workload.CONFIGS["c2_tets_96"]["nparcels"])
+    ap.add_argument("--tets-only", action="store_true",
+                    help="time configuration 2 alone and print its object (profiling runs)")
     ap.add_argument("--no-clouds", dest="clouds", action="store_false",
                     help="skip the configuration-3 multi-cloud timing")
     return ap.parse_args()
@@ -383,7 +386,7 @@ def run_ours(args):
 
     # ---- face walk on the jittered tet mesh ----
     if not args.no_extras and rank == 0 and args.tets:
-        extras["tets"] = run_tets(st, torch, local, dev, args.tet_steps)
+        extras["tets"] = run_tets(st, torch, local, dev, args.tet_steps, args.tet_nparcels)
 
     # ---- adjoint of the time-averaged source ----
     if not args.no_extras and rank == 0 and args.adjoint:
@@ -473,13 +476,14 @@ def run_clouds(st, torch, local, dev):
             "ms_per_step_graph": ms_graph / steps, "ms_per_step_launches": ms_plain / steps}
 
 
-def run_tets(st, torch, local, dev, steps):
+def run_tets(st, torch, local, dev, steps, npcl=None):
     """Configuration 2: 96^3 hexes split into 6 jittered tets (5,308,416 tets), 2e7 parcels,
     carrier field U0 = 3 m/s at the tet centroids, Schiller-Naumann, one substep, mixed
     precision, greedy face walk after every position update, re-sort by owning tet every 20
     steps."""
     c = workload.CONFIGS["c2_tets_96"]
-    n, npcl, dt = c["n"], c["nparcels"], workload.DT
+    n, dt = c["n"], workload.DT
+    npcl = npcl or c["nparcels"]
     verts, tets, nbr, hex_ijk = workload.kuhn_tet_mesh(n, workload.L_BOX, c["jitter"],
                                                        c["mesh_seed"])
     xyz, uvw, d = workload.parcels(npcl, c["seed"])
@@ -529,7 +533,7 @@ def run_tets(st, torch, local, dev, steps):
         sync(h)
     peak, peak_src = measured_hbm_peak()
     step_avg = step_ms / max(nstep, 1)
-    algo = workload.tet_step_kernel_bytes(c["precision"], npcl, tets.shape[0], verts.shape[0])
+    algo = workload.tet_step_kernel_bytes(c["precision"], npcl, tets.shape[0])
     walks = float(hops.sum())
     return {"workload": "BASELINE config 2: 96^3 x 6 jittered tets (5,308,416), 2e7 parcels, "
                         "U0 = 3 m/s, Schiller-Naumann, dt = 1e-4 s, 1 substep, mixed precision, "
@@ -677,7 +681,13 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.tets_only:
+        import torch
+        import scaletrack as st
+        torch.cuda.set_device(0)
+        print(json.dumps(run_tets(st, torch, 0, torch.device("cuda", 0), a.tet_steps,
+                                  a.tet_nparcels)), flush=True)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

@@ -8,11 +8,12 @@
  * Canonical order: every tet's vertex ids are first sorted in increasing order, its
  * neighbour list permuted with them (canonical_tets), so the three vertices of a face shared
  * by two tets appear in the same order in both.
- * Face planes (computed at use, FP64): face f of tet (v0, v1, v2, v3) is opposite v_f, with
- * vertices (p, q, r) the other three in increasing order; n = (q - p) x (r - p), negated
- * when n . (v_f - p) > 0 so that it points out of the tet; the signed distance of a point x
- * is s_f = n . (x - p).  x is inside the closed tet when every s_f <= 0.  Both tets of a
- * shared face compute the same n bit for bit, up to the exact negation, so a point is never
+ * Face planes (FP64): face f of tet (v0, v1, v2, v3) is opposite v_f, with vertices
+ * (p, q, r) the other three in increasing order; n = (q - p) x (r - p), negated when
+ * n . (v_f - p) > 0 so that it points out of the tet, and c = n . p; the signed distance of
+ * a point x is s_f = n . x - c (sums left to right).  x is inside the closed tet when every
+ * s_f <= 0.  Both tets of a shared face compute the same (n, c) bit for bit up to the exact
+ * negation, so their signed distances are exact negatives of each other: a point is never
  * outside both of them (no walk can bounce between two tets).
  * Walk: from the current tet, if some s_f > 0 move across the face with the largest s_f
  * (first index on ties) to the neighbour; stop when inside, when the face is on the boundary
@@ -61,23 +62,34 @@ inline void canonical_tets(int64_t nt, const int32_t* tets, const int32_t* nbr, 
     }
 }
 
-inline void tet_signed(const TetMesh& m, int32_t t, const double x[3], double s[4])
+/* Plane (n0, n1, n2, c) of face f of tet t. */
+inline void tet_plane(const TetMesh& m, int32_t t, int f, double pl[4])
 {
+    static const int F[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
     const double* v[4];
     for (int k = 0; k < 4; ++k) v[k] = m.verts + 3 * (int64_t)m.tets[4 * (int64_t)t + k];
-    static const int F[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+    const double* p = v[F[f][0]];
+    const double* q = v[F[f][1]];
+    const double* r = v[F[f][2]];
+    const double a0 = q[0] - p[0], a1 = q[1] - p[1], a2 = q[2] - p[2];
+    const double b0 = r[0] - p[0], b1 = r[1] - p[1], b2 = r[2] - p[2];
+    double n0 = a1 * b2 - a2 * b1;
+    double n1 = a2 * b0 - a0 * b2;
+    double n2 = a0 * b1 - a1 * b0;
+    const double e = (n0 * (v[f][0] - p[0]) + n1 * (v[f][1] - p[1])) + n2 * (v[f][2] - p[2]);
+    if (e > 0.0) { n0 = -n0; n1 = -n1; n2 = -n2; }
+    pl[0] = n0;
+    pl[1] = n1;
+    pl[2] = n2;
+    pl[3] = (n0 * p[0] + n1 * p[1]) + n2 * p[2];
+}
+
+inline void tet_signed(const TetMesh& m, int32_t t, const double x[3], double s[4])
+{
     for (int f = 0; f < 4; ++f) {
-        const double* p = v[F[f][0]];
-        const double* q = v[F[f][1]];
-        const double* r = v[F[f][2]];
-        const double a0 = q[0] - p[0], a1 = q[1] - p[1], a2 = q[2] - p[2];
-        const double b0 = r[0] - p[0], b1 = r[1] - p[1], b2 = r[2] - p[2];
-        double n0 = a1 * b2 - a2 * b1;
-        double n1 = a2 * b0 - a0 * b2;
-        double n2 = a0 * b1 - a1 * b0;
-        const double e = (n0 * (v[f][0] - p[0]) + n1 * (v[f][1] - p[1])) + n2 * (v[f][2] - p[2]);
-        if (e > 0.0) { n0 = -n0; n1 = -n1; n2 = -n2; }
-        s[f] = (n0 * (x[0] - p[0]) + n1 * (x[1] - p[1])) + n2 * (x[2] - p[2]);
+        double pl[4];
+        tet_plane(m, t, f, pl);
+        s[f] = ((pl[0] * x[0] + pl[1] * x[1]) + pl[2] * x[2]) - pl[3];
     }
 }
 

@@ -157,6 +157,7 @@ struct st_handle {
     TetMeshK tmesh = {};
     double* d_verts = nullptr;
     int32_t* d_tets = nullptr;
+    double4* d_planes = nullptr;            /* [nt][4] face planes */
     int32_t* d_nbr = nullptr;
     unsigned long long* d_hops = nullptr;   /* walk-length histogram [8] */
     /* CUDA-graph replay of a step sequence */
@@ -1169,6 +1170,7 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
         const size_t nv = (size_t)tm->n_vertices, nt = (size_t)tm->n_tets;
         if ((e = cudaMalloc((void**)&h->d_verts, nv * 3 * sizeof(double))) != cudaSuccess ||
             (e = cudaMalloc((void**)&h->d_tets, nt * 4 * sizeof(int32_t))) != cudaSuccess ||
+            (e = cudaMalloc((void**)&h->d_planes, nt * 4 * sizeof(double4))) != cudaSuccess ||
             (e = cudaMalloc((void**)&h->d_nbr, nt * 4 * sizeof(int32_t))) != cudaSuccess ||
             (e = cudaMalloc((void**)&h->d_hops, 8 * sizeof(unsigned long long))) != cudaSuccess)
             return bail(fail(e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA,
@@ -1181,11 +1183,18 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
                                  cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
             (e = cudaMemsetAsync(h->d_hops, 0, 8 * sizeof(unsigned long long), h->stream)) !=
                 cudaSuccess ||
+            (e = launch_tet_planes(h->d_verts, h->d_tets, (int64_t)nt, h->d_planes,
+                                   h->stream)) != cudaSuccess ||
             (e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
-            return bail(fail(ST_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e)));
+            return bail(fail(ST_ERR_CUDA, "tet mesh set-up: %s", cudaGetErrorString(e)));
+        h->launches += 1;
+        /* the walk needs only the planes and the neighbours */
+        cudaFree(h->d_verts);
+        cudaFree(h->d_tets);
+        h->d_verts = nullptr;
+        h->d_tets = nullptr;
         TetMeshK& k = h->tmesh;
-        k.verts = h->d_verts;
-        k.tets = h->d_tets;
+        k.planes = h->d_planes;
         k.nbr = h->d_nbr;
         k.nt = (int64_t)nt;
         for (int a = 0; a < 3; ++a) {
@@ -1285,7 +1294,7 @@ int st_destroy(st_handle* h)
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
     void* arrs[] = {h->dU, h->dsrc, h->dacc, h->dctl, h->dcounter, h->dcount, h->dclouds,
-                    h->dstage, h->adj.mem, h->dclouds2, h->d_verts, h->d_tets, h->d_nbr,
+                    h->dstage, h->adj.mem, h->dclouds2, h->d_verts, h->d_tets, h->d_planes, h->d_nbr,
                     h->d_hops};
     for (void* p : arrs)
         if (p) cudaFree(p);

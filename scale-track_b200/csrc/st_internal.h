@@ -94,11 +94,10 @@ struct StepArgs {
 
 /* Unstructured tetrahedral mesh (st_tet.cu). */
 struct TetMeshK {
-    const double* verts;        /* [nv][3] */
-    const int32_t* tets;        /* [nt][4] vertex indices */
+    const double4* planes;      /* [nt][4] outward face planes (n0, n1, n2, c), s = n.x - c */
     const int32_t* nbr;         /* [nt][4] tet across the face opposite local vertex k, or -1 */
     int64_t nt;
-    double origin[3];           /* box of the walls */
+    double origin[3];
     double ending[3];
     int32_t hop_limit;          /* face-walk hops per substep before a parcel counts as lost */
     int32_t pad;
@@ -126,6 +125,9 @@ template <class V>
 int step_tet_max_active_blocks(int dep, int block);
 /* Walks every parcel from hint[i] to the tet that contains it (hop limit of the mesh);
  * cells[i] = tet or -1, and `outside` counts failures. */
+/* Face planes of every tet (canonical vertex order) from vertices and vertex ids. */
+cudaError_t launch_tet_planes(const double* verts, const int32_t* tets, int64_t nt,
+                              double4* planes, cudaStream_t s);
 cudaError_t launch_tet_locate(const TetMeshK& m, const double* x, const double* y,
                               const double* z, const int32_t* hint, int64_t n, int32_t* cells,
                               unsigned long long* outside, cudaStream_t s);

@@ -7,14 +7,15 @@
  * position outside the box keeps its old coordinate on that axis and mirrors the old
  * velocity component (the reference's wall rule, A:1313-1329), then a greedy walk moves from
  * the current tet across the face with the largest positive signed distance until the
- * position is inside.  Face planes are computed at use in FP64 from the tet's four vertices
- * (the 22 MB vertex array of configuration 2 stays in L2).  Each tet's vertex ids are stored
- * in increasing order (st_create_tet sorts them and permutes the neighbours with them), and
+ * position is inside.  The four FP64 face planes of every tet are computed once, when the
+ * mesh is created (k_tet_planes), from its vertices with the vertex ids in increasing order
+ * (st_create_tet sorts them and permutes the neighbours with them):
  *   face f opposite vertex f, (p, q, r) = the other vertices in increasing order,
- *   n = (q - p) x (r - p), negated if n . (v_f - p) > 0; s_f(x) = n . (x - p); inside iff all
- *   s_f <= 0; ties between faces go to the lowest index.
- * The two tets of a shared face therefore compute the same plane bit for bit up to an exact
- * negation: a point is never outside both, and no walk bounces between two tets.
+ *   n = (q - p) x (r - p), negated if n . (v_f - p) > 0, c = n . p; s_f(x) = n . x - c;
+ *   inside iff all s_f <= 0; ties between faces go to the lowest index.
+ * The two tets of a shared face therefore hold the same plane bit for bit up to an exact
+ * negation: a point is never outside both, and no walk bounces between two tets.  A walk
+ * step reads 128 bytes of planes (one dependent load level) and costs 24 FP64 operations.
  * The same arithmetic, without fused multiply-adds, is in the CPU oracle, so owning tets agree
  * bit for bit.  A walk that reaches a boundary face or exceeds the hop limit marks the parcel
  * as lost (its state is left unchanged and the host reports it).  Deposits use the same
@@ -29,22 +30,33 @@ namespace st {
 
 enum { TWALK_OK = 0, TWALK_EXIT = 1, TWALK_HOPS = 2 };
 
+/* Signed distances of x to the four face planes of tet t (planes read as 2 x 16 bytes). */
 __device__ __forceinline__ void tet_signed(const TetMeshK& m, int32_t t, const double x[3],
                                            double s[4])
 {
-    const int4 tv = __ldg(reinterpret_cast<const int4*>(m.tets) + t);
-    const int ids[4] = {tv.x, tv.y, tv.z, tv.w};
-    double v[4][3];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const double* pv = m.verts + 3 * (int64_t)ids[k];
-        v[k][0] = __ldg(pv);
-        v[k][1] = __ldg(pv + 1);
-        v[k][2] = __ldg(pv + 2);
-    }
-    const int F[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+    const double2* pl = reinterpret_cast<const double2*>(m.planes + 4 * (int64_t)t);
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
+        const double2 nxy = __ldg(pl + 2 * f);
+        const double2 nzc = __ldg(pl + 2 * f + 1);
+        s[f] = ((nxy.x * x[0] + nxy.y * x[1]) + nzc.x * x[2]) - nzc.y;
+    }
+}
+
+/* Face planes at mesh creation: face f of tet t is opposite its vertex f (vertex ids in
+ * increasing order), (p, q, r) the other three in increasing order, n = (q - p) x (r - p)
+ * negated if n . (v_f - p) > 0, c = n . p. */
+__global__ void k_tet_planes(const double* __restrict__ verts, const int32_t* __restrict__ tets,
+                             int64_t nt, double4* __restrict__ planes)
+{
+    const int F[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 4 * nt;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = i >> 2;
+        const int f = (int)(i & 3);
+        const double* v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = verts + 3 * (int64_t)tets[4 * t + k];
         const double* p = v[F[f][0]];
         const double* q = v[F[f][1]];
         const double* r = v[F[f][2]];
@@ -55,8 +67,18 @@ __device__ __forceinline__ void tet_signed(const TetMeshK& m, int32_t t, const d
         double n2 = a0 * b1 - a1 * b0;
         const double e = (n0 * (v[f][0] - p[0]) + n1 * (v[f][1] - p[1])) + n2 * (v[f][2] - p[2]);
         if (e > 0.0) { n0 = -n0; n1 = -n1; n2 = -n2; }
-        s[f] = (n0 * (x[0] - p[0]) + n1 * (x[1] - p[1])) + n2 * (x[2] - p[2]);
+        planes[i] = make_double4(n0, n1, n2, (n0 * p[0] + n1 * p[1]) + n2 * p[2]);
     }
+}
+
+cudaError_t launch_tet_planes(const double* verts, const int32_t* tets, int64_t nt,
+                              double4* planes, cudaStream_t s)
+{
+    if (nt == 0) return cudaSuccess;
+    int64_t g = (4 * nt + 255) / 256;
+    if (g > 148 * 32) g = 148 * 32;
+    k_tet_planes<<<(int)g, 256, 0, s>>>(verts, tets, nt, planes);
+    return cudaGetLastError();
 }
 
 /* Greedy walk; at most hop_limit moves (bounded loop). */
@@ -101,12 +123,19 @@ __device__ __forceinline__ int tet_find_cloud(const TetStepArgs<V>& a, int64_t t
     return lo;
 }
 
+#ifndef ST_TET_PREFETCH
+#define ST_TET_PREFETCH 1
+#endif
+/* Resident blocks of 256 threads per SM the compiler must allow: 4 (64 registers). */
+#ifndef ST_TET_MIN_BLOCKS
+#define ST_TET_MIN_BLOCKS 4
+#endif
 template <class V>
 struct TetMinBlocks {
-    static constexpr int value = 2;
+    static constexpr int value = ST_TET_MIN_BLOCKS;
 };
 
-template <class V, int DEP>
+template <class V, int DEP, bool ONE>
 __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const TetStepArgs<V> a)
 {
     const int lane = threadIdx.x & 31;
@@ -118,7 +147,12 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
     Quant qp = {0.0, 0.0, 0.0f, 0.0f, 0, false};
     AmaxT<V> amax = (V)0;
     unsigned ovf = 0, nlost = 0;
-    unsigned hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int nsub = ONE ? 1 : ph.nsub;
+    /* walk-length histogram of the block, flushed once at the end */
+    __shared__ unsigned s_hist[8];
+    const bool count_hops = a.hop_hist != nullptr && DEP != DEP_PROBE;
+    if (threadIdx.x < 8) s_hist[threadIdx.x] = 0;
+    __syncthreads();
 
     for (int64_t tile = warp0; tile < a.total_tiles; tile += nwarps) {
         const int c = (a.nclouds == 1) ? 0 : tet_find_cloud(a, tile);
@@ -140,6 +174,11 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
             V vel[3] = {ld_stream(cl->u + i), ld_stream(cl->v + i), ld_stream(cl->w + i)};
             const V d = ld_stream(cl->d + i) * ph.dscale;
             int32_t cur = ld_stream(cl->cell + i);
+#if ST_TET_PREFETCH
+            /* the first walk step reads this tet's planes: start that line towards L1 now,
+             * alongside the cell-velocity gather */
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(a.mesh.planes + 4 * (int64_t)cur));
+#endif
             const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
             const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
             const V* Uc = a.U + 3 * (int64_t)cur;
@@ -149,7 +188,7 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
             V velNew[3] = {vel[0], vel[1], vel[2]};
             int32_t tNew = cur;
             bool lost = false;
-            for (int t = 1; t <= ph.nsub; ++t) {
+            for (int t = 1; t <= nsub; ++t) {
                 if (ph.drag == 0) {
 #pragma unroll
                     for (int k = 0; k < 3; ++k) velNew[k] = (vel[k] + f * uc[k]) / ((V)1 + f);
@@ -179,12 +218,8 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
                 int status = TWALK_OK, hops = 0;
                 tNew = tet_walk(a.mesh, tNew, posNew, a.mesh.hop_limit, status, hops);
                 if (status != TWALK_OK) { lost = true; break; }
-                if (a.hop_hist && DEP != DEP_PROBE) {
-                    const int hb = hops < 7 ? hops : 7;
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) hist[k] += (hb == k);
-                }
-                if (t != ph.nsub && tNew != cur) {
+                if (count_hops) atomicAdd(&s_hist[hops < 7 ? hops : 7], 1u);
+                if (t != nsub && tNew != cur) {
                     V di[3];
 #pragma unroll
                     for (int k = 0; k < 3; ++k) di[k] = mB * (state0[k] - velNew[k]);
@@ -226,41 +261,53 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
         }
     }
     if (cur_cloud >= 0) flush_ctl<DEP>(a.ctl + cur_cloud, lane, amax, ovf, nlost);
-    if (a.hop_hist && DEP != DEP_PROBE) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const unsigned v = __reduce_add_sync(FULL_MASK, hist[k]);
-            if (lane == 0 && v) atomicAdd(a.hop_hist + k, (unsigned long long)v);
-        }
-    }
+    __syncthreads();
+    if (count_hops && threadIdx.x < 8 && s_hist[threadIdx.x])
+        atomicAdd(a.hop_hist + threadIdx.x, (unsigned long long)s_hist[threadIdx.x]);
 }
 
-template <class V>
-cudaError_t launch_step_tet(const TetStepArgs<V>& a, int dep, int grid, int block, cudaStream_t s)
+template <class V, bool ONE>
+static cudaError_t launch_step_tet_t(const TetStepArgs<V>& a, int dep, int grid, int block,
+                                     cudaStream_t s)
 {
     switch (dep) {
-    case DEP_DET1: k_step_tet<V, DEP_DET1><<<grid, block, 0, s>>>(a); break;
-    case DEP_DET2: k_step_tet<V, DEP_DET2><<<grid, block, 0, s>>>(a); break;
-    case DEP_ATOMIC: k_step_tet<V, DEP_ATOMIC><<<grid, block, 0, s>>>(a); break;
-    case DEP_PROBE: k_step_tet<V, DEP_PROBE><<<grid, block, 0, s>>>(a); break;
+    case DEP_DET1: k_step_tet<V, DEP_DET1, ONE><<<grid, block, 0, s>>>(a); break;
+    case DEP_DET2: k_step_tet<V, DEP_DET2, ONE><<<grid, block, 0, s>>>(a); break;
+    case DEP_ATOMIC: k_step_tet<V, DEP_ATOMIC, ONE><<<grid, block, 0, s>>>(a); break;
+    case DEP_PROBE: k_step_tet<V, DEP_PROBE, ONE><<<grid, block, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
 template <class V>
-int step_tet_max_active_blocks(int dep, int block)
+cudaError_t launch_step_tet(const TetStepArgs<V>& a, int dep, int grid, int block, cudaStream_t s)
+{
+    return a.phys.nsub == 1 ? launch_step_tet_t<V, true>(a, dep, grid, block, s)
+                            : launch_step_tet_t<V, false>(a, dep, grid, block, s);
+}
+
+template <class V, bool ONE>
+static int tet_max_active_t(int dep, int block)
 {
     int nb = 0;
     cudaError_t e = cudaErrorInvalidValue;
     switch (dep) {
-    case DEP_DET1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_DET1>, block, 0); break;
-    case DEP_DET2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_DET2>, block, 0); break;
-    case DEP_ATOMIC: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_ATOMIC>, block, 0); break;
-    case DEP_PROBE: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_PROBE>, block, 0); break;
+    case DEP_DET1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_DET1, ONE>, block, 0); break;
+    case DEP_DET2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_DET2, ONE>, block, 0); break;
+    case DEP_ATOMIC: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_ATOMIC, ONE>, block, 0); break;
+    case DEP_PROBE: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_step_tet<V, DEP_PROBE, ONE>, block, 0); break;
     default: break;
     }
     return e == cudaSuccess ? nb : 0;
+}
+
+template <class V>
+int step_tet_max_active_blocks(int dep, int block)
+{
+    const int x = tet_max_active_t<V, true>(dep, block);
+    const int y = tet_max_active_t<V, false>(dep, block);
+    return x < y ? x : y;
 }
 
 __global__ void k_tet_locate(const TetMeshK m, const double* __restrict__ x,

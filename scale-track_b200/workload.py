@@ -193,14 +193,14 @@ def algorithmic_bytes(precision, nparcels, ncells):
     return nparcels * bp + ncells * bc
 
 
-def tet_step_kernel_bytes(precision, nparcels, ntets, nverts):
+def tet_step_kernel_bytes(precision, nparcels, ntets):
     """Compulsory traffic of the tet step kernel: the parcel state as on cuboid meshes plus
-    the owning tet read and written (8 B), and once per step every tet's U (12 or 24 B),
-    vertex ids (16 B) and neighbours (16 B) and every vertex (24 B); with several parcels per
-    tet every tet is visited."""
+    the owning tet read and written (8 B), and once per step every tet's U (12 or 24 B), four
+    FP64 face planes (128 B) and four neighbour ids (16 B); with several parcels per tet
+    every tet is visited."""
     bp = {"mixed": 76, "fp64": 104}[precision] + 8
-    bt = {"mixed": 12, "fp64": 24}[precision] + 32
-    return nparcels * bp + ntets * bt + nverts * 24
+    bt = {"mixed": 12, "fp64": 24}[precision] + 128 + 16
+    return nparcels * bp + ntets * bt
 
 
 def step_kernel_bytes(precision, nparcels, ncells):
