@@ -246,6 +246,14 @@ ST_API void* st_allocate_array(const char* name, int size, int nComponents, int 
  * cloud 0 into the adopted "UTrans" before returning (the synchronous variant of the
  * reference's coupling, syncSerialTracking.jl:547-567). */
 ST_API int st_evolve_cloud(double dt);
+/* The reference's asynchronous coupling (A:1062-1190 with its ConstExtrapolator, A:300-316,
+ * A:742-747): call k takes U_k (the caller may overwrite it on return) and leaves in UTrans
+ * the estimate est_k = 2 S_{k-1} - est_{k-1} (est_0 = 0, carried in FP64), where S_{k-1} is
+ * the true source of the step the previous call launched; step k runs on the GPU while the
+ * caller solves the next fluid step, and its source feeds the next call's estimate.  Device
+ * errors of a step are reported by the call after it.  Do not mix with st_evolve_cloud
+ * between st_setup and st_finalize. */
+ST_API int st_evolve_cloud_async(double dt);
 /* Releases the default handle and the adopted arrays (F/juliaWrapper.C:33-50 detaches
  * the caller's fields first). */
 ST_API int st_finalize(void);

@@ -1710,6 +1710,40 @@ static std::mutex g_mu;
 static st_handle* g_default = nullptr;
 static std::map<std::string, Adopted> g_arrays;
 
+/* State of the asynchronous coupling (st_evolve_cloud_async) of the default handle. */
+struct AsyncCoupling {
+    bool ready = false;
+    bool stepped = false;          /* a step has been launched: its source feeds the estimate */
+    cudaStream_t copy = nullptr;   /* host <-> device exchange, beside the compute stream */
+    cudaEvent_t up = nullptr;      /* U of this call is on the device */
+    cudaEvent_t est = nullptr;     /* estimate of this call is ready */
+    cudaEvent_t down = nullptr;    /* estimate is in UTrans */
+    cudaEvent_t taken = nullptr;   /* the step has its own copy of U (duraw is free) */
+    double* dest = nullptr;        /* FP64 estimate, carried from call to call */
+    float* dest32 = nullptr;       /* its FP32 copy for a 4-byte UTrans */
+    void* duraw = nullptr;         /* U as the host holds it */
+    CloudCtl* hctl = nullptr;      /* pinned copy of the control blocks */
+};
+static AsyncCoupling g_async;
+
+static void async_release()
+{
+    AsyncCoupling& a = g_async;
+    /* the compute stream may still read duraw; the copy stream may still write UTrans */
+    if (g_default && g_default->stream) cudaStreamSynchronize(g_default->stream);
+    if (a.copy) cudaStreamSynchronize(a.copy);
+    if (a.taken) cudaEventDestroy(a.taken);
+    if (a.up) cudaEventDestroy(a.up);
+    if (a.est) cudaEventDestroy(a.est);
+    if (a.down) cudaEventDestroy(a.down);
+    if (a.copy) cudaStreamDestroy(a.copy);
+    if (a.dest) cudaFree(a.dest);
+    if (a.dest32) cudaFree(a.dest32);
+    if (a.duraw) cudaFree(a.duraw);
+    if (a.hctl) cudaFreeHost(a.hctl);
+    a = AsyncCoupling();
+}
+
 int st_setup(const st_params* p, const st_mesh_desc* m)
 {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -1718,6 +1752,7 @@ int st_setup(const st_params* p, const st_mesh_desc* m)
     st_handle* h = nullptr;
     int rc = st_create(p, m, dev, &h);
     if (rc) return rc;
+    async_release();
     if (g_default) st_destroy(g_default);
     g_default = h;
     return ST_OK;
@@ -1814,9 +1849,101 @@ int st_evolve_cloud(double dt)
     return check_device_errors(h);
 }
 
+/* One fluid step of the asynchronous coupling (the reference's default mode, A:1062-1190
+ * with the ConstExtrapolator of A:300-316 and A:742-747).  Call k returns once U_k has been
+ * taken and UTrans holds the estimate est_k = 2 S_{k-1} - est_{k-1} (est_0 = 0), where
+ * S_{k-1} is the true source of the step launched by call k-1; step k itself runs on the
+ * GPU while the caller solves the next fluid step.  U's upload and the estimate's download
+ * go through a second stream, so they overlap the step still running. */
+int st_evolve_cloud_async(double dt)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    st_handle* h = g_default;
+    if (!h) return fail(ST_ERR_NOT_INITIALISED, "st_evolve_cloud_async called before st_setup");
+    auto iu = g_arrays.find("U");
+    auto is = g_arrays.find("UTrans");
+    if (iu == g_arrays.end() || is == g_arrays.end())
+        return fail(ST_ERR_NOT_INITIALISED, "U and UTrans must be allocated with "
+                                            "st_allocate_array before st_evolve_cloud_async");
+    if (!(dt > 0) || !(dt < 1e300))
+        return fail(ST_ERR_INVALID_ARGUMENT, "dt must be positive and finite, got %g", dt);
+    if (h->tet) return fail(ST_ERR_INVALID_ARGUMENT, "the shims drive cuboid meshes");
+    DeviceGuard g(h->device);
+    const int64_t ncomp = h->ncells * 3;
+    const int nc = h->p.n_clouds;
+    AsyncCoupling& A = g_async;
+    int rc;
+    if (!A.ready) {
+        CK(cudaStreamCreateWithFlags(&A.copy, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&A.up, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&A.est, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&A.down, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&A.taken, cudaEventDisableTiming));
+        CK(cudaMalloc((void**)&A.dest, ncomp * sizeof(double)));
+        CK(cudaMalloc((void**)&A.dest32, ncomp * sizeof(float)));
+        CK(cudaMalloc(&A.duraw, ncomp * 8));
+        CK(cudaHostAlloc((void**)&A.hctl, sizeof(CloudCtl) * nc, cudaHostAllocPortable));
+        CK(cudaMemsetAsync(A.dest, 0, ncomp * sizeof(double), h->stream));
+        CK(cudaEventRecord(A.taken, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        A.ready = true;
+    }
+    /* duraw is free once the previous call's step has copied U out of it */
+    CK(cudaStreamWaitEvent(A.copy, A.taken, 0));
+    /* U_k in, on the copy stream (the step still running reads the handle's own U) */
+    const int ub = iu->second.tbytes;
+    CK(cudaMemcpyAsync(A.duraw, iu->second.ptr, ncomp * ub, cudaMemcpyHostToDevice, A.copy));
+    CK(cudaEventRecord(A.up, A.copy));
+    /* after step k-1: its bookkeeping, then est_k from its source */
+    CK(cudaMemcpyAsync(A.hctl, h->dctl, sizeof(CloudCtl) * nc, cudaMemcpyDeviceToHost,
+                       h->stream));
+    {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        CK(launch_extrapolate(A.stepped ? h->dsrc : nullptr, A.dest,
+                              is->second.tbytes == 4 ? A.dest32 : nullptr, ncomp, h->stream));
+        h->launches += 1;
+    }
+    CK(cudaEventRecord(A.est, h->stream));
+    CK(cudaStreamWaitEvent(A.copy, A.est, 0));
+    if (is->second.tbytes == 4)
+        CK(cudaMemcpyAsync(is->second.ptr, A.dest32, ncomp * 4, cudaMemcpyDeviceToHost, A.copy));
+    else
+        CK(cudaMemcpyAsync(is->second.ptr, A.dest, ncomp * 8, cudaMemcpyDeviceToHost, A.copy));
+    CK(cudaEventRecord(A.down, A.copy));
+    /* step k on U_k */
+    CK(cudaStreamWaitEvent(h->stream, A.up, 0));
+    if ((size_t)ub == h->vsz) {
+        CK(cudaMemcpyAsync(h->dU, A.duraw, ncomp * ub, cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        if (ub == 8)
+            CK(launch_f64_to_f32((const double*)A.duraw, (float*)h->dU, ncomp, h->stream));
+        else
+            CK(launch_f32_to_f64((const float*)A.duraw, (double*)h->dU, ncomp, h->stream));
+        h->launches += 1;
+    }
+    CK(cudaEventRecord(A.taken, h->stream));
+    if ((rc = DISPATCH(h, do_step, h, dt, 1.0))) return rc;
+    A.stepped = true;
+    /* return once U_k is taken and est_k is in UTrans; step k keeps running */
+    CK(cudaEventSynchronize(A.down));
+    unsigned long long lost = 0, ovf = 0;
+    for (int c = 0; c < nc; ++c) {
+        lost += A.hctl[c].lost;
+        ovf += A.hctl[c].overflow;
+    }
+    if (lost || ovf) {
+        /* reported once: the counters are cleared on the device, in stream order */
+        CK(cudaStreamSynchronize(h->stream));
+        return check_device_errors(h);
+    }
+    return ST_OK;
+}
+
 int st_finalize(void)
 {
     std::lock_guard<std::mutex> lk(g_mu);
+    async_release();
     if (g_default) st_destroy(g_default);
     g_default = nullptr;
     for (auto& kv : g_arrays)

@@ -189,6 +189,8 @@ cudaError_t launch_set_scale(CloudCtl* ctl, int nclouds, cudaStream_t s);
 cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s);
 cudaError_t launch_f64_to_f32(const double* in, float* out, int64_t n, cudaStream_t s);
 cudaError_t launch_f32_to_f64(const float* in, double* out, int64_t n, cudaStream_t s);
+cudaError_t launch_extrapolate(const double* s, double* est, float* est32, int64_t n,
+                               cudaStream_t st);
 
 /* Morton re-sort and order restoration (st_sort.cu). */
 template <class P, class V>

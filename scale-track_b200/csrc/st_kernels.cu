@@ -549,6 +549,30 @@ __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ 
         out[j] = (float)in[j];
 }
 
+/* Constant extrapolation of the source (A:742-747): est = 2 S - est_prev, in place on
+ * `est`, with S = 0 when there is no completed step yet (s == nullptr); the FP32 copy for a
+ * 4-byte exchange array is written alongside. */
+__global__ void k_extrapolate(const double* __restrict__ s, double* __restrict__ est,
+                             float* __restrict__ est32, int64_t n)
+{
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const double e = (s ? 2.0 * s[j] : 0.0) - est[j];
+        est[j] = e;
+        if (est32) est32[j] = (float)e;
+    }
+}
+
+cudaError_t launch_extrapolate(const double* s, double* est, float* est32, int64_t n,
+                               cudaStream_t st)
+{
+    int64_t g = (n + 255) / 256;
+    if (g > 148 * 8) g = 148 * 8;
+    if (g < 1) g = 1;
+    k_extrapolate<<<(int)g, 256, 0, st>>>(s, est, est32, n);
+    return cudaGetLastError();
+}
+
 __global__ void k_f32_to_f64(const float* __restrict__ in, double* __restrict__ out, int64_t n)
 {
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;

@@ -41,7 +41,7 @@ EXPORTS = [
     "st_allocate_array", "st_evolve_cloud", "st_finalize", "st_step_noalloc",
     "st_noalloc_max_cells", "st_mean_source_forward", "st_mean_source_pullback",
     "st_graph_capture", "st_graph_launch", "st_graph_release", "st_autotune",
-    "st_create_tet", "st_set_parcels_tet", "st_tet_hop_histogram",
+    "st_create_tet", "st_set_parcels_tet", "st_tet_hop_histogram", "st_evolve_cloud_async",
 ]
 
 
@@ -129,6 +129,7 @@ def lib():
         "st_allocate_array": ([ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int],
                               ctypes.c_void_p),
         "st_evolve_cloud": ([ctypes.c_double], ctypes.c_int),
+        "st_evolve_cloud_async": ([ctypes.c_double], ctypes.c_int),
         "st_finalize": ([], ctypes.c_int),
         "st_step_noalloc": ([P(Params), P(MeshDesc), ctypes.c_int64] + [ctypes.c_void_p] * 9 +
                             [ctypes.c_double, ctypes.c_double, ctypes.c_void_p], ctypes.c_int),
@@ -413,6 +414,12 @@ def allocate_array(name, size, n_components, type_byte_size):
 def evolve_cloud(dt):
     """evolve_cloud (A:1485-1528): one synchronous step on the default handle."""
     _check(lib().st_evolve_cloud(dt))
+
+
+def evolve_cloud_async(dt):
+    """The reference's asynchronous coupling: U is taken, UTrans receives the constant
+    extrapolation 2 S_prev - est_prev of the source, and this step runs in the background."""
+    _check(lib().st_evolve_cloud_async(dt))
 
 
 def finalize():

@@ -1,0 +1,93 @@
+"""GPU tests of the asynchronous coupling shim (st_evolve_cloud_async), the reference's default
+mode: each call returns the constant extrapolation est_k = 2 S_{k-1} - est_{k-1} (est_0 = 0)
+of the source, where S_{k-1} is the true source of the step the previous call launched, and
+that step runs with the U given to its own call.
+
+The true sources come from the synchronous shim (st_evolve_cloud) on the same inputs, which
+the parity tests tie to the oracle; the step is deterministic, so the recursion is checked
+bit for bit in FP64 and to FP32 rounding with 4-byte exchange arrays."""
+import numpy as np
+import pytest
+
+import scaletrack as st
+import workload
+
+pytestmark = pytest.mark.gpu
+
+N, NPCL, STEPS = 24, 40000, 7
+
+
+def _setup(tbytes):
+    prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                    drag_model="schiller_naumann", precision="mixed", n_substeps=1,
+                    sort_interval=3)
+    st.setup(prm, st.mesh_desc(N, 0.0, workload.L_BOX))
+    xyz, uvw, d = workload.parcels(NPCL, 21)
+    h = st.default_handle()
+    assert st.lib().st_set_parcels(h, 0, NPCL, xyz.ctypes.data, uvw.ctypes.data,
+                                   d.ctypes.data) == 0
+    U = st.allocate_array("U", N ** 3, 3, tbytes)
+    UT = st.allocate_array("UTrans", N ** 3, 3, tbytes)
+    return U, UT
+
+
+def _fields():
+    base = workload.tgv_field(N).astype(np.float64)
+    return [base * workload.fluid_scale(k, workload.DT, True) for k in range(STEPS)]
+
+
+def _true_sources(tbytes):
+    """S_k of the synchronous shim for the same U sequence."""
+    U, UT = _setup(tbytes)
+    try:
+        out = []
+        for Uk in _fields():
+            U[:] = Uk
+            st.evolve_cloud(workload.DT)
+            out.append(UT.astype(np.float64).copy())
+        return out
+    finally:
+        st.finalize()
+
+
+def _async_outputs(tbytes):
+    U, UT = _setup(tbytes)
+    try:
+        out = []
+        for Uk in _fields():
+            U[:] = Uk
+            st.evolve_cloud_async(workload.DT)
+            out.append(UT.astype(np.float64).copy())
+        return out
+    finally:
+        st.finalize()
+
+
+def test_async_coupling_is_constant_extrapolation_fp64():
+    S = _true_sources(8)
+    E = _async_outputs(8)
+    est = np.zeros_like(S[0])
+    assert np.array_equal(E[0], est)                      # est_0 = 0
+    for k in range(1, STEPS):
+        est = 2.0 * S[k - 1] - est
+        assert np.array_equal(E[k], est), k
+    assert np.abs(S[-1]).max() > 0
+
+
+def test_async_coupling_with_float_exchange_arrays():
+    S = _true_sources(8)                                  # FP64 true sources
+    E = _async_outputs(4)
+    est = np.zeros_like(S[0])
+    for k in range(1, STEPS):
+        est = 2.0 * S[k - 1] - est
+        assert np.array_equal(E[k], est.astype(np.float32).astype(np.float64)), k
+
+
+def test_async_then_finalize_and_setup_again():
+    """A step still running at st_finalize or at a new st_setup is drained first."""
+    for _ in range(2):
+        U, UT = _setup(4)
+        U[:] = workload.tgv_field(N)
+        st.evolve_cloud_async(workload.DT)
+        st.evolve_cloud_async(workload.DT)
+    st.finalize()
