@@ -104,6 +104,13 @@ ST_API int st_destroy(st_handle* h);
  * allocate!/initWithHilbert! (A:474-482, A:559-638) with caller-provided parcels. */
 ST_API int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
                    const double* d);
+/* n parcels of cloud `cloud` generated on the device, clustered along a Hilbert curve as
+ * the reference's initWithHilbert! (A:559-638): the cloud takes its own segment of a 1024^3
+ * Hilbert curve, each parcel a random point of the cell its curve point selects, velocity
+ * zero, diameter uniform in [d_min, d_max).  Counter-based random numbers: the same seed
+ * gives the same parcels on any GPU and in the CPU oracle. */
+ST_API int st_init_parcels(st_handle* h, int cloud, int64_t n, uint64_t seed, double d_min,
+                           double d_max);
 /* Current parcel state in the order given to st_set_parcels (re-sorting is undone). */
 ST_API int st_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d);
 /* 0-based owning cell of each parcel (locate, A:680-693), order as st_set_parcels. */
@@ -169,6 +176,20 @@ ST_API int st_set_parcels_tet(st_handle* h, int cloud, int64_t n, const double* 
 /* Walk lengths of every substep since the last reset: out[k] = substeps whose walk took k
  * hops (k < 7), out[7] = 7 or more.  Synchronises the stream. */
 ST_API int st_tet_hop_histogram(st_handle* h, uint64_t out[8], int reset);
+
+/* ---- output and restart -------------------------------------------------------------- */
+/* ParaView dump of one cloud (the reference's write, A:1367-1430): a VTK XML
+ * UnstructuredGrid file with one vertex per parcel, point data "U" (velocity) and "d"
+ * (diameter), FP64, appended raw binary; parcels in the order of st_set_parcels. */
+ST_API int st_write_vtu(st_handle* h, int cloud, const char* path);
+/* ParaView collection (.pvd) listing n dumps with their times (A:1414-1430). */
+ST_API int st_write_pvd(const char* path, int n, const double* times, const char* const* files);
+/* Restart file of the whole handle: every cloud's parcels (and owning tets on tet meshes),
+ * the fixed-point scale of the next step and the step bookkeeping.  Loading it into a handle
+ * created with the same parameters and mesh continues the run bit for bit (after the same
+ * fluid velocity is set).  No counterpart in the reference, which has no restart. */
+ST_API int st_save_state(st_handle* h, const char* path);
+ST_API int st_load_state(st_handle* h, const char* path);
 
 /* ---- CUDA-graph replay and autotuning ---------------------------------------------- */
 /* Captures n_steps calls of st_step (dt, fluid_scale[k] or 1) into a CUDA graph on the

@@ -19,6 +19,7 @@
 #include "step_oracle.hpp"
 #include "adjoint_oracle.hpp"
 #include "tet_oracle.hpp"
+#include "../scale-track_b200/csrc/st_init.h"
 
 using namespace st_oracle;
 
@@ -555,6 +556,34 @@ int oracle_tet_run(const oracle_cfg* cfg, int64_t nv, const double* verts, int64
         return tet_run<double>(cfg, m, np, xyz, uvw, d, cells, U, nsteps, dt, fscale, src_seq,
                                src_quant, scale_io, stats, hop_hist, hop_limit);
     return -2;
+}
+
+/* Parcels of st_init_parcels (the shared generator of st_init.h): positions rounded to
+ * the position precision (pbytes 4 or 8) and returned as doubles, [3][n]; diameters in
+ * double (the library rounds them to the velocity precision). */
+void oracle_init_parcels(int pbytes, uint64_t seed, int cloud, int nclouds, int64_t n,
+                         const int32_t N[3], const double origin[3], const double ending[3],
+                         double d_min, double d_max, double* xyz, double* d)
+{
+    for (int64_t j = 0; j < n; ++j) {
+        if (pbytes == 4) {
+            float p[3];
+            st_init_parcel<float>(seed, cloud, nclouds, (uint64_t)j, N, origin, ending, p, d[j],
+                                  d_min, d_max);
+            for (int a = 0; a < 3; ++a) xyz[a * n + j] = p[a];
+        } else {
+            double p[3];
+            st_init_parcel<double>(seed, cloud, nclouds, (uint64_t)j, N, origin, ending, p, d[j],
+                                   d_min, d_max);
+            for (int a = 0; a < 3; ++a) xyz[a * n + j] = p[a];
+        }
+    }
+}
+
+/* Hilbert curve point of each index (3 x bits bits) */
+void oracle_hilbert3(int64_t n, const uint64_t* h, int bits, uint32_t* p)
+{
+    for (int64_t i = 0; i < n; ++i) st_hilbert3(h[i], bits, p + 3 * i);
 }
 
 /* Walk from start[i] to the tet containing xyz[:, i]; status[i] as WALK_*. */

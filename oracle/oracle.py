@@ -78,6 +78,12 @@ def lib():
             ctypes.c_int64, P(ctypes.c_double), ctypes.c_int64, P(ctypes.c_int32),
             P(ctypes.c_int32), ctypes.c_int64, P(ctypes.c_double), P(ctypes.c_int32),
             P(ctypes.c_int32), P(ctypes.c_int32), ctypes.c_int]
+        L.oracle_init_parcels.argtypes = [
+            ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+            P(ctypes.c_int32), P(ctypes.c_double), P(ctypes.c_double), ctypes.c_double,
+            ctypes.c_double, P(ctypes.c_double), P(ctypes.c_double)]
+        L.oracle_hilbert3.argtypes = [ctypes.c_int64, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -236,6 +242,27 @@ def tet_run(cfg, mesh, xyz, uvw, d, cells, U, nsteps, dt, fscale=None, want_seq=
                 src_seq=None if src_seq is None else src_seq.reshape(nt, 3),
                 src_quant=None if src_q is None else src_q.reshape(nt, 3), scale=int(sc[0]),
                 lost=int(stats[0]), overflow=int(stats[1]), hop_hist=hist, status=st)
+
+
+def init_parcels(pbytes, seed, cloud, nclouds, n, N, origin, ending, d_min, d_max):
+    """Parcels of st_init_parcels: (xyz [3, n] rounded to the position precision, d [n])."""
+    N = (ctypes.c_int32 * 3)(*([N] * 3 if np.isscalar(N) else list(N)))
+    o = (ctypes.c_double * 3)(*([origin] * 3 if np.isscalar(origin) else list(origin)))
+    e = (ctypes.c_double * 3)(*([ending] * 3 if np.isscalar(ending) else list(ending)))
+    xyz = np.zeros((3, n))
+    d = np.zeros(n)
+    lib().oracle_init_parcels(pbytes, ctypes.c_uint64(seed), cloud, nclouds, n, N, o, e,
+                              ctypes.c_double(d_min), ctypes.c_double(d_max),
+                              _ptr(xyz, ctypes.c_double), _ptr(d, ctypes.c_double))
+    return xyz, d
+
+
+def hilbert3(h, bits):
+    h = np.ascontiguousarray(h, dtype=np.uint64)
+    p = np.zeros((h.size, 3), dtype=np.uint32)
+    lib().oracle_hilbert3(h.size, h.ctypes.data_as(ctypes.c_void_p), bits,
+                          p.ctypes.data_as(ctypes.c_void_p))
+    return p
 
 
 def tet_locate(mesh, xyz, start, hop_limit=1024):

@@ -529,9 +529,15 @@ int do_step_tet(st_handle* h, double dt, double fscale)
     return ST_OK;
 }
 
+/* Parcels generated on the device instead of uploaded (st_init_parcels). */
+struct InitSpec {
+    uint64_t seed;
+    double d_min, d_max;
+};
+
 template <class P, class V>
 int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
-                   const double* d, const int32_t* hint)
+                   const double* d, const int32_t* hint, const InitSpec* gen = nullptr)
 {
     CloudBufs& c = h->clouds[cloud];
     if (n > c.cap) {
@@ -562,7 +568,15 @@ int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
     }
     c.n = n;
     c.cur = 0;
-    if (n > 0) {
+    if (n > 0 && gen) {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        CK(launch_init_cloud<P, V>(gen->seed, cloud, h->p.n_clouds, n, mesh_k<P>(h), h->m.origin,
+                                   h->m.ending, gen->d_min, gen->d_max, (P*)c.x[0],
+                                   (P*)c.y[0], (P*)c.z[0], (V*)c.u[0], (V*)c.v[0], (V*)c.w[0],
+                                   (V*)c.d[0], c.id[0], h->stream));
+        h->launches += 1;
+    }
+    if (n > 0 && !gen) {
         std::vector<P> hp(n);
         std::vector<V> hv(n);
         std::vector<int32_t> hid(n);
@@ -584,6 +598,9 @@ int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
          * legacy stream, which the handle's non-blocking stream does not wait for */
         CK(cudaMemcpyAsync(c.id[0], hid.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice,
                            h->stream));
+        CK(cudaStreamSynchronize(h->stream));   /* hid is freed at the end of this block */
+    }
+    if (n > 0) {
         /* every parcel must start inside the mesh: the reference would index out of bounds */
         CK(cudaMemsetAsync(h->dcount, 0, sizeof(unsigned long long), h->stream));
         if (h->tet) {
@@ -1345,6 +1362,25 @@ int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
     return set_parcels_impl(h, cloud, n, xyz, uvw, d, nullptr);
 }
 
+int st_init_parcels(st_handle* h, int cloud, int64_t n, uint64_t seed, double d_min,
+                    double d_max)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    if (h->tet) return fail(ST_ERR_INVALID_ARGUMENT, "st_init_parcels fills cuboid meshes");
+    if (n < 0 || n > INT32_MAX)
+        return fail(ST_ERR_INVALID_ARGUMENT, "parcel count %lld out of range", (long long)n);
+    if (!(d_min > 0) || !(d_max >= d_min) || !(d_max < 1e300))
+        return fail(ST_ERR_INVALID_ARGUMENT, "diameters must satisfy 0 < d_min <= d_max");
+    DeviceGuard g(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    release_graph(h);
+    const InitSpec spec = {seed, d_min, d_max};
+    rc = DISPATCH(h, do_set_parcels, h, cloud, n, nullptr, nullptr, nullptr, nullptr, &spec);
+    if (rc) return rc;
+    return update_headroom(h);
+}
+
 int st_set_parcels_tet(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
                        const double* d, const int32_t* hint)
 {
@@ -1694,6 +1730,133 @@ int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out)
     h->p.sort_interval = best.sort_interval;
     h->steps_since_sort = 0;
     if (out) *out = best;
+    return ST_OK;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* restart files                                                                        */
+/* ------------------------------------------------------------------------------------ */
+/* Layout (little endian): "STSTATE1", int32 precision, n_clouds, tet flag, pad, int64
+ * nCells, double last dt, int64 steps, int32 steps since the last re-sort, int32 "probe
+ * pending"; per cloud int32 L, int32 H, int64 n, then double xyz[3][n], uvw[3][n], d[n] and,
+ * for tet meshes, int32 owning tet[n].  Parcel order is that of st_set_parcels.  With the
+ * fixed-point scale L carried over, a restarted run continues bit for bit. */
+static const char ST_STATE_MAGIC[8] = {'S', 'T', 'S', 'T', 'A', 'T', 'E', '1'};
+
+int st_save_state(st_handle* h, const char* path)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (!path) return fail(ST_ERR_INVALID_ARGUMENT, "null path");
+    DeviceGuard g(h->device);
+    if ((rc = st_synchronize(h))) return rc;
+    const int nc = h->p.n_clouds;
+    std::vector<CloudCtl> ctl(nc);
+    CK(cudaMemcpyAsync(ctl.data(), h->dctl, sizeof(CloudCtl) * nc, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(ST_ERR_INVALID_ARGUMENT, "cannot open %s for writing", path);
+    bool ok = fwrite(ST_STATE_MAGIC, 8, 1, f) == 1;
+    const int32_t hdr[4] = {h->p.precision, nc, h->tet ? 1 : 0, 0};
+    const int64_t nce = h->ncells;
+    const int32_t sched[2] = {h->steps_since_sort, h->need_probe ? 1 : 0};
+    ok = ok && fwrite(hdr, sizeof hdr, 1, f) == 1 && fwrite(&nce, 8, 1, f) == 1 &&
+         fwrite(&h->last_dt, 8, 1, f) == 1 && fwrite(&h->steps, 8, 1, f) == 1 &&
+         fwrite(sched, sizeof sched, 1, f) == 1;
+    for (int c = 0; c < nc && ok; ++c) {
+        const int64_t n = h->clouds[c].n;
+        const int32_t lh[2] = {ctl[c].L, ctl[c].H};
+        std::vector<double> xyz(3 * n), uvw(3 * n), d(n);
+        if (n > 0 && (rc = DISPATCH(h, do_get_parcels, h, c, xyz.data(), uvw.data(), d.data()))) {
+            fclose(f);
+            return rc;
+        }
+        ok = fwrite(lh, sizeof lh, 1, f) == 1 && fwrite(&n, 8, 1, f) == 1;
+        if (n > 0)
+            ok = ok && fwrite(xyz.data(), 8, 3 * n, f) == (size_t)(3 * n) &&
+                 fwrite(uvw.data(), 8, 3 * n, f) == (size_t)(3 * n) &&
+                 fwrite(d.data(), 8, n, f) == (size_t)n;
+        if (h->tet && n > 0) {
+            std::vector<int32_t> cells(n);
+            if ((rc = do_get_cells<double>(h, c, cells.data()))) {
+                fclose(f);
+                return rc;
+            }
+            ok = ok && fwrite(cells.data(), 4, n, f) == (size_t)n;
+        }
+    }
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) return fail(ST_ERR_INVALID_ARGUMENT, "short write to %s", path);
+    return ST_OK;
+}
+
+int st_load_state(st_handle* h, const char* path)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (!path) return fail(ST_ERR_INVALID_ARGUMENT, "null path");
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(ST_ERR_INVALID_ARGUMENT, "cannot open %s", path);
+    auto bad = [&](const char* why) {
+        fclose(f);
+        return fail(ST_ERR_INVALID_ARGUMENT, "%s: %s", path, why);
+    };
+    char magic[8];
+    int32_t hdr[4], sched[2];
+    int64_t nce, steps;
+    double last_dt;
+    if (fread(magic, 8, 1, f) != 1 || memcmp(magic, ST_STATE_MAGIC, 8) != 0)
+        return bad("not a scaletrack state file");
+    if (fread(hdr, sizeof hdr, 1, f) != 1 || fread(&nce, 8, 1, f) != 1 ||
+        fread(&last_dt, 8, 1, f) != 1 || fread(&steps, 8, 1, f) != 1 ||
+        fread(sched, sizeof sched, 1, f) != 1)
+        return bad("truncated header");
+    if (hdr[0] != h->p.precision || hdr[1] != h->p.n_clouds || hdr[2] != (h->tet ? 1 : 0) ||
+        nce != h->ncells)
+        return bad("precision, cloud count, mesh kind or cell count differ from the handle's");
+    const int nc = h->p.n_clouds;
+    std::vector<int32_t> L(nc), H(nc);
+    for (int c = 0; c < nc; ++c) {
+        int32_t lh[2];
+        int64_t n;
+        if (fread(lh, sizeof lh, 1, f) != 1 || fread(&n, 8, 1, f) != 1 || n < 0 ||
+            n > INT32_MAX)
+            return bad("truncated cloud header");
+        L[c] = lh[0];
+        H[c] = lh[1];
+        std::vector<double> xyz(3 * n), uvw(3 * n), d(n);
+        std::vector<int32_t> cells(h->tet ? n : 0);
+        if (n > 0 && (fread(xyz.data(), 8, 3 * n, f) != (size_t)(3 * n) ||
+                      fread(uvw.data(), 8, 3 * n, f) != (size_t)(3 * n) ||
+                      fread(d.data(), 8, n, f) != (size_t)n ||
+                      (h->tet && fread(cells.data(), 4, n, f) != (size_t)n)))
+            return bad("truncated parcel data");
+        if ((rc = set_parcels_impl(h, c, n, xyz.data(), uvw.data(), d.data(),
+                                   h->tet ? cells.data() : nullptr))) {
+            fclose(f);
+            return rc;
+        }
+    }
+    fclose(f);
+    /* the scale of the next step and the step bookkeeping, as saved */
+    DeviceGuard g(h->device);
+    std::vector<CloudCtl> ctl(nc);
+    CK(cudaMemcpyAsync(ctl.data(), h->dctl, sizeof(CloudCtl) * nc, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < nc; ++c) {
+        ctl[c].L = L[c];
+        ctl[c].H = H[c];
+        ctl[c].emax = EXP_NONE;
+    }
+    CK(cudaMemcpyAsync(h->dctl, ctl.data(), sizeof(CloudCtl) * nc, cudaMemcpyHostToDevice,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->last_dt = last_dt;
+    h->steps = steps;
+    h->steps_since_sort = sched[0];
+    h->need_probe = sched[1] != 0;
     return ST_OK;
 }
 

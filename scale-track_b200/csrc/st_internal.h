@@ -189,6 +189,11 @@ cudaError_t launch_set_scale(CloudCtl* ctl, int nclouds, cudaStream_t s);
 cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s);
 cudaError_t launch_f64_to_f32(const double* in, float* out, int64_t n, cudaStream_t s);
 cudaError_t launch_f32_to_f64(const float* in, double* out, int64_t n, cudaStream_t s);
+template <class P, class V>
+cudaError_t launch_init_cloud(uint64_t seed, int cloud, int nclouds, int64_t n,
+                              const MeshK<P>& m, const double origin[3], const double ending[3],
+                              double d_min, double d_max, P* x, P* y, P* z, V* u, V* v, V* w,
+                              V* d, int32_t* id, cudaStream_t s);
 cudaError_t launch_extrapolate(const double* s, double* est, float* est32, int64_t n,
                                cudaStream_t st);
 

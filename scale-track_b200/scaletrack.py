@@ -42,6 +42,7 @@ EXPORTS = [
     "st_noalloc_max_cells", "st_mean_source_forward", "st_mean_source_pullback",
     "st_graph_capture", "st_graph_launch", "st_graph_release", "st_autotune",
     "st_create_tet", "st_set_parcels_tet", "st_tet_hop_histogram", "st_evolve_cloud_async",
+    "st_init_parcels", "st_write_vtu", "st_write_pvd", "st_save_state", "st_load_state",
 ]
 
 
@@ -130,6 +131,13 @@ def lib():
                               ctypes.c_void_p),
         "st_evolve_cloud": ([ctypes.c_double], ctypes.c_int),
         "st_evolve_cloud_async": ([ctypes.c_double], ctypes.c_int),
+        "st_write_vtu": ([c_h, ctypes.c_int, ctypes.c_char_p], ctypes.c_int),
+        "st_write_pvd": ([ctypes.c_char_p, ctypes.c_int, P(ctypes.c_double),
+                          P(ctypes.c_char_p)], ctypes.c_int),
+        "st_save_state": ([c_h, ctypes.c_char_p], ctypes.c_int),
+        "st_load_state": ([c_h, ctypes.c_char_p], ctypes.c_int),
+        "st_init_parcels": ([c_h, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double,
+                             ctypes.c_double], ctypes.c_int),
         "st_finalize": ([], ctypes.c_int),
         "st_step_noalloc": ([P(Params), P(MeshDesc), ctypes.c_int64] + [ctypes.c_void_p] * 9 +
                             [ctypes.c_double, ctypes.c_double, ctypes.c_void_p], ctypes.c_int),
@@ -280,6 +288,20 @@ class ParcelTracker:
         _check(lib().st_tet_hop_histogram(self._h, _dptr(out), int(reset)))
         return out
 
+    def init_parcels(self, n, seed, d_min, d_max, cloud=0):
+        """n parcels generated on the device, clustered along a Hilbert curve per cloud."""
+        _check(lib().st_init_parcels(self._h, cloud, n, seed, d_min, d_max))
+
+    def write_vtu(self, path, cloud=0):
+        """ParaView dump of a cloud: positions, point data U (velocity) and d (diameter)."""
+        _check(lib().st_write_vtu(self._h, cloud, os.fsencode(path)))
+
+    def save_state(self, path):
+        _check(lib().st_save_state(self._h, os.fsencode(path)))
+
+    def load_state(self, path):
+        _check(lib().st_load_state(self._h, os.fsencode(path)))
+
     def num_parcels(self, cloud=0):
         return int(lib().st_num_parcels(self._h, cloud))
 
@@ -420,6 +442,14 @@ def evolve_cloud_async(dt):
     """The reference's asynchronous coupling: U is taken, UTrans receives the constant
     extrapolation 2 S_prev - est_prev of the source, and this step runs in the background."""
     _check(lib().st_evolve_cloud_async(dt))
+
+
+def write_pvd(path, times, files):
+    """ParaView collection of dumps: times[i] -> files[i]."""
+    n = len(times)
+    t = (ctypes.c_double * n)(*[float(x) for x in times])
+    fs = (ctypes.c_char_p * n)(*[os.fsencode(x) for x in files])
+    _check(lib().st_write_pvd(os.fsencode(path), n, t, fs))
 
 
 def finalize():
