@@ -420,6 +420,9 @@ def run_ours(args):
     cpu = None
     if not args.no_extras and rank == 0 and args.cpu_seconds > 0:
         cpu = cpu_rate(n, xyz, uvw, d, U, args.cpu_seconds)
+        # the reference's own CPU executor is a serial loop (A:818-823): one thread too
+        extras["cpu_baseline_1thread"] = cpu_rate(n, xyz, uvw, d, U, args.cpu_seconds / 3,
+                                                  threads=1)
 
     if pg is not None:
         pg.barrier()

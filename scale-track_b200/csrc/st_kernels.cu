@@ -1,9 +1,10 @@
 /*
  * st_kernels.cu -- the parcel step and the source reduction, written for sm_100a.
  *
- * One warp owns a tile of 128 consecutive parcels (four slices of 32); lanes read the SoA
- * arrays with consecutive addresses (streaming loads that do not displace the L2-resident
- * cell arrays), gather the cell velocity, run the substeps in registers and write back.
+ * One warp owns a tile of 32 consecutive parcels; lanes read the SoA arrays with
+ * consecutive addresses (streaming loads, issued one tile ahead, that do not displace the
+ * L2-resident cell arrays), gather the cell velocity, run the substeps in registers and
+ * write back.
  * The deposit of each parcel into its cell (A:1342-1345, A:1361) is reduced inside the warp
  * over runs of equal cells (parcels are kept Morton-sorted by cell, so neighbours mostly
  * share a cell) and only the last lane of each run touches memory.
@@ -208,14 +209,16 @@ __device__ __forceinline__ void evolve_one(const StepArgs<P, V>& a, P pos[3], V 
 #pragma unroll
     for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (P)velNew[k] * a.dtP;              /* A:1296 */
     V state0[3] = {vel[0], vel[1], vel[2]};
-    bool bad = false;
-    const int32_t I = floor_label((posNew[0] - mesh.origin[0]) * mesh.rD[0], bad);
-    const int32_t J = floor_label((posNew[1] - mesh.origin[1]) * mesh.rD[1], bad);
-    const int32_t K = floor_label((posNew[2] - mesh.origin[2]) * mesh.rD[2], bad);
-    if (bad) { lost = true; return; }
-    if (!((uint32_t)I < (uint32_t)mesh.N[0] && (uint32_t)J < (uint32_t)mesh.N[1] &&
-          (uint32_t)K < (uint32_t)mesh.N[2])) {
+    /* floor(t) lies in [0, N) exactly when t does, so the fractional cell coordinates decide
+     * whether the new position is inside without converting them */
+    const P tx = (posNew[0] - mesh.origin[0]) * mesh.rD[0];
+    const P ty = (posNew[1] - mesh.origin[1]) * mesh.rD[1];
+    const P tz = (posNew[2] - mesh.origin[2]) * mesh.rD[2];
+    if (!(tx >= (P)0 && tx < (P)mesh.N[0] && ty >= (P)0 && ty < (P)mesh.N[1] && tz >= (P)0 &&
+          tz < (P)mesh.N[2])) {
+        bool bad = false;
         LocK ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);                  /* A:1303 */
+        if (bad) { lost = true; return; }
         if (ln.posI != posI || ln.part != 1) {                                          /* A:1306 */
             const bool bx = (ln.I < 0) || (ln.I >= mesh.N[0]);
             const bool by = (ln.J < 0) || (ln.J >= mesh.N[1]);
