@@ -252,6 +252,24 @@ def test_profile_counters_and_launch_count():
 
 
 @pytest.mark.slow
+def test_configuration_0_fp64_full_run():
+    """The CPU-runnable configuration in full: 32^3 cells, 1e5 parcels, FP64, 100 steps of
+    Schiller-Naumann drag with a frozen field.  Positions, velocities and cells bit-exact with
+    the FP64 oracle after 100 steps; the two-limb source bit-exact with its fixed-point model
+    and within 1e-14 of the FP64 sum of the same deposits."""
+    c = workload.CONFIGS["c0_fp64_32"]
+    n, nparcels, steps = c["n"], c["nparcels"], c["steps"]
+    xyz, uvw, d = workload.parcels(nparcels, c["seed"], dtype_v=np.float64)
+    U = workload.tgv_field(n, U0=c["U0"], dtype=np.float64)
+    prm = bench_params("fp64")
+    fs = [1.0] * steps
+    g, r = check_against_oracle(prm, n, workload.L_BOX, xyz, uvw, d, U, workload.DT, fs,
+                                nthreads=0)
+    assert np.array_equal(g[3], r["src_quant"])
+    assert relerr(g[3], r["src_seq"]) <= TOL_SRC_2LIMB
+
+
+@pytest.mark.slow
 def test_full_size_mixed_against_oracle():
     """BASELINE configuration 1 sizes (128^3 cells, 1e7 parcels), a few steps: bit-exact
     state and cells and fixed-point source against the (multi-threaded) oracle."""
