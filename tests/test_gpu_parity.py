@@ -175,6 +175,71 @@ def test_multiple_clouds_ragged_sizes():
             assert not np.any(g[k][3])
 
 
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("drag", ["stokes_implicit", "schiller_naumann"])
+def test_parcels_on_faces_walls_and_corners(prec, drag):
+    """Edge positions against the oracle, bit for bit: parcels exactly on interior faces
+    (floor puts them in the upper cell), on the lower walls, one ulp below the upper walls,
+    in the eight corner cells, with velocities that push them across faces and into walls
+    along every axis, and one cell holding many parcels (one long run for the warp scan)."""
+    n, L = 8, 0.1
+    h = L / n
+    P = np.float32 if prec == "fp32" else np.float64
+    below = float(np.nextafter(P(L), P(0)))
+    pts, vel = [], []
+    rng = np.random.default_rng(31)
+    faces = [k * h for k in range(1, n)]
+    for k in range(200):                          # exactly on interior faces
+        p = rng.random(3) * L * 0.999
+        p[k % 3] = faces[k % len(faces)]
+        pts.append(p)
+        vel.append(rng.normal(0, 2.0, 3))
+    for axis in range(3):                         # on and next to every wall, moving out
+        for wall, v in ((0.0, -3.0), (below, 3.0)):
+            for _ in range(20):
+                p = rng.random(3) * L * 0.999
+                p[axis] = wall
+                u = rng.normal(0, 0.5, 3)
+                u[axis] = v
+                pts.append(p)
+                vel.append(u)
+    for cx in (0.01 * h, L - 0.01 * h):           # corner cells
+        for cy in (0.01 * h, L - 0.01 * h):
+            for cz in (0.01 * h, L - 0.01 * h):
+                pts.append(np.array([cx, cy, cz]))
+                vel.append(rng.normal(0, 5.0, 3))
+    for _ in range(300):                          # one crowded cell
+        pts.append(np.array([3.5 * h, 4.5 * h, 2.5 * h]) + rng.uniform(-0.4, 0.4, 3) * h)
+        vel.append(rng.normal(0, 0.3, 3))
+    xyz = np.array(pts).T.astype(P).astype(np.float64)
+    uvw = np.array(vel).T.astype(np.float32).astype(np.float64)
+    d = np.full(xyz.shape[1], 30e-6)
+    U = workload.tgv_field(n, U0=2.0, dtype=np.float64 if prec == "fp64" else np.float32)
+    prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                    drag_model=drag, precision=prec, n_substeps=3 if drag == "stokes_implicit"
+                    else 1, sort_interval=1)
+    g, r = check_against_oracle(prm, n, L, xyz, uvw, d, U, 2e-3, [1.0, 0.9, 1.1])
+    assert np.array_equal(g[3], r["src_quant"])
+    assert r["lost"] == 0
+
+
+def test_empty_and_single_parcel_clouds():
+    """Clouds of 0 and 1 parcels next to a normal one, through set-up, steps and read-back."""
+    n = 8
+    prm = bench_params("mixed", n_clouds=3, sort_interval=2)
+    xyz, uvw, d, U = bench_inputs(500, n, 13, "mixed")
+    clouds = [(np.zeros((3, 0)), np.zeros((3, 0)), np.zeros(0)),
+              (xyz[:, :1], uvw[:, :1], d[:1]),
+              (xyz, uvw, d)]
+    out = gpu_run(prm, n, workload.L_BOX, clouds, U, workload.DT, [1.0, 1.0, 1.0])
+    assert out[0][0].shape == (3, 0) and not out[0][3].any()
+    for c in (1, 2):
+        r = oracle.run(oracle_cfg(n, workload.L_BOX, prm), *clouds[c], U.astype(np.float64), 3,
+                       workload.DT)
+        assert np.array_equal(out[c][0], r["xyz"]) and np.array_equal(out[c][2], r["cells"])
+        assert np.array_equal(out[c][3], r["src_quant"])
+
+
 def test_parcel_outside_mesh_is_rejected():
     prm = st.params(precision="mixed")
     with st.ParcelTracker(prm, st.mesh_desc(4, 0.0, 1.0)) as h:
