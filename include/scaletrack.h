@@ -275,6 +275,14 @@ ST_API int st_evolve_cloud(double dt);
  * errors of a step are reported by the call after it.  Do not mix with st_evolve_cloud
  * between st_setup and st_finalize. */
 ST_API int st_evolve_cloud_async(double dt);
+/* How st_evolve_cloud moves U and UTrans.  The arrays of st_allocate_array are pinned host
+ * pages mapped into the device's address space.  ST_EXCHANGE_COPY (default): DMA copies
+ * (plus a conversion pass on the device when the element size differs from the handle's
+ * precision).  ST_EXCHANGE_MAPPED: zero copy, the library's kernels read U from and write
+ * the source to those pages directly (F/juliaWrapper.H:105-172 with device-visible storage;
+ * no counterpart in the reference, which copies, A:1081, A:1149-1152). */
+enum { ST_EXCHANGE_COPY = 0, ST_EXCHANGE_MAPPED = 1 };
+ST_API int st_set_exchange_mode(int mode);
 /* Releases the default handle and the adopted arrays (F/juliaWrapper.C:33-50 detaches
  * the caller's fields first). */
 ST_API int st_finalize(void);

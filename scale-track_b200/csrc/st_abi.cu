@@ -1865,10 +1865,12 @@ int st_load_state(st_handle* h, const char* path)
 /* ------------------------------------------------------------------------------------ */
 struct Adopted {
     void* ptr = nullptr;
+    void* dptr = nullptr;   /* the same pinned pages as the device addresses them */
     int size = 0;
     int ncomp = 0;
     int tbytes = 0;
 };
+static int g_exchange = ST_EXCHANGE_COPY;
 static std::mutex g_mu;
 static st_handle* g_default = nullptr;
 static std::map<std::string, Adopted> g_arrays;
@@ -1965,9 +1967,14 @@ void* st_allocate_array(const char* name, int size, int nComponents, int typeByt
     Adopted a;
     DeviceGuard g(g_default->device);
     cudaError_t e = cudaHostAlloc(&a.ptr, (size_t)size * nComponents * typeByteSize,
-                                  cudaHostAllocPortable);
+                                  cudaHostAllocPortable | cudaHostAllocMapped);
     if (e != cudaSuccess) {
         fail(ST_ERR_CUDA, "cudaHostAlloc: %s", cudaGetErrorString(e));
+        return nullptr;
+    }
+    if ((e = cudaHostGetDevicePointer(&a.dptr, a.ptr, 0)) != cudaSuccess) {
+        cudaFreeHost(a.ptr);
+        fail(ST_ERR_CUDA, "cudaHostGetDevicePointer: %s", cudaGetErrorString(e));
         return nullptr;
     }
     memset(a.ptr, 0, (size_t)size * nComponents * typeByteSize);
@@ -1991,6 +1998,24 @@ int st_evolve_cloud(double dt)
     DeviceGuard g(h->device);
     const int64_t ncomp = h->ncells * 3;
     int rc;
+    if (g_exchange == ST_EXCHANGE_MAPPED) {
+        /* zero-copy: kernels read U from and write the source to the pinned pages */
+        {
+            ProfScope ps(h, ST_KERNEL_OTHER);
+            CK(launch_convert(iu->second.dptr, iu->second.tbytes, h->dU, (int)h->vsz, ncomp,
+                              h->stream));
+            h->launches += 1;
+        }
+        if ((rc = DISPATCH(h, do_step, h, dt, 1.0))) return rc;
+        {
+            ProfScope ps(h, ST_KERNEL_OTHER);
+            CK(launch_convert(h->dsrc, 8, is->second.dptr, is->second.tbytes, ncomp,
+                              h->stream));
+            h->launches += 1;
+        }
+        CK(cudaStreamSynchronize(h->stream));
+        return check_device_errors(h);
+    }
     /* U host -> device (A:1079-1083) */
     if ((size_t)iu->second.tbytes == h->vsz) {
         CK(cudaMemcpyAsync(h->dU, iu->second.ptr, ncomp * h->vsz, cudaMemcpyHostToDevice,
@@ -2103,9 +2128,19 @@ int st_evolve_cloud_async(double dt)
     return ST_OK;
 }
 
+int st_set_exchange_mode(int mode)
+{
+    if (mode != ST_EXCHANGE_COPY && mode != ST_EXCHANGE_MAPPED)
+        return fail(ST_ERR_INVALID_ARGUMENT, "unknown exchange mode %d", mode);
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_exchange = mode;
+    return ST_OK;
+}
+
 int st_finalize(void)
 {
     std::lock_guard<std::mutex> lk(g_mu);
+    g_exchange = ST_EXCHANGE_COPY;
     async_release();
     if (g_default) st_destroy(g_default);
     g_default = nullptr;

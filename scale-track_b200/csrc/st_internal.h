@@ -194,6 +194,8 @@ cudaError_t launch_init_cloud(uint64_t seed, int cloud, int nclouds, int64_t n,
                               const MeshK<P>& m, const double origin[3], const double ending[3],
                               double d_min, double d_max, P* x, P* y, P* z, V* u, V* v, V* w,
                               V* d, int32_t* id, cudaStream_t s);
+cudaError_t launch_convert(const void* in, int in_bytes, void* out, int out_bytes, int64_t n,
+                           cudaStream_t s);
 cudaError_t launch_extrapolate(const double* s, double* est, float* est32, int64_t n,
                                cudaStream_t st);
 

@@ -552,6 +552,33 @@ __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ 
         out[j] = (float)in[j];
 }
 
+/* Element-wise conversion between FP32 and FP64 arrays; either side may be mapped host
+ * memory (the zero-copy exchange reads U from and writes the source to it directly). */
+template <class I, class O>
+__global__ void k_convert(const I* __restrict__ in, O* __restrict__ out, int64_t n)
+{
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x)
+        out[j] = (O)in[j];
+}
+
+cudaError_t launch_convert(const void* in, int in_bytes, void* out, int out_bytes, int64_t n,
+                           cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    int64_t g = (n + 255) / 256;
+    if (g > 148 * 16) g = 148 * 16;
+    if (in_bytes == 4 && out_bytes == 4)
+        k_convert<float, float><<<(int)g, 256, 0, s>>>((const float*)in, (float*)out, n);
+    else if (in_bytes == 4)
+        k_convert<float, double><<<(int)g, 256, 0, s>>>((const float*)in, (double*)out, n);
+    else if (out_bytes == 4)
+        k_convert<double, float><<<(int)g, 256, 0, s>>>((const double*)in, (float*)out, n);
+    else
+        k_convert<double, double><<<(int)g, 256, 0, s>>>((const double*)in, (double*)out, n);
+    return cudaGetLastError();
+}
+
 /* Constant extrapolation of the source (A:742-747): est = 2 S - est_prev, in place on
  * `est`, with S = 0 when there is no completed step yet (s == nullptr); the FP32 copy for a
  * 4-byte exchange array is written alongside. */

@@ -43,6 +43,7 @@ EXPORTS = [
     "st_graph_capture", "st_graph_launch", "st_graph_release", "st_autotune",
     "st_create_tet", "st_set_parcels_tet", "st_tet_hop_histogram", "st_evolve_cloud_async",
     "st_init_parcels", "st_write_vtu", "st_write_pvd", "st_save_state", "st_load_state",
+    "st_set_exchange_mode",
 ]
 
 
@@ -131,6 +132,7 @@ def lib():
                               ctypes.c_void_p),
         "st_evolve_cloud": ([ctypes.c_double], ctypes.c_int),
         "st_evolve_cloud_async": ([ctypes.c_double], ctypes.c_int),
+        "st_set_exchange_mode": ([ctypes.c_int], ctypes.c_int),
         "st_write_vtu": ([c_h, ctypes.c_int, ctypes.c_char_p], ctypes.c_int),
         "st_write_pvd": ([ctypes.c_char_p, ctypes.c_int, P(ctypes.c_double),
                           P(ctypes.c_char_p)], ctypes.c_int),
@@ -450,6 +452,14 @@ def write_pvd(path, times, files):
     t = (ctypes.c_double * n)(*[float(x) for x in times])
     fs = (ctypes.c_char_p * n)(*[os.fsencode(x) for x in files])
     _check(lib().st_write_pvd(os.fsencode(path), n, t, fs))
+
+
+EXCHANGE = {"copy": 0, "mapped": 1}
+
+
+def set_exchange_mode(mode):
+    """"copy" (DMA copies of U and UTrans) or "mapped" (kernels use the pinned pages)."""
+    _check(lib().st_set_exchange_mode(EXCHANGE[mode] if isinstance(mode, str) else mode))
 
 
 def finalize():

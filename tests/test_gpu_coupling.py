@@ -91,3 +91,19 @@ def test_async_then_finalize_and_setup_again():
         st.evolve_cloud_async(workload.DT)
         st.evolve_cloud_async(workload.DT)
     st.finalize()
+
+
+@pytest.mark.parametrize("tbytes", [4, 8])
+def test_mapped_exchange_equals_copies(tbytes):
+    """Zero-copy exchange (kernels use the pinned U / UTrans pages) gives the same UTrans as
+    the DMA copies, step after step."""
+    ref = _true_sources(tbytes)
+    U, UT = _setup(tbytes)
+    try:
+        st.set_exchange_mode("mapped")
+        for k, Uk in enumerate(_fields()):
+            U[:] = Uk
+            st.evolve_cloud(workload.DT)
+            assert np.array_equal(UT.astype(np.float64), ref[k]), k
+    finally:
+        st.finalize()
