@@ -240,7 +240,10 @@ def run_ours(args):
 
     extras = {}
     # ---- accuracy: mixed vs all-FP64 on the same inputs (source of the last step) ----
-    if not args.no_extras and rank == 0:
+    # single-GPU extras run on one rank only when the job has one rank: with several ranks
+    # the others would wait in a collective for minutes
+    solo = ws == 1
+    if not args.no_extras and solo:
         S = {}
         for prec, dep in (("mixed", "deterministic"), ("fp64", "deterministic")):
             with st.ParcelTracker(make_params(st, prec, dep), mesh, device=local) as h:
@@ -338,7 +341,7 @@ def run_ours(args):
     h.close()
 
     # ---- the plain FP64 GPU step (FP64 atomics), same inputs ----
-    if not args.no_extras and rank == 0 and args.fp64_steps > 0:
+    if not args.no_extras and solo and args.fp64_steps > 0:
         with st.ParcelTracker(make_params(st, "fp64", "atomic"), mesh, device=local) as h64:
             h64.set_parcels(xyz, uvw, d)
             h64.set_fluid_velocity(U.astype(np.float64))
@@ -356,7 +359,9 @@ def run_ours(args):
 
     # ---- end to end through the reference-facing shim (pinned host exchange arrays) ----
     e2e = None
-    if not args.no_extras and rank == 0 and args.e2e_steps > 0:
+    if not args.no_extras and args.e2e_steps > 0:
+        # every rank drives its own shard through its own default handle; the job's time is
+        # the slowest rank's
         st.setup(make_params(st, "mixed"), mesh)
         hd = st.default_handle()
         if st.lib().st_set_parcels(hd, 0, npcl, xyz.ctypes.data, uvw.ctypes.data,
@@ -367,18 +372,23 @@ def run_ours(args):
         Uh[:] = U
         for j in range(args.warmup):
             st.evolve_cloud(dt)
-        torch.cuda.synchronize()
+        barrier_sync()
         t0 = time.perf_counter()
         for j in range(args.e2e_steps):
             st.evolve_cloud(dt)
         el = time.perf_counter() - t0
+        if pg is not None:
+            t = torch.tensor([el], device=dev, dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            el = float(t.item())
         assert np.isfinite(UT).all()
         st.finalize()
-        e2e = {"value": npcl * args.e2e_steps / el, "unit": UNIT,
+        e2e = {"value": ws * npcl * args.e2e_steps / el, "unit": UNIT,
                "h2d_bytes_per_step": ncells * 3 * 4, "d2h_bytes_per_step": ncells * 3 * 4,
                "steps": args.e2e_steps,
                "path": "st_evolve_cloud: U (float32 [nCells][3], pinned) H2D, step, source "
                        "(float32 UTrans, pinned) D2H; fixed fluid scale"}
+    if not args.no_extras and args.e2e_steps > 0 and solo:
         # zero-copy exchange: the library's kernels read U from and write UTrans to the
         # pinned pages directly
         st.setup(make_params(st, "mixed"), mesh)
@@ -430,20 +440,20 @@ def run_ours(args):
                     "extrapolated source D2H on a copy stream, overlapping the previous step"}
 
     # ---- 64 clouds in one launch, graph replay, autotuned ----
-    if not args.no_extras and rank == 0 and args.clouds:
+    if not args.no_extras and solo and args.clouds:
         extras["clouds"] = run_clouds(st, torch, local, dev)
 
     # ---- face walk on the jittered tet mesh ----
-    if not args.no_extras and rank == 0 and args.tets:
+    if not args.no_extras and solo and args.tets:
         extras["tets"] = run_tets(st, torch, local, dev, args.tet_steps, args.tet_nparcels)
 
     # ---- adjoint of the time-averaged source ----
-    if not args.no_extras and rank == 0 and args.adjoint:
+    if not args.no_extras and solo and args.adjoint:
         extras["adjoint"] = run_adjoint(st, local)
 
     # ---- CPU baseline: the oracle on this host's cores (bounded sample) ----
     cpu = None
-    if not args.no_extras and rank == 0 and args.cpu_seconds > 0:
+    if not args.no_extras and solo and args.cpu_seconds > 0:
         cpu = cpu_rate(n, xyz, uvw, d, U, args.cpu_seconds)
         # the reference's own CPU executor is a serial loop (A:818-823): one thread too
         extras["cpu_baseline_1thread"] = cpu_rate(n, xyz, uvw, d, U, args.cpu_seconds / 3,
