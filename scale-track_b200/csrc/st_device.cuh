@@ -18,8 +18,6 @@ namespace st {
 #define FULL_MASK 0xffffffffu
 #endif
 
-__device__ __forceinline__ float st_floor(float v) { return floorf(v); }
-__device__ __forceinline__ double st_floor(double v) { return floor(v); }
 __device__ __forceinline__ float st_sqrt(float v) { return __fsqrt_rn(v); }
 __device__ __forceinline__ double st_sqrt(double v) { return __dsqrt_rn(v); }
 

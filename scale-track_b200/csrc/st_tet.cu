@@ -123,9 +123,6 @@ __device__ __forceinline__ int tet_find_cloud(const TetStepArgs<V>& a, int64_t t
     return lo;
 }
 
-#ifndef ST_TET_PREFETCH
-#define ST_TET_PREFETCH 1
-#endif
 /* Resident blocks of 256 threads per SM the compiler must allow: 4 (64 registers). */
 #ifndef ST_TET_MIN_BLOCKS
 #define ST_TET_MIN_BLOCKS 4
@@ -174,11 +171,9 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
             V vel[3] = {ld_stream(cl->u + i), ld_stream(cl->v + i), ld_stream(cl->w + i)};
             const V d = ld_stream(cl->d + i) * ph.dscale;
             int32_t cur = ld_stream(cl->cell + i);
-#if ST_TET_PREFETCH
             /* the first walk step reads this tet's planes: start that line towards L1 now,
              * alongside the cell-velocity gather */
             asm volatile("prefetch.global.L1 [%0];" ::"l"(a.mesh.planes + 4 * (int64_t)cur));
-#endif
             const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
             const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
             const V* Uc = a.U + 3 * (int64_t)cur;
