@@ -111,6 +111,11 @@ ST_API int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz,
  * gives the same parcels on any GPU and in the CPU oracle. */
 ST_API int st_init_parcels(st_handle* h, int cloud, int64_t n, uint64_t seed, double d_min,
                            double d_max);
+/* Injection: m more parcels (same SoA layout as st_set_parcels) appended to a cloud of a
+ * cuboid mesh, in place on the device; they take the order positions n .. n+m-1.  The next
+ * step re-derives the fixed-point scale.  The reference injects only at start-up. */
+ST_API int st_append_parcels(st_handle* h, int cloud, int64_t m, const double* xyz,
+                             const double* uvw, const double* d);
 /* Current parcel state in the order given to st_set_parcels (re-sorting is undone). */
 ST_API int st_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d);
 /* 0-based owning cell of each parcel (locate, A:680-693), order as st_set_parcels. */

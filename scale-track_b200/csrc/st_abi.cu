@@ -647,6 +647,92 @@ int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
     return ST_OK;
 }
 
+/* Appends m parcels to a cloud in place (injection): the buffers grow by at least half when
+ * full (the current parcels are copied on the device), the new parcels go to the end of the
+ * current buffers with ids n .. n+m-1, and the next step re-derives the fixed-point scale. */
+template <class P, class V>
+int do_append_parcels(st_handle* h, int cloud, int64_t m, const double* xyz, const double* uvw,
+                      const double* d)
+{
+    CloudBufs& c = h->clouds[cloud];
+    const int64_t n = c.n, nn = n + m;
+    if (nn > c.cap) {
+        int64_t cap = c.cap + c.cap / 2;
+        if (cap < nn) cap = nn;
+        void** arrs[] = {&c.x[0], &c.y[0], &c.z[0], &c.u[0], &c.v[0], &c.w[0], &c.d[0]};
+        void** arrs1[] = {&c.x[1], &c.y[1], &c.z[1], &c.u[1], &c.v[1], &c.w[1], &c.d[1]};
+        for (int a = 0; a < 8; ++a) {
+            const size_t es = a < 3 ? sizeof(P) : (a < 7 ? sizeof(V) : sizeof(int32_t));
+            void** b0 = a < 7 ? arrs[a] : (void**)&c.id[0];
+            void** b1 = a < 7 ? arrs1[a] : (void**)&c.id[1];
+            void* keep = c.cur == 0 ? *b0 : *b1;
+            void* fresh0 = nullptr;
+            void* fresh1 = nullptr;
+            CK(cudaMalloc(&fresh0, (size_t)cap * es));
+            CK(cudaMalloc(&fresh1, (size_t)cap * es));
+            if (n > 0)
+                CK(cudaMemcpyAsync(fresh0, keep, (size_t)n * es, cudaMemcpyDeviceToDevice,
+                                   h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            if (*b0) cudaFree(*b0);
+            if (*b1) cudaFree(*b1);
+            *b0 = fresh0;
+            *b1 = fresh1;
+        }
+        for (int k = 0; k < 2; ++k) {
+            if (c.keys[k]) cudaFree(c.keys[k]);
+            if (c.perm[k]) cudaFree(c.perm[k]);
+            c.keys[k] = c.perm[k] = nullptr;
+            CK(cudaMalloc(&c.keys[k], (size_t)cap * sizeof(uint32_t)));
+            CK(cudaMalloc(&c.perm[k], (size_t)cap * sizeof(uint32_t)));
+        }
+        if (c.temp) cudaFree(c.temp);
+        c.temp = nullptr;
+        c.temp_bytes = sort_temp_bytes<P, V>(cap);
+        CK(cudaMalloc(&c.temp, c.temp_bytes > 0 ? c.temp_bytes : 16));
+        c.cap = cap;
+        c.cur = 0;
+    }
+    const int k = c.cur;
+    std::vector<P> hp(m);
+    std::vector<V> hv(m);
+    std::vector<int32_t> hid(m);
+    P* dstp[3] = {(P*)c.x[k] + n, (P*)c.y[k] + n, (P*)c.z[k] + n};
+    for (int a = 0; a < 3; ++a) {
+        for (int64_t i = 0; i < m; ++i) hp[i] = (P)xyz[a * m + i];
+        CK(cudaMemcpyAsync(dstp[a], hp.data(), m * sizeof(P), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    V* dstv[4] = {(V*)c.u[k] + n, (V*)c.v[k] + n, (V*)c.w[k] + n, (V*)c.d[k] + n};
+    for (int a = 0; a < 4; ++a) {
+        const double* srcp = a < 3 ? uvw + a * m : d;
+        for (int64_t i = 0; i < m; ++i) hv[i] = (V)srcp[i];
+        CK(cudaMemcpyAsync(dstv[a], hv.data(), m * sizeof(V), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    for (int64_t i = 0; i < m; ++i) hid[i] = (int32_t)(n + i);
+    CK(cudaMemcpyAsync(c.id[k] + n, hid.data(), m * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       h->stream));
+    /* the new parcels must lie inside the mesh */
+    CK(cudaMemsetAsync(h->dcount, 0, sizeof(unsigned long long), h->stream));
+    {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        CK(cells_cloud<P>(dstp[0], dstp[1], dstp[2], nullptr, m, mesh_k<P>(h),
+                          (int32_t*)c.keys[0], h->dcount, h->stream));
+        h->launches += 1;
+    }
+    unsigned long long outside = 0;
+    CK(cudaMemcpyAsync(&outside, h->dcount, sizeof outside, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (outside)
+        return fail(ST_ERR_PARCEL_OUTSIDE, "%llu of %lld appended parcels lie outside the mesh",
+                    outside, (long long)m);
+    c.n = nn;
+    h->clouds_dirty = true;
+    h->need_probe = true;
+    return ST_OK;
+}
+
 template <class P, class V>
 int do_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d)
 {
@@ -1360,6 +1446,24 @@ int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
                    const double* d)
 {
     return set_parcels_impl(h, cloud, n, xyz, uvw, d, nullptr);
+}
+
+int st_append_parcels(st_handle* h, int cloud, int64_t m, const double* xyz, const double* uvw,
+                      const double* d)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    if (h->tet) return fail(ST_ERR_INVALID_ARGUMENT, "st_append_parcels fills cuboid meshes");
+    if (m < 0 || h->clouds[cloud].n + m > INT32_MAX)
+        return fail(ST_ERR_INVALID_ARGUMENT, "parcel count out of range");
+    if (m == 0) return ST_OK;
+    if (!xyz || !uvw || !d) return fail(ST_ERR_INVALID_ARGUMENT, "null parcel array");
+    DeviceGuard g(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    release_graph(h);
+    rc = DISPATCH(h, do_append_parcels, h, cloud, m, xyz, uvw, d);
+    if (rc) return rc;
+    return update_headroom(h);
 }
 
 int st_init_parcels(st_handle* h, int cloud, int64_t n, uint64_t seed, double d_min,

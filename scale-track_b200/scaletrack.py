@@ -43,7 +43,7 @@ EXPORTS = [
     "st_graph_capture", "st_graph_launch", "st_graph_release", "st_autotune",
     "st_create_tet", "st_set_parcels_tet", "st_tet_hop_histogram", "st_evolve_cloud_async",
     "st_init_parcels", "st_write_vtu", "st_write_pvd", "st_save_state", "st_load_state",
-    "st_set_exchange_mode",
+    "st_set_exchange_mode", "st_append_parcels",
 ]
 
 
@@ -133,6 +133,8 @@ def lib():
         "st_evolve_cloud": ([ctypes.c_double], ctypes.c_int),
         "st_evolve_cloud_async": ([ctypes.c_double], ctypes.c_int),
         "st_set_exchange_mode": ([ctypes.c_int], ctypes.c_int),
+        "st_append_parcels": ([c_h, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p,
+                               ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
         "st_write_vtu": ([c_h, ctypes.c_int, ctypes.c_char_p], ctypes.c_int),
         "st_write_pvd": ([ctypes.c_char_p, ctypes.c_int, P(ctypes.c_double),
                           P(ctypes.c_char_p)], ctypes.c_int),
@@ -289,6 +291,15 @@ class ParcelTracker:
         out = np.zeros(8, dtype=np.uint64)
         _check(lib().st_tet_hop_histogram(self._h, _dptr(out), int(reset)))
         return out
+
+    def append_parcels(self, xyz, uvw, d, cloud=0):
+        """Injection: parcels added to the end of a cloud, in place on the device."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        uvw = np.ascontiguousarray(uvw, dtype=np.float64)
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        m = d.shape[0]
+        assert xyz.shape == (3, m) and uvw.shape == (3, m)
+        _check(lib().st_append_parcels(self._h, cloud, m, _dptr(xyz), _dptr(uvw), _dptr(d)))
 
     def init_parcels(self, n, seed, d_min, d_max, cloud=0):
         """n parcels generated on the device, clustered along a Hilbert curve per cloud."""

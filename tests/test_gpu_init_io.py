@@ -158,3 +158,40 @@ def test_load_state_rejects_other_handles(tmp_path):
     with st.ParcelTracker(prm, st.mesh_desc(8, 0.0, L)) as h3:
         with pytest.raises(st.ScaleTrackError):
             h3.load_state(str(tmp_path / "junk.bin"))
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_append_parcels_continues_like_the_oracle(prec):
+    """Injection: parcels appended after two steps (the buffers grow on the device) step on
+    with the others exactly as the oracle steps the combined set."""
+    N, n, m = 12, 3000, 2500
+    xyz, uvw, d = workload.parcels(n + m, 19)
+    vt = np.float64 if prec == "fp64" else np.float32
+    U = workload.tgv_field(N, dtype=vt)
+    prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                    drag_model="schiller_naumann", precision=prec, n_substeps=1,
+                    sort_interval=2)
+    with st.ParcelTracker(prm, st.mesh_desc(N, 0.0, L)) as h:
+        h.set_parcels(xyz[:, :n], uvw[:, :n], d[:n])
+        h.set_fluid_velocity(U)
+        h.step(workload.DT)
+        h.step(workload.DT)
+        h.append_parcels(xyz[:, n:], uvw[:, n:], d[n:])
+        assert h.num_parcels() == n + m
+        h.step(workload.DT)
+        h.step(workload.DT)
+        h.synchronize()
+        gx, gv, _ = h.get_parcels()
+        gc = h.get_cells()
+        gs = h.get_source(0)
+    cfg = oracle.make_cfg(N, 0.0, L, workload.MU_F, workload.RHO_F, workload.RHO_P,
+                          drag="sn_explicit", precision=prec, n_substeps=1,
+                          quant_limbs=2 if prec == "fp64" else 1)
+    U64 = U.astype(np.float64)
+    r1 = oracle.run(cfg, xyz[:, :n], uvw[:, :n], d[:n], U64, 2, workload.DT)
+    x2 = np.concatenate([r1["xyz"], xyz[:, n:]], axis=1)
+    v2 = np.concatenate([r1["uvw"], uvw[:, n:].astype(vt).astype(np.float64)], axis=1)
+    r2 = oracle.run(cfg, x2, v2, d, U64, 2, workload.DT)
+    assert np.array_equal(gx, r2["xyz"]) and np.array_equal(gv, r2["uvw"])
+    assert np.array_equal(gc, r2["cells"])
+    assert np.array_equal(gs, r2["src_quant"])
