@@ -1983,7 +1983,8 @@ static std::map<std::string, Adopted> g_arrays;
 struct AsyncCoupling {
     bool ready = false;
     bool stepped = false;          /* a step has been launched: its source feeds the estimate */
-    cudaStream_t copy = nullptr;   /* host <-> device exchange, beside the compute stream */
+    cudaStream_t copy = nullptr;   /* U in, beside the compute stream */
+    cudaStream_t back = nullptr;   /* estimate out, concurrent with the upload (full duplex) */
     cudaEvent_t up = nullptr;      /* U of this call is on the device */
     cudaEvent_t est = nullptr;     /* estimate of this call is ready */
     cudaEvent_t down = nullptr;    /* estimate is in UTrans */
@@ -2001,11 +2002,13 @@ static void async_release()
     /* the compute stream may still read duraw; the copy stream may still write UTrans */
     if (g_default && g_default->stream) cudaStreamSynchronize(g_default->stream);
     if (a.copy) cudaStreamSynchronize(a.copy);
+    if (a.back) cudaStreamSynchronize(a.back);
     if (a.taken) cudaEventDestroy(a.taken);
     if (a.up) cudaEventDestroy(a.up);
     if (a.est) cudaEventDestroy(a.est);
     if (a.down) cudaEventDestroy(a.down);
     if (a.copy) cudaStreamDestroy(a.copy);
+    if (a.back) cudaStreamDestroy(a.back);
     if (a.dest) cudaFree(a.dest);
     if (a.dest32) cudaFree(a.dest32);
     if (a.duraw) cudaFree(a.duraw);
@@ -2146,7 +2149,7 @@ int st_evolve_cloud(double dt)
  * taken and UTrans holds the estimate est_k = 2 S_{k-1} - est_{k-1} (est_0 = 0), where
  * S_{k-1} is the true source of the step launched by call k-1; step k itself runs on the
  * GPU while the caller solves the next fluid step.  U's upload and the estimate's download
- * go through a second stream, so they overlap the step still running. */
+ * go through two more streams, so they overlap the step still running and each other. */
 int st_evolve_cloud_async(double dt)
 {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -2167,6 +2170,7 @@ int st_evolve_cloud_async(double dt)
     int rc;
     if (!A.ready) {
         CK(cudaStreamCreateWithFlags(&A.copy, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&A.back, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&A.up, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&A.est, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&A.down, cudaEventDisableTiming));
@@ -2196,12 +2200,12 @@ int st_evolve_cloud_async(double dt)
         h->launches += 1;
     }
     CK(cudaEventRecord(A.est, h->stream));
-    CK(cudaStreamWaitEvent(A.copy, A.est, 0));
+    CK(cudaStreamWaitEvent(A.back, A.est, 0));
     if (is->second.tbytes == 4)
-        CK(cudaMemcpyAsync(is->second.ptr, A.dest32, ncomp * 4, cudaMemcpyDeviceToHost, A.copy));
+        CK(cudaMemcpyAsync(is->second.ptr, A.dest32, ncomp * 4, cudaMemcpyDeviceToHost, A.back));
     else
-        CK(cudaMemcpyAsync(is->second.ptr, A.dest, ncomp * 8, cudaMemcpyDeviceToHost, A.copy));
-    CK(cudaEventRecord(A.down, A.copy));
+        CK(cudaMemcpyAsync(is->second.ptr, A.dest, ncomp * 8, cudaMemcpyDeviceToHost, A.back));
+    CK(cudaEventRecord(A.down, A.back));
     /* step k on U_k */
     CK(cudaStreamWaitEvent(h->stream, A.up, 0));
     if ((size_t)ub == h->vsz) {
@@ -2218,6 +2222,7 @@ int st_evolve_cloud_async(double dt)
     if ((rc = DISPATCH(h, do_step, h, dt, 1.0))) return rc;
     A.stepped = true;
     /* return once U_k is taken and est_k is in UTrans; step k keeps running */
+    CK(cudaEventSynchronize(A.up));
     CK(cudaEventSynchronize(A.down));
     unsigned long long lost = 0, ovf = 0;
     for (int c = 0; c < nc; ++c) {
