@@ -541,6 +541,10 @@ int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
 {
     CloudBufs& c = h->clouds[cloud];
     if (n > c.cap) {
+        /* a failed allocation below leaves an empty cloud that the next call reallocates */
+        c.cap = 0;
+        c.n = 0;
+        h->clouds_dirty = true;
         for (int k = 0; k < 2; ++k) {
             void** arrs[] = {&c.x[k], &c.y[k], &c.z[k], &c.u[k], &c.v[k], &c.w[k], &c.d[k]};
             for (int a = 0; a < 7; ++a) {
@@ -659,39 +663,58 @@ int do_append_parcels(st_handle* h, int cloud, int64_t m, const double* xyz, con
     if (nn > c.cap) {
         int64_t cap = c.cap + c.cap / 2;
         if (cap < nn) cap = nn;
-        void** arrs[] = {&c.x[0], &c.y[0], &c.z[0], &c.u[0], &c.v[0], &c.w[0], &c.d[0]};
-        void** arrs1[] = {&c.x[1], &c.y[1], &c.z[1], &c.u[1], &c.v[1], &c.w[1], &c.d[1]};
-        for (int a = 0; a < 8; ++a) {
-            const size_t es = a < 3 ? sizeof(P) : (a < 7 ? sizeof(V) : sizeof(int32_t));
-            void** b0 = a < 7 ? arrs[a] : (void**)&c.id[0];
-            void** b1 = a < 7 ? arrs1[a] : (void**)&c.id[1];
-            void* keep = c.cur == 0 ? *b0 : *b1;
-            void* fresh0 = nullptr;
-            void* fresh1 = nullptr;
-            CK(cudaMalloc(&fresh0, (size_t)cap * es));
-            CK(cudaMalloc(&fresh1, (size_t)cap * es));
-            if (n > 0)
-                CK(cudaMemcpyAsync(fresh0, keep, (size_t)n * es, cudaMemcpyDeviceToDevice,
-                                   h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-            if (*b0) cudaFree(*b0);
-            if (*b1) cudaFree(*b1);
-            *b0 = fresh0;
-            *b1 = fresh1;
+        /* every new buffer is allocated before anything is replaced, so a failure leaves the
+         * cloud as it was */
+        void** arrs[2][8] = {{&c.x[0], &c.y[0], &c.z[0], &c.u[0], &c.v[0], &c.w[0], &c.d[0],
+                              (void**)&c.id[0]},
+                             {&c.x[1], &c.y[1], &c.z[1], &c.u[1], &c.v[1], &c.w[1], &c.d[1],
+                              (void**)&c.id[1]}};
+        size_t es[8];
+        for (int a = 0; a < 8; ++a)
+            es[a] = a < 3 ? sizeof(P) : (a < 7 ? sizeof(V) : sizeof(int32_t));
+        std::vector<void*> fresh;
+        auto grab = [&](size_t bytes) -> void* {
+            void* p = nullptr;
+            if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+            fresh.push_back(p);
+            return p;
+        };
+        void* nb[2][8];
+        void* nkeys[2];
+        void* nperm[2];
+        bool ok = true;
+        for (int k = 0; k < 2 && ok; ++k) {
+            for (int a = 0; a < 8 && ok; ++a) ok = (nb[k][a] = grab((size_t)cap * es[a])) != nullptr;
+            ok = ok && (nkeys[k] = grab((size_t)cap * sizeof(uint32_t))) != nullptr;
+            ok = ok && (nperm[k] = grab((size_t)cap * sizeof(uint32_t))) != nullptr;
         }
+        const size_t tb = sort_temp_bytes<P, V>(cap);
+        void* ntemp = ok ? grab(tb > 0 ? tb : 16) : nullptr;
+        if (!ok || !ntemp) {
+            for (void* p : fresh) cudaFree(p);
+            cudaGetLastError();
+            return fail(ST_ERR_OUT_OF_MEMORY, "no device memory for %lld parcels", (long long)cap);
+        }
+        for (int a = 0; a < 8 && n > 0; ++a)
+            CK(cudaMemcpyAsync(nb[0][a], *arrs[c.cur][a], (size_t)n * es[a],
+                               cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
         for (int k = 0; k < 2; ++k) {
+            for (int a = 0; a < 8; ++a) {
+                if (*arrs[k][a]) cudaFree(*arrs[k][a]);
+                *arrs[k][a] = nb[k][a];
+            }
             if (c.keys[k]) cudaFree(c.keys[k]);
             if (c.perm[k]) cudaFree(c.perm[k]);
-            c.keys[k] = c.perm[k] = nullptr;
-            CK(cudaMalloc(&c.keys[k], (size_t)cap * sizeof(uint32_t)));
-            CK(cudaMalloc(&c.perm[k], (size_t)cap * sizeof(uint32_t)));
+            c.keys[k] = (uint32_t*)nkeys[k];
+            c.perm[k] = (uint32_t*)nperm[k];
         }
         if (c.temp) cudaFree(c.temp);
-        c.temp = nullptr;
-        c.temp_bytes = sort_temp_bytes<P, V>(cap);
-        CK(cudaMalloc(&c.temp, c.temp_bytes > 0 ? c.temp_bytes : 16));
+        c.temp = ntemp;
+        c.temp_bytes = tb;
         c.cap = cap;
         c.cur = 0;
+        h->clouds_dirty = true;
     }
     const int k = c.cur;
     std::vector<P> hp(m);
