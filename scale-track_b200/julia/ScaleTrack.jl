@@ -163,4 +163,43 @@ end
 
 evolve_cloud(dt::Real) = check(ccall((:st_evolve_cloud, libscaletrack), Cint, (Cdouble,), dt))
 
+# the reference's default, asynchronous coupling: UTrans receives the extrapolated source
+evolve_cloud_async(dt::Real) =
+    check(ccall((:st_evolve_cloud_async, libscaletrack), Cint, (Cdouble,), dt))
+
+# zero-copy exchange: 0 = copies, 1 = the kernels use the pinned U / UTrans pages in place
+set_exchange_mode(mode::Integer) =
+    check(ccall((:st_set_exchange_mode, libscaletrack), Cint, (Cint,), mode))
+
+# ---- initialisation, injection, output, restart ----------------------------------------
+init_parcels!(t::Tracker, n::Integer, seed::Integer, dmin::Real, dmax::Real;
+              cloud::Integer = 0) =
+    check(ccall((:st_init_parcels, libscaletrack), Cint,
+                (Ptr{Cvoid}, Cint, Int64, UInt64, Cdouble, Cdouble),
+                t.h, cloud, n, seed, dmin, dmax))
+
+function append_parcels!(t::Tracker, xyz::Matrix{Float64}, uvw::Matrix{Float64},
+                         d::Vector{Float64}; cloud::Integer = 0)
+    n = length(d)
+    @assert size(xyz) == (n, 3) && size(uvw) == (n, 3)   # column-major: x block, y, z
+    check(ccall((:st_append_parcels, libscaletrack), Cint,
+                (Ptr{Cvoid}, Cint, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                t.h, cloud, n, xyz, uvw, d))
+end
+
+write_vtu(t::Tracker, path::String; cloud::Integer = 0) =
+    check(ccall((:st_write_vtu, libscaletrack), Cint, (Ptr{Cvoid}, Cint, Cstring),
+                t.h, cloud, path))
+
+function write_pvd(path::String, times::Vector{Float64}, files::Vector{String})
+    check(ccall((:st_write_pvd, libscaletrack), Cint,
+                (Cstring, Cint, Ptr{Float64}, Ptr{Cstring}),
+                path, length(times), times, files))
+end
+
+save_state(t::Tracker, path::String) =
+    check(ccall((:st_save_state, libscaletrack), Cint, (Ptr{Cvoid}, Cstring), t.h, path))
+load_state!(t::Tracker, path::String) =
+    check(ccall((:st_load_state, libscaletrack), Cint, (Ptr{Cvoid}, Cstring), t.h, path))
+
 end # module

@@ -90,3 +90,20 @@ def test_null_handle_is_rejected():
     assert L.st_synchronize(None) == st.ST_ERR_INVALID_ARGUMENT
     assert L.st_num_parcels(None, 0) == -1
     assert L.st_launch_count(None) == -1
+
+
+def test_pvd_collection_written_on_the_host(tmp_path):
+    """st_write_pvd is host-only: the collection lists every dump with its time."""
+    import xml.etree.ElementTree as ET
+    path = str(tmp_path / "c.pvd")
+    st.write_pvd(path, [0.0, 2.5e-4, 5e-4], ["a.vtu", "b.vtu", "c.vtu"])
+    ds = ET.parse(path).getroot().findall("Collection/DataSet")
+    assert [d.get("file") for d in ds] == ["a.vtu", "b.vtu", "c.vtu"]
+    assert [float(d.get("timestep")) for d in ds] == [0.0, 2.5e-4, 5e-4]
+    assert st.lib().st_write_pvd(None, 0, None, None) == st.ST_ERR_INVALID_ARGUMENT
+
+
+def test_exchange_mode_is_validated():
+    assert st.lib().st_set_exchange_mode(7) == st.ST_ERR_INVALID_ARGUMENT
+    assert "exchange mode" in st.last_error()
+    st.set_exchange_mode("copy")
