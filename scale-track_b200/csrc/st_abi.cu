@@ -1,11 +1,13 @@
 /*
  * st_abi.cu -- the C ABI of libscaletrack.so (declared in include/scaletrack.h).
  *
- * Host side of the parcel step: handle and device memory management, the per-step launch
- * sequence (probe -> step -> finalize, periodic Morton re-sort), device error reporting and
- * the two shims with the reference's coupling surface (allocate_array_ptr and
- * evolve_cloud, A:1436-1528).  There is no CPU fallback: without a CUDA device every entry
- * point that needs one fails with ST_ERR_CUDA.
+ * Host side of the parcel step: handle and device memory management (cuboid and tet
+ * meshes), the per-step launch sequence (probe -> step -> finalize, periodic re-sort), device
+ * error reporting, CUDA-graph capture and the autotuner, the adjoint driver, device-side
+ * initialisation and injection, restart files, and the shims with the reference's coupling
+ * surface (allocate_array_ptr and evolve_cloud, A:1436-1528, in its synchronous and
+ * asynchronous forms, with copied or mapped exchange arrays).  There is no CPU fallback:
+ * without a CUDA device every entry point that needs one fails with ST_ERR_CUDA.
  *
  * Per-step launch sequence on the handle's stream (all clouds in each launch):
  *   [probe + set_scale]   only on the first step after st_set_parcels or a new dt
