@@ -14,7 +14,10 @@ parcel (including the source finalize and, every 20th step, the re-sort).
              host exchange arrays: U copied in and the source copied out every step
   roofline   the step kernel's algorithmic bytes / its event-timed duration vs measured HBM
   cpu_baseline  the CPU oracle (restatement of the reference's CPU path) on this host
-  fp64_*     the plain all-FP64 GPU step (FP64 atomics) on the same inputs
+  fp64_*     the all-FP64 GPU step (same kernel design, FP64 atomics, re-sorted) on the
+             same inputs
+  fp64_plain_*  the reference's plain method in FP64 on the GPU: parcels in their given
+             order, never re-sorted, three FP64 atomics per parcel
 --impl reference times the CPU restatement of the reference's path with all host threads.
 Multi-GPU (torchrun): every rank steps its own 1e7 parcels (weak scaling) against the
 replicated U, and the per-cell source is summed over ranks with an NCCL all-reduce.
@@ -340,9 +343,12 @@ def run_ours(args):
     extras["whole_step_hbm_frac"] = round(whole_step_frac, 4)
     h.close()
 
-    # ---- the plain FP64 GPU step (FP64 atomics), same inputs ----
-    if not args.no_extras and solo and args.fp64_steps > 0:
-        with st.ParcelTracker(make_params(st, "fp64", "atomic"), mesh, device=local) as h64:
+    # ---- all-FP64 GPU steps on the same inputs: the same kernel design with FP64 atomics
+    # (re-sorted like the mixed step), and the reference's plain method in FP64 (one pass
+    # over the parcels in their given order, three FP64 atomics per parcel, no re-sort) ----
+    def time_fp64(sort_interval):
+        with st.ParcelTracker(make_params(st, "fp64", "atomic", sort_interval), mesh,
+                              device=local) as h64:
             h64.set_parcels(xyz, uvw, d)
             h64.set_fluid_velocity(U.astype(np.float64))
             t64 = DeviceTimer(torch, h64.stream(), dev)
@@ -352,10 +358,17 @@ def run_ours(args):
             t64.start()
             for j in range(args.fp64_steps):
                 h64.step(dt, fs(args.warmup + j))
-            ms64 = t64.stop()
+            return t64.stop()
+
+    if not args.no_extras and solo and args.fp64_steps > 0:
+        ms64 = time_fp64(None)
         extras["fp64_value"] = npcl * args.fp64_steps / (ms64 / 1e3)
         extras["fp64_ms_per_step"] = ms64 / args.fp64_steps
         extras["mixed_over_fp64"] = round(value / ws / extras["fp64_value"], 3)
+        ms64p = time_fp64(0)
+        extras["fp64_plain_value"] = npcl * args.fp64_steps / (ms64p / 1e3)
+        extras["fp64_plain_ms_per_step"] = ms64p / args.fp64_steps
+        extras["mixed_over_fp64_plain"] = round(value / ws / extras["fp64_plain_value"], 3)
 
     # ---- end to end through the reference-facing shim (pinned host exchange arrays) ----
     e2e = None

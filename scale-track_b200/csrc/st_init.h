@@ -25,6 +25,7 @@
 
 #include <stdint.h>
 #include <math.h>
+#include <string.h>
 
 #if defined(__CUDACC__)
 #define ST_IHD __host__ __device__ __forceinline__
@@ -90,8 +91,27 @@ ST_IHD void st_hilbert_segment(int c, int nc, int bits, uint64_t& lo, uint64_t& 
     hi = (2 * (uint64_t)(c + 1) * L + (uint64_t)nc) / (2 * (uint64_t)nc);
 }
 
-ST_IHD float st_next_down(float v) { return nextafterf(v, -INFINITY); }
-ST_IHD double st_next_down(double v) { return nextafter(v, -INFINITY); }
+/* nextafter(v, -inf) on the IEEE bit patterns (the same on host and device, no math
+ * library): zeros step to the negative smallest subnormal, +inf to the largest finite value,
+ * -inf and NaN stay. */
+ST_IHD float st_next_down(float v)
+{
+    if (v != v || v == -INFINITY) return v;
+    uint32_t b;
+    memcpy(&b, &v, sizeof b);
+    b = (v == 0.0f) ? 0x80000001u : (v > 0.0f ? b - 1u : b + 1u);
+    memcpy(&v, &b, sizeof b);
+    return v;
+}
+ST_IHD double st_next_down(double v)
+{
+    if (v != v || v == -(double)INFINITY) return v;
+    uint64_t b;
+    memcpy(&b, &v, sizeof b);
+    b = (v == 0.0) ? 0x8000000000000001ull : (v > 0.0 ? b - 1u : b + 1u);
+    memcpy(&v, &b, sizeof b);
+    return v;
+}
 
 /* v, or the largest value of type P below `ending` when v is not below it. */
 template <class P>
