@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <climits>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 #include <map>
@@ -118,6 +119,7 @@ struct st_handle {
     st_params p;
     st_mesh_desc m;
     int device = 0;
+    int nsm = 148;         /* streaming multiprocessors of the device */
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int dep = DEP_DET1;
@@ -236,7 +238,10 @@ cudaEvent_t take_event(st_handle* h)
         return e;
     }
     cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
+    if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
     return e;
 }
 
@@ -249,18 +254,40 @@ struct ProfScope {
     {
         if (h->prof) {
             a = take_event(h);
-            cudaEventRecord(a, h->stream);
+            if (a && cudaEventRecord(a, h->stream) != cudaSuccess) {
+                cudaGetLastError();
+                h->pool.push_back(a);
+                a = nullptr;
+            }
         }
     }
     ~ProfScope()
     {
+        /* a launch whose events could not be recorded is left out of the profile */
         if (h->prof && a) {
             cudaEvent_t b = take_event(h);
-            cudaEventRecord(b, h->stream);
-            h->recs.push_back({kind, a, b});
+            if (b && cudaEventRecord(b, h->stream) == cudaSuccess) {
+                h->recs.push_back({kind, a, b});
+                return;
+            }
+            cudaGetLastError();
+            h->pool.push_back(a);
+            if (b) h->pool.push_back(b);
         }
     }
 };
+
+/* Blocks per cloud of the finalize pass: four 256-thread blocks per SM over all clouds
+ * (measured on configuration 1: 23 us against 28 us with eight), each thread looping over
+ * groups of four components. */
+int finalize_grid(const st_handle* h)
+{
+    int64_t gx = (h->stride / COMP_ALIGN + 255) / 256;
+    const int64_t cap = ((int64_t)h->nsm * 4 + h->p.n_clouds - 1) / h->p.n_clouds;
+    if (gx > cap) gx = cap;
+    if (gx < 1) gx = 1;
+    return (int)gx;
+}
 
 int ensure_stage(st_handle* h, size_t bytes)
 {
@@ -291,10 +318,11 @@ int check_device_errors(st_handle* h)
         CK(cudaMemcpyAsync(h->dctl, ctl.data(), sizeof(CloudCtl) * nc, cudaMemcpyHostToDevice,
                            h->stream));
         CK(cudaStreamSynchronize(h->stream));
+        /* lost parcels take precedence in the status; the message counts both */
         if (lost)
             return fail(ST_ERR_PARCEL_OUTSIDE,
                         "%llu parcel(s) could not be located in the mesh and were left "
-                        "unchanged", lost);
+                        "unchanged; %llu deposit component(s) out of range", lost, ovf);
         return fail(ST_ERR_SOURCE_RANGE,
                     "%llu deposit component(s) were non-finite or exceeded the fixed-point "
                     "range of the deterministic source and were dropped", ovf);
@@ -440,14 +468,10 @@ int do_step(st_handle* h, double dt, double fscale)
         h->launches += 1;
     }
     if (det) {
-        int64_t gx = (h->stride / COMP_ALIGN + 255) / 256;
-        int64_t cap = (148 * 8 + h->p.n_clouds - 1) / h->p.n_clouds;
-        if (gx > cap) gx = cap;
-        if (gx < 1) gx = 1;
         {
             ProfScope ps(h, ST_KERNEL_FINALIZE);
             CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter,
-                               h->p.n_clouds, h->stride, (int)gx, h->stream));
+                               h->p.n_clouds, h->stride, finalize_grid(h), h->stream));
             h->launches += 1;
         }
         CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * h->p.n_clouds * h->limbs * 8,
@@ -511,14 +535,10 @@ int do_step_tet(st_handle* h, double dt, double fscale)
         h->launches += 1;
     }
     if (det) {
-        int64_t gx = (h->stride / COMP_ALIGN + 255) / 256;
-        int64_t cap = (148 * 8 + h->p.n_clouds - 1) / h->p.n_clouds;
-        if (gx > cap) gx = cap;
-        if (gx < 1) gx = 1;
         {
             ProfScope ps(h, ST_KERNEL_FINALIZE);
             CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter,
-                               h->p.n_clouds, h->stride, (int)gx, h->stream));
+                               h->p.n_clouds, h->stride, finalize_grid(h), h->stream));
             h->launches += 1;
         }
         CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * h->p.n_clouds * h->limbs * 8,
@@ -1172,6 +1192,18 @@ int adj_pullback(st_handle* h, int cloud, const st_adjoint_desc* d, const double
 /* ------------------------------------------------------------------------------------ */
 /* public API                                                                           */
 /* ------------------------------------------------------------------------------------ */
+/* Host-side staging grows with the parcel count; an allocation failure becomes a status
+ * instead of an exception crossing the C ABI. */
+template <class F>
+static int guard_host_alloc(const char* what, F&& body)
+{
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        return fail(ST_ERR_OUT_OF_MEMORY, "%s: out of host memory", what);
+    }
+}
+
 extern "C" {
 
 const char* st_version(void) { return "scaletrack-b200 0.1 sm_100a"; }
@@ -1274,10 +1306,11 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
         (e = cudaMalloc(&h->dclouds, 256 * (size_t)p->n_clouds)) != cudaSuccess)
         return bail(fail(e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA,
                          "device allocation: %s", cudaGetErrorString(e)));
-    cudaMemsetAsync(h->dU, 0, ncomp * h->vsz, h->stream);
-    cudaMemsetAsync(h->dsrc, 0, cells_total * sizeof(double), h->stream);
-    cudaMemsetAsync(h->dacc, 0, cells_total * h->limbs * 8, h->stream);
-    cudaMemsetAsync(h->dcounter, 0, sizeof(unsigned int), h->stream);
+    if ((e = cudaMemsetAsync(h->dU, 0, ncomp * h->vsz, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->dsrc, 0, cells_total * sizeof(double), h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->dacc, 0, cells_total * h->limbs * 8, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->dcounter, 0, sizeof(unsigned int), h->stream)) != cudaSuccess)
+        return bail(fail(ST_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e)));
     {
         std::vector<CloudCtl> ctl(p->n_clouds);
         /* bound on the deposits one cloud makes per step: one per parcel and substep */
@@ -1334,6 +1367,7 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
     }
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    h->nsm = nsm > 0 ? nsm : 148;
     int occ = h->tet ? (p->precision == ST_PREC_FP64
                             ? step_tet_max_active_blocks<double>(h->dep, h->block)
                             : step_tet_max_active_blocks<float>(h->dep, h->block))
@@ -1359,10 +1393,20 @@ int st_create(const st_params* p, const st_mesh_desc* m, int device, st_handle**
     if (ncells > INT32_MAX)
         return fail(ST_ERR_INVALID_ARGUMENT, "mesh has %lld cells; at most 2^31-1 supported",
                     (long long)ncells);
-    return create_impl(p, m, ncells, nullptr, device, out);
+    return guard_host_alloc("st_create",
+                            [&] { return create_impl(p, m, ncells, nullptr, device, out); });
 }
 
+static int create_tet_impl(const st_params* p, const st_tet_mesh_desc* tm, int device,
+                           st_handle** out);
+
 int st_create_tet(const st_params* p, const st_tet_mesh_desc* tm, int device, st_handle** out)
+{
+    return guard_host_alloc("st_create_tet", [&] { return create_tet_impl(p, tm, device, out); });
+}
+
+static int create_tet_impl(const st_params* p, const st_tet_mesh_desc* tm, int device,
+                           st_handle** out)
 {
     if (!p || !tm || !out) return fail(ST_ERR_INVALID_ARGUMENT, "null argument to st_create_tet");
     *out = nullptr;
@@ -1470,7 +1514,8 @@ static int set_parcels_impl(st_handle* h, int cloud, int64_t n, const double* xy
 int st_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const double* uvw,
                    const double* d)
 {
-    return set_parcels_impl(h, cloud, n, xyz, uvw, d, nullptr);
+    return guard_host_alloc("st_set_parcels",
+                            [&] { return set_parcels_impl(h, cloud, n, xyz, uvw, d, nullptr); });
 }
 
 int st_append_parcels(st_handle* h, int cloud, int64_t m, const double* xyz, const double* uvw,
@@ -1486,7 +1531,9 @@ int st_append_parcels(st_handle* h, int cloud, int64_t m, const double* xyz, con
     DeviceGuard g(h->device);
     CK(cudaStreamSynchronize(h->stream));
     release_graph(h);
-    rc = DISPATCH(h, do_append_parcels, h, cloud, m, xyz, uvw, d);
+    rc = guard_host_alloc("st_append_parcels",
+                          [&] { return DISPATCH(h, do_append_parcels, h, cloud, m, xyz, uvw,
+                                                d); });
     if (rc) return rc;
     return update_headroom(h);
 }
@@ -1514,7 +1561,8 @@ int st_set_parcels_tet(st_handle* h, int cloud, int64_t n, const double* xyz, co
                        const double* d, const int32_t* hint)
 {
     if (h && !h->tet) return fail(ST_ERR_INVALID_ARGUMENT, "st_set_parcels_tet on a cuboid mesh");
-    return set_parcels_impl(h, cloud, n, xyz, uvw, d, hint);
+    return guard_host_alloc("st_set_parcels_tet",
+                            [&] { return set_parcels_impl(h, cloud, n, xyz, uvw, d, hint); });
 }
 
 int st_tet_hop_histogram(st_handle* h, uint64_t out[8], int reset)
@@ -1561,10 +1609,12 @@ int st_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d)
     DeviceGuard g(h->device);
     if ((rc = check_device_errors(h))) {
         /* still hand back the state: lost parcels were left unchanged */
-        int rc2 = DISPATCH(h, do_get_parcels, h, cloud, xyz, uvw, d);
+        int rc2 = guard_host_alloc(
+            "st_get_parcels", [&] { return DISPATCH(h, do_get_parcels, h, cloud, xyz, uvw, d); });
         return rc2 ? rc2 : rc;
     }
-    return DISPATCH(h, do_get_parcels, h, cloud, xyz, uvw, d);
+    return guard_host_alloc("st_get_parcels",
+                            [&] { return DISPATCH(h, do_get_parcels, h, cloud, xyz, uvw, d); });
 }
 
 int st_get_cells(st_handle* h, int cloud, int32_t* cells)
@@ -1574,8 +1624,10 @@ int st_get_cells(st_handle* h, int cloud, int32_t* cells)
     if (!cells && h->clouds[cloud].n > 0) return fail(ST_ERR_INVALID_ARGUMENT, "null cells");
     DeviceGuard g(h->device);
     int err = check_device_errors(h);
-    rc = h->p.precision == ST_PREC_FP32 ? do_get_cells<float>(h, cloud, cells)
-                                        : do_get_cells<double>(h, cloud, cells);
+    rc = guard_host_alloc("st_get_cells", [&] {
+        return h->p.precision == ST_PREC_FP32 ? do_get_cells<float>(h, cloud, cells)
+                                              : do_get_cells<double>(h, cloud, cells);
+    });
     return rc ? rc : err;
 }
 
@@ -1702,15 +1754,22 @@ int st_profile_read(st_handle* h, int kind, int64_t* launches, double* ms, int r
         return fail(ST_ERR_INVALID_ARGUMENT, "unknown kernel kind %d", kind);
     DeviceGuard g(h->device);
     CK(cudaStreamSynchronize(h->stream));
+    cudaError_t err = cudaSuccess;
     for (auto& r : h->recs) {
         float t = 0.f;
-        CK(cudaEventElapsedTime(&t, r.a, r.b));
-        h->prof_ms[r.kind] += t;
-        h->prof_launches[r.kind] += 1;
+        const cudaError_t e = cudaEventElapsedTime(&t, r.a, r.b);
+        if (e == cudaSuccess) {
+            h->prof_ms[r.kind] += t;
+            h->prof_launches[r.kind] += 1;
+        } else if (err == cudaSuccess) {
+            err = e;
+        }
         h->pool.push_back(r.a);
         h->pool.push_back(r.b);
     }
     h->recs.clear();
+    if (err != cudaSuccess)
+        return fail(ST_ERR_CUDA, "cudaEventElapsedTime: %s", cudaGetErrorString(err));
     if (launches) *launches = h->prof_launches[kind];
     if (ms) *ms = h->prof_ms[kind];
     if (reset) {
@@ -1731,8 +1790,11 @@ int st_mean_source_forward(st_handle* h, int cloud, const st_adjoint_desc* desc,
     if ((rc = adj_check(h, cloud, desc))) return rc;
     DeviceGuard g(h->device);
     CK(cudaStreamSynchronize(h->stream));
-    return h->p.precision == ST_PREC_MIXED ? adj_forward<double, float>(h, cloud, desc, mean_source)
-                                           : adj_forward<double, double>(h, cloud, desc, mean_source);
+    return guard_host_alloc("st_mean_source_forward", [&] {
+        return h->p.precision == ST_PREC_MIXED
+                   ? adj_forward<double, float>(h, cloud, desc, mean_source)
+                   : adj_forward<double, double>(h, cloud, desc, mean_source);
+    });
 }
 
 int st_mean_source_pullback(st_handle* h, int cloud, const st_adjoint_desc* desc,
@@ -1744,11 +1806,13 @@ int st_mean_source_pullback(st_handle* h, int cloud, const st_adjoint_desc* desc
     if (!cotangent) return fail(ST_ERR_INVALID_ARGUMENT, "null cotangent");
     DeviceGuard g(h->device);
     CK(cudaStreamSynchronize(h->stream));
-    return h->p.precision == ST_PREC_MIXED
-               ? adj_pullback<double, float>(h, cloud, desc, cotangent, d_drag_multiplier,
-                                             d_diameter_scale, d_velocity0)
-               : adj_pullback<double, double>(h, cloud, desc, cotangent, d_drag_multiplier,
-                                              d_diameter_scale, d_velocity0);
+    return guard_host_alloc("st_mean_source_pullback", [&] {
+        return h->p.precision == ST_PREC_MIXED
+                   ? adj_pullback<double, float>(h, cloud, desc, cotangent, d_drag_multiplier,
+                                                 d_diameter_scale, d_velocity0)
+                   : adj_pullback<double, double>(h, cloud, desc, cotangent, d_drag_multiplier,
+                                                  d_diameter_scale, d_velocity0);
+    });
 }
 
 int st_graph_capture(st_handle* h, int n_steps, double dt, const double* fluid_scale)
@@ -1789,7 +1853,15 @@ int st_graph_release(st_handle* h)
     return ST_OK;
 }
 
+static int autotune_impl(st_handle* h, double dt, int trial_steps, st_tune_result* out);
+
 int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out)
+{
+    return guard_host_alloc("st_autotune",
+                            [&] { return autotune_impl(h, dt, trial_steps, out); });
+}
+
+static int autotune_impl(st_handle* h, double dt, int trial_steps, st_tune_result* out)
 {
     int rc;
     if ((rc = check_handle(h))) return rc;
@@ -1821,8 +1893,11 @@ int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out)
     best.sort_interval = h->p.sort_interval;
     best.ms_per_step = 1e300;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    if (rc == ST_OK) {
+        cudaError_t e = cudaEventCreate(&e0);
+        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        if (e != cudaSuccess) rc = fail(ST_ERR_CUDA, "cudaEventCreate: %s", cudaGetErrorString(e));
+    }
     for (int bi = 0; bi < 2 && rc == ST_OK; ++bi) {
         for (int si = 0; si < 4 && rc == ST_OK; ++si) {
             if (sorts[si] > trial_steps) continue;
@@ -1832,13 +1907,19 @@ int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out)
             t->steps_since_sort = 0;
             if ((rc = DISPATCH(t, do_sort_all, t))) break;  /* every trial starts sorted */
             for (int k = 0; k < 2 && rc == ST_OK; ++k) rc = st_step(t, dt, 1.0);
-            cudaEventRecord(e0, t->stream);
-            for (int k = 0; k < trial_steps && rc == ST_OK; ++k) rc = st_step(t, dt, 1.0);
-            cudaEventRecord(e1, t->stream);
+            if (rc) break;
+            cudaError_t e = cudaEventRecord(e0, t->stream);
+            for (int k = 0; k < trial_steps && rc == ST_OK && e == cudaSuccess; ++k)
+                rc = st_step(t, dt, 1.0);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, t->stream);
             if (rc) break;
             if ((rc = st_synchronize(t))) break;
             float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) {
+                rc = fail(ST_ERR_CUDA, "autotuner timing: %s", cudaGetErrorString(e));
+                break;
+            }
             const double per = ms / trial_steps;
             if (per < best.ms_per_step) {
                 best.block_size = blocks[bi];
@@ -1848,8 +1929,8 @@ int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out)
             }
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
     st_destroy(t);
     if (rc) return rc;
     h->block = best.block_size;
@@ -1872,7 +1953,7 @@ int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out)
  * fixed-point scale L carried over, a restarted run continues bit for bit. */
 static const char ST_STATE_MAGIC[8] = {'S', 'T', 'S', 'T', 'A', 'T', 'E', '1'};
 
-int st_save_state(st_handle* h, const char* path)
+static int save_state_impl(st_handle* h, const char* path)
 {
     int rc;
     if ((rc = check_handle(h))) return rc;
@@ -1920,17 +2001,26 @@ int st_save_state(st_handle* h, const char* path)
     return ST_OK;
 }
 
-int st_load_state(st_handle* h, const char* path)
+int st_save_state(st_handle* h, const char* path)
+{
+    return guard_host_alloc("st_save_state", [&] { return save_state_impl(h, path); });
+}
+
+/* Reads the whole file and checks it before the handle is touched, so a truncated or
+ * inconsistent file leaves the handle as it was. */
+static int load_state_impl(st_handle* h, const char* path)
 {
     int rc;
-    if ((rc = check_handle(h))) return rc;
-    if (!path) return fail(ST_ERR_INVALID_ARGUMENT, "null path");
-    FILE* f = fopen(path, "rb");
+    struct Closer {
+        FILE* f;
+        ~Closer() { if (f) fclose(f); }
+    } file{fopen(path, "rb")};
+    FILE* f = file.f;
     if (!f) return fail(ST_ERR_INVALID_ARGUMENT, "cannot open %s", path);
-    auto bad = [&](const char* why) {
-        fclose(f);
-        return fail(ST_ERR_INVALID_ARGUMENT, "%s: %s", path, why);
-    };
+    auto bad = [&](const char* why) { return fail(ST_ERR_INVALID_ARGUMENT, "%s: %s", path, why); };
+    if (fseek(f, 0, SEEK_END) != 0) return bad("cannot seek");
+    const long fsize = ftell(f);
+    if (fsize < 0 || fseek(f, 0, SEEK_SET) != 0) return bad("cannot seek");
     char magic[8];
     int32_t hdr[4], sched[2];
     int64_t nce, steps;
@@ -1944,30 +2034,49 @@ int st_load_state(st_handle* h, const char* path)
     if (hdr[0] != h->p.precision || hdr[1] != h->p.n_clouds || hdr[2] != (h->tet ? 1 : 0) ||
         nce != h->ncells)
         return bad("precision, cloud count, mesh kind or cell count differ from the handle's");
+    if (steps < 0 || sched[0] < 0 || (sched[1] != 0 && sched[1] != 1) || !(last_dt >= 0.0) ||
+        !(last_dt < 1e300))
+        return bad("invalid step bookkeeping");
     const int nc = h->p.n_clouds;
-    std::vector<int32_t> L(nc), H(nc);
+    const int64_t per_parcel = 7 * 8 + (h->tet ? 4 : 0);
+    struct Cloud {
+        int32_t L = 0, H = 0;
+        int64_t n = 0;
+        std::vector<double> xyz, uvw, d;
+        std::vector<int32_t> cells;
+    };
+    std::vector<Cloud> cl(nc);
     for (int c = 0; c < nc; ++c) {
         int32_t lh[2];
         int64_t n;
-        if (fread(lh, sizeof lh, 1, f) != 1 || fread(&n, 8, 1, f) != 1 || n < 0 ||
-            n > INT32_MAX)
+        if (fread(lh, sizeof lh, 1, f) != 1 || fread(&n, 8, 1, f) != 1)
             return bad("truncated cloud header");
-        L[c] = lh[0];
-        H[c] = lh[1];
-        std::vector<double> xyz(3 * n), uvw(3 * n), d(n);
-        std::vector<int32_t> cells(h->tet ? n : 0);
-        if (n > 0 && (fread(xyz.data(), 8, 3 * n, f) != (size_t)(3 * n) ||
-                      fread(uvw.data(), 8, 3 * n, f) != (size_t)(3 * n) ||
-                      fread(d.data(), 8, n, f) != (size_t)n ||
-                      (h->tet && fread(cells.data(), 4, n, f) != (size_t)n)))
+        /* the deposit exponent lies in [-1074, 1024] and the headroom in [0, 62] */
+        if (n < 0 || n > INT32_MAX || lh[1] < 0 || lh[1] > 62 || lh[0] < -1200 || lh[0] > 1100)
+            return bad("invalid cloud header");
+        const long here = ftell(f);
+        if (here < 0 || (int64_t)(fsize - here) < n * per_parcel)
             return bad("truncated parcel data");
-        if ((rc = set_parcels_impl(h, c, n, xyz.data(), uvw.data(), d.data(),
-                                   h->tet ? cells.data() : nullptr))) {
-            fclose(f);
-            return rc;
-        }
+        Cloud& k = cl[c];
+        k.L = lh[0];
+        k.H = lh[1];
+        k.n = n;
+        k.xyz.resize(3 * n);
+        k.uvw.resize(3 * n);
+        k.d.resize(n);
+        k.cells.resize(h->tet ? n : 0);
+        if (n > 0 && (fread(k.xyz.data(), 8, 3 * n, f) != (size_t)(3 * n) ||
+                      fread(k.uvw.data(), 8, 3 * n, f) != (size_t)(3 * n) ||
+                      fread(k.d.data(), 8, n, f) != (size_t)n ||
+                      (h->tet && fread(k.cells.data(), 4, n, f) != (size_t)n)))
+            return bad("truncated parcel data");
     }
-    fclose(f);
+    for (int c = 0; c < nc; ++c) {
+        Cloud& k = cl[c];
+        if ((rc = set_parcels_impl(h, c, k.n, k.xyz.data(), k.uvw.data(), k.d.data(),
+                                   h->tet ? k.cells.data() : nullptr)))
+            return rc;
+    }
     /* the scale of the next step and the step bookkeeping, as saved */
     DeviceGuard g(h->device);
     std::vector<CloudCtl> ctl(nc);
@@ -1975,8 +2084,8 @@ int st_load_state(st_handle* h, const char* path)
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
     for (int c = 0; c < nc; ++c) {
-        ctl[c].L = L[c];
-        ctl[c].H = H[c];
+        ctl[c].L = cl[c].L;
+        ctl[c].H = cl[c].H;
         ctl[c].emax = EXP_NONE;
     }
     CK(cudaMemcpyAsync(h->dctl, ctl.data(), sizeof(CloudCtl) * nc, cudaMemcpyHostToDevice,
@@ -1987,6 +2096,14 @@ int st_load_state(st_handle* h, const char* path)
     h->steps_since_sort = sched[0];
     h->need_probe = sched[1] != 0;
     return ST_OK;
+}
+
+int st_load_state(st_handle* h, const char* path)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (!path) return fail(ST_ERR_INVALID_ARGUMENT, "null path");
+    return guard_host_alloc("st_load_state", [&] { return load_state_impl(h, path); });
 }
 
 /* ------------------------------------------------------------------------------------ */
@@ -2039,6 +2156,20 @@ static void async_release()
     if (a.duraw) cudaFree(a.duraw);
     if (a.hctl) cudaFreeHost(a.hctl);
     a = AsyncCoupling();
+}
+
+/* st_setup with another mesh keeps the exchange arrays (the caller may still hold them),
+ * so a step checks that they were allocated for the default handle's cell count;
+ * st_finalize releases them for a new allocation. */
+static int check_exchange_sizes(const st_handle* h, const Adopted& U, const Adopted& S)
+{
+    for (const Adopted* a : {&U, &S})
+        if ((int64_t)a->size != h->ncells || a->ncomp != 3)
+            return fail(ST_ERR_INVALID_ARGUMENT,
+                        "the exchange arrays hold %d cells, the mesh of st_setup has %lld: "
+                        "call st_finalize and allocate them again", a->size,
+                        (long long)h->ncells);
+    return ST_OK;
 }
 
 int st_setup(const st_params* p, const st_mesh_desc* m)
@@ -2127,6 +2258,7 @@ int st_evolve_cloud(double dt)
     if (iu == g_arrays.end() || is == g_arrays.end())
         return fail(ST_ERR_NOT_INITIALISED, "U and UTrans must be allocated with "
                                             "st_allocate_array before st_evolve_cloud");
+    if (int rc0 = check_exchange_sizes(h, iu->second, is->second)) return rc0;
     DeviceGuard g(h->device);
     const int64_t ncomp = h->ncells * 3;
     int rc;
@@ -2185,6 +2317,7 @@ int st_evolve_cloud_async(double dt)
     if (iu == g_arrays.end() || is == g_arrays.end())
         return fail(ST_ERR_NOT_INITIALISED, "U and UTrans must be allocated with "
                                             "st_allocate_array before st_evolve_cloud_async");
+    if (int rc0 = check_exchange_sizes(h, iu->second, is->second)) return rc0;
     if (!(dt > 0) || !(dt < 1e300))
         return fail(ST_ERR_INVALID_ARGUMENT, "dt must be positive and finite, got %g", dt);
     if (h->tet) return fail(ST_ERR_INVALID_ARGUMENT, "the shims drive cuboid meshes");

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <new>
 #include <vector>
 
 #include "scaletrack.h"
@@ -34,7 +35,19 @@ struct Block {
 
 extern "C" {
 
+static int write_vtu_impl(st_handle* h, int cloud, const char* path);
+
 int st_write_vtu(st_handle* h, int cloud, const char* path)
+{
+    try {
+        return write_vtu_impl(h, cloud, path);
+    } catch (const std::bad_alloc&) {
+        st::st_set_last_error("st_write_vtu: out of host memory");
+        return ST_ERR_OUT_OF_MEMORY;
+    }
+}
+
+static int write_vtu_impl(st_handle* h, int cloud, const char* path)
 {
     if (!h || !path) return io_fail("null argument to st_write_vtu");
     const int64_t n = st_num_parcels(h, cloud);

@@ -63,7 +63,7 @@ __global__ void k_sort_keys(const P* __restrict__ x, const P* __restrict__ y,
 
 /* Permutes the SoA arrays into sorted order.  Each thread handles GATHER_ILP outputs and
  * issues all their (scattered) loads before any store, so that many reads are in flight. */
-constexpr int GATHER_ILP = 4;
+constexpr int GATHER_ILP = 2;
 
 /* tet meshes: the key is the owning tet (tets are numbered with spatial locality) */
 __global__ void k_sort_keys_cell(const int32_t* __restrict__ cell, int64_t n,

@@ -107,3 +107,22 @@ def test_mapped_exchange_equals_copies(tbytes):
             assert np.array_equal(UT.astype(np.float64), ref[k]), k
     finally:
         st.finalize()
+
+
+def test_setup_with_another_mesh_rejects_old_exchange_arrays():
+    """st_setup on a different mesh keeps the arrays the caller holds; a step then refuses
+    them (instead of copying past their end) until st_finalize releases them."""
+    U, UT = _setup(4)
+    try:
+        prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                        precision="mixed")
+        st.setup(prm, st.mesh_desc(2 * N, 0.0, workload.L_BOX))
+        for call in (st.evolve_cloud, st.evolve_cloud_async):
+            with pytest.raises(st.ScaleTrackError) as ei:
+                call(workload.DT)
+            assert ei.value.code == st.ST_ERR_INVALID_ARGUMENT
+            assert "st_finalize" in str(ei.value)
+    finally:
+        st.finalize()
+    _setup(4)                      # a fresh allocation after st_finalize works again
+    st.finalize()

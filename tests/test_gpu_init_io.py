@@ -195,3 +195,31 @@ def test_append_parcels_continues_like_the_oracle(prec):
     assert np.array_equal(gx, r2["xyz"]) and np.array_equal(gv, r2["uvw"])
     assert np.array_equal(gc, r2["cells"])
     assert np.array_equal(gs, r2["src_quant"])
+
+
+def test_load_state_checks_the_whole_file_before_changing_the_handle(tmp_path):
+    """A truncated file, or one with an impossible fixed-point scale, is rejected and the
+    handle keeps its parcels."""
+    prm = st.params(precision="mixed")
+    path = str(tmp_path / "s.bin")
+    with st.ParcelTracker(prm, st.mesh_desc(8, 0.0, L)) as h:
+        h.init_parcels(100, 1, 5e-6, 5e-5)
+        h.save_state(path)
+    raw = open(path, "rb").read()
+    hdr = 8 + 16 + 8 + 8 + 8 + 8                  # magic, 4 int32, nCells, dt, steps, sched
+    bad_scale = bytearray(raw)
+    bad_scale[hdr:hdr + 4] = (5000).to_bytes(4, "little", signed=True)   # L
+    cases = {"truncated": raw[:-12], "bad_scale": bytes(bad_scale)}
+    for name, blob in cases.items():
+        p = str(tmp_path / (name + ".bin"))
+        with open(p, "wb") as f:
+            f.write(blob)
+        with st.ParcelTracker(prm, st.mesh_desc(8, 0.0, L)) as h2:
+            h2.init_parcels(37, 2, 5e-6, 5e-5)
+            before = h2.get_parcels()
+            with pytest.raises(st.ScaleTrackError) as ei:
+                h2.load_state(p)
+            assert ei.value.code == st.ST_ERR_INVALID_ARGUMENT, name
+            after = h2.get_parcels()
+            for a, b in zip(before, after):
+                assert np.array_equal(a, b), name
