@@ -120,6 +120,10 @@ ST_API int st_append_parcels(st_handle* h, int cloud, int64_t m, const double* x
 ST_API int st_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d);
 /* 0-based owning cell of each parcel (locate, A:680-693), order as st_set_parcels. */
 ST_API int st_get_cells(st_handle* h, int cloud, int32_t* cells);
+/* Device-side order of a cloud: ids[k] = index (in the order given to st_set_parcels) of the
+ * parcel stored at position k of the device arrays, which the periodic re-sort groups by
+ * owning cell.  Diagnostic; no counterpart in the reference. */
+ST_API int st_get_order(st_handle* h, int cloud, int32_t* ids);
 ST_API int64_t st_num_parcels(st_handle* h, int cloud);
 ST_API int64_t st_num_cells(st_handle* h);
 

@@ -155,6 +155,11 @@ struct st_handle {
     double prof_ms[ST_KERNEL_KINDS] = {};
     void* dstage = nullptr;
     size_t stage_bytes = 0;
+    /* counting-sort bins shared by the clouds (key ranges up to 2^COUNT_SORT_MAX_BITS) */
+    uint32_t* dbins = nullptr;
+    uint32_t* doffs = nullptr;
+    void* dscan = nullptr;
+    size_t scan_bytes = 0;
     AdjTape adj;
     /* unstructured tetrahedral mesh */
     bool tet = false;
@@ -331,9 +336,13 @@ int check_device_errors(st_handle* h)
 }
 
 template <class P, class V>
-SortBufs<P, V> sort_bufs(CloudBufs& c)
+SortBufs<P, V> sort_bufs(const st_handle* h, CloudBufs& c)
 {
     SortBufs<P, V> b;
+    b.bins = h->dbins;
+    b.offsets = h->doffs;
+    b.scan_temp = h->dscan;
+    b.scan_temp_bytes = h->scan_bytes;
     for (int k = 0; k < 2; ++k) {
         b.x[k] = (P*)c.x[k];
         b.y[k] = (P*)c.y[k];
@@ -390,7 +399,7 @@ int do_sort_all(st_handle* h)
     const MeshK<P> mk = mesh_k<P>(h);
     for (auto& c : h->clouds) {
         if (c.n <= 1) continue;
-        SortBufs<P, V> b = sort_bufs<P, V>(c);
+        SortBufs<P, V> b = sort_bufs<P, V>(h, c);
         int nl = 0;
         {
             ProfScope ps(h, ST_KERNEL_SORT);
@@ -662,7 +671,7 @@ int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
     h->need_probe = true;
     if (h->p.sort_interval > 0 && n > 1) {
         CloudBufs& cc = h->clouds[cloud];
-        SortBufs<P, V> b = sort_bufs<P, V>(cc);
+        SortBufs<P, V> b = sort_bufs<P, V>(h, cc);
         int nl = 0;
         ProfScope ps(h, ST_KERNEL_SORT);
         CK(sort_cloud<P, V>(b, cc.cur, cc.n, mesh_k<P>(h), h->key_bits, h->morton, h->stream,
@@ -784,7 +793,7 @@ int do_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d)
     CloudBufs& c = h->clouds[cloud];
     const int64_t n = c.n;
     if (n == 0) return ST_OK;
-    SortBufs<P, V> b = sort_bufs<P, V>(c);
+    SortBufs<P, V> b = sort_bufs<P, V>(h, c);
     {
         ProfScope ps(h, ST_KERNEL_OTHER);
         CK(unpermute_cloud<P, V>(b, c.cur, n, h->stream));
@@ -1311,6 +1320,15 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
         (e = cudaMemsetAsync(h->dacc, 0, cells_total * h->limbs * 8, h->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->dcounter, 0, sizeof(unsigned int), h->stream)) != cudaSuccess)
         return bail(fail(ST_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e)));
+    if (h->key_bits <= COUNT_SORT_MAX_BITS) {
+        const size_t nb = (size_t)1 << h->key_bits;
+        h->scan_bytes = count_sort_scan_bytes(h->key_bits);
+        if ((e = cudaMalloc((void**)&h->dbins, nb * sizeof(uint32_t))) != cudaSuccess ||
+            (e = cudaMalloc((void**)&h->doffs, nb * sizeof(uint32_t))) != cudaSuccess ||
+            (e = cudaMalloc(&h->dscan, h->scan_bytes > 0 ? h->scan_bytes : 16)) != cudaSuccess)
+            return bail(fail(e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA,
+                             "device allocation: %s", cudaGetErrorString(e)));
+    }
     {
         std::vector<CloudCtl> ctl(p->n_clouds);
         /* bound on the deposits one cloud makes per step: one per parcel and substep */
@@ -1467,7 +1485,7 @@ int st_destroy(st_handle* h)
     if (h->graph) cudaGraphDestroy(h->graph);
     void* arrs[] = {h->dU, h->dsrc, h->dacc, h->dctl, h->dcounter, h->dcount, h->dclouds,
                     h->dstage, h->adj.mem, h->dclouds2, h->d_verts, h->d_tets, h->d_planes, h->d_nbr,
-                    h->d_hops};
+                    h->d_hops, h->dbins, h->doffs, h->dscan};
     for (void* p : arrs)
         if (p) cudaFree(p);
     for (auto& r : h->recs) {
@@ -1629,6 +1647,20 @@ int st_get_cells(st_handle* h, int cloud, int32_t* cells)
                                               : do_get_cells<double>(h, cloud, cells);
     });
     return rc ? rc : err;
+}
+
+int st_get_order(st_handle* h, int cloud, int32_t* ids)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    const CloudBufs& c = h->clouds[cloud];
+    if (c.n == 0) return ST_OK;
+    if (!ids) return fail(ST_ERR_INVALID_ARGUMENT, "null ids");
+    DeviceGuard g(h->device);
+    CK(cudaMemcpyAsync(ids, c.id[c.cur], c.n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ST_OK;
 }
 
 static int set_fluid(st_handle* h, const void* U, int elem_bytes, bool device)

@@ -215,9 +215,17 @@ struct SortBufs {
     uint32_t* perm[2];
     void* temp;
     size_t temp_bytes;
+    /* counting sort (key range of at most 2^COUNT_SORT_MAX_BITS): per-key counts and
+     * offsets, shared by the clouds of a handle; nullptr selects the radix sort */
+    uint32_t* bins;
+    uint32_t* offsets;
+    void* scan_temp;
+    size_t scan_temp_bytes;
 };
+constexpr int COUNT_SORT_MAX_BITS = 24;
 template <class P, class V>
 size_t sort_temp_bytes(int64_t n);
+size_t count_sort_scan_bytes(int key_bits);
 template <class P, class V>
 cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& mesh, int key_bits,
                        bool morton, cudaStream_t s, int* launches);

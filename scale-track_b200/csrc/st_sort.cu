@@ -5,14 +5,20 @@
  * Sorting keeps parcels of the same cell next to each other, so the warp-level run
  * reduction of the deposit collapses most of a tile into a few atomics, and neighbouring
  * warps gather neighbouring cells of U (L2 locality).  Keys are the Morton code of the cell
- * (i, j, k) (or the linear cell index for meshes wider than 1024 cells), sorted with CUB's
- * stable LSD radix sort, then every SoA array and the parcel id are gathered out of place
- * into the other buffer.  The reference has no re-sort: its parcels keep their Hilbert
- * ordered initial positions inside each chunk (A:559-638).
+ * (i, j, k) (the linear cell index for meshes wider than 1024 cells, the owning tet on tet
+ * meshes).  Key ranges of at most 2^24 values are ranked by a counting sort: per-key counts
+ * with warp-aggregated atomics, an exclusive scan, then each warp claims its slots of each
+ * key with one atomic.  Parcels of one key keep their order inside a warp; across warps it
+ * follows the order of the atomics, which no result depends on (the deposit is an exact
+ * integer sum and everything else is per parcel).  Wider key ranges use CUB's LSD radix
+ * sort.  Then every SoA array and the parcel id are gathered out of place into the other
+ * buffer.  The reference has no re-sort: its parcels keep their Hilbert ordered initial
+ * positions inside each chunk (A:559-638).
  */
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "st_internal.h"
 
@@ -57,7 +63,7 @@ __global__ void k_sort_keys(const P* __restrict__ x, const P* __restrict__ y,
                                  (spread3((uint32_t)k) << 2))
                               : (uint32_t)(k * m.NxNy + j * m.N[0] + i);
         keys[p] = key;
-        perm[p] = (uint32_t)p;
+        if (perm) perm[p] = (uint32_t)p;
     }
 }
 
@@ -72,7 +78,7 @@ __global__ void k_sort_keys_cell(const int32_t* __restrict__ cell, int64_t n,
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (int64_t)gridDim.x * blockDim.x) {
         keys[p] = (uint32_t)cell[p];
-        perm[p] = (uint32_t)p;
+        if (perm) perm[p] = (uint32_t)p;
     }
 }
 
@@ -202,6 +208,58 @@ __global__ void k_cells(const P* __restrict__ x, const P* __restrict__ y,
     }
 }
 
+/* ------------------------------------------------------------------------------------ */
+/* counting sort                                                                        */
+/* ------------------------------------------------------------------------------------ */
+constexpr unsigned FULL_WARP = 0xffffffffu;
+constexpr uint32_t NO_KEY = 0xffffffffu;   /* lanes past the end (keys are below 2^24) */
+
+/* bins[key] += number of parcels with that key; one atomic per distinct key and warp */
+__global__ void k_bin_count(const uint32_t* __restrict__ keys, int64_t n, uint32_t nbins,
+                            uint32_t* __restrict__ bins)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 < n;
+         w += nw) {
+        const int64_t p = w * 32 + lane;
+        /* keys are below nbins by construction; the clamp only guards the bins */
+        const uint32_t key = p < n ? min(__ldcs(keys + p), nbins - 1u) : NO_KEY;
+        const unsigned same = __match_any_sync(FULL_WARP, key);
+        if (key != NO_KEY && lane == __ffs(same) - 1) atomicAdd(bins + key, (uint32_t)__popc(same));
+    }
+}
+
+/* perm[slot] = p, slot = the key's offset + the parcel's rank among the parcels of the
+ * same key; each warp reserves its parcels' slots of a key with one atomic (offsets are
+ * the exclusive scan of the counts and move forward as slots are taken). */
+__global__ void k_bin_rank(const uint32_t* __restrict__ keys, int64_t n, uint32_t nbins,
+                           uint32_t* __restrict__ offsets, uint32_t* __restrict__ perm)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 < n;
+         w += nw) {
+        const int64_t p = w * 32 + lane;
+        const uint32_t key = p < n ? min(__ldcs(keys + p), nbins - 1u) : NO_KEY;
+        const unsigned same = __match_any_sync(FULL_WARP, key);
+        const int leader = __ffs(same) - 1;
+        uint32_t base = 0;
+        if (key != NO_KEY && lane == leader) base = atomicAdd(offsets + key, (uint32_t)__popc(same));
+        base = __shfl_sync(FULL_WARP, base, leader);
+        if (key != NO_KEY) perm[base + __popc(same & below)] = (uint32_t)p;
+    }
+}
+
+size_t count_sort_scan_bytes(int key_bits)
+{
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (int)((int64_t)1 << key_bits));
+    return bytes;
+}
+
 static int grid_for(int64_t n)
 {
     int64_t g = (n + 255) / 256;
@@ -226,17 +284,33 @@ cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& me
 {
     if (n <= 1) return cudaSuccess;
     const int o = 1 - cur;
+    const bool counting = b.bins && key_bits <= COUNT_SORT_MAX_BITS;
+    uint32_t* const iota = counting ? nullptr : b.perm[0];   /* the radix sort's values */
     if (b.cell[cur])
-        k_sort_keys_cell<<<grid_for(n), 256, 0, s>>>(b.cell[cur], n, b.keys[0], b.perm[0]);
+        k_sort_keys_cell<<<grid_for(n), 256, 0, s>>>(b.cell[cur], n, b.keys[0], iota);
     else
         k_sort_keys<P><<<grid_for(n), 256, 0, s>>>(b.x[cur], b.y[cur], b.z[cur], n, mesh,
-                                                   morton ? 1 : 0, b.keys[0], b.perm[0]);
+                                                   morton ? 1 : 0, b.keys[0], iota);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    size_t bytes = b.temp_bytes;
-    e = cub::DeviceRadixSort::SortPairs(b.temp, bytes, b.keys[0], b.keys[1], b.perm[0],
-                                        b.perm[1], (int)n, 0, key_bits, s);
-    if (e != cudaSuccess) return e;
+    if (counting) {
+        const int64_t nbins = (int64_t)1 << key_bits;
+        if ((e = cudaMemsetAsync(b.bins, 0, nbins * sizeof(uint32_t), s)) != cudaSuccess) return e;
+        const int wg = grid_for(n);
+        k_bin_count<<<wg, 256, 0, s>>>(b.keys[0], n, (uint32_t)nbins, b.bins);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        size_t bytes = b.scan_temp_bytes;
+        e = cub::DeviceScan::ExclusiveSum(b.scan_temp, bytes, b.bins, b.offsets, (int)nbins, s);
+        if (e != cudaSuccess) return e;
+        k_bin_rank<<<wg, 256, 0, s>>>(b.keys[0], n, (uint32_t)nbins, b.offsets, b.perm[1]);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (launches) *launches += 2;
+    } else {
+        size_t bytes = b.temp_bytes;
+        e = cub::DeviceRadixSort::SortPairs(b.temp, bytes, b.keys[0], b.keys[1], b.perm[0],
+                                            b.perm[1], (int)n, 0, key_bits, s);
+        if (e != cudaSuccess) return e;
+    }
     int64_t gblocks = (n + 256 * GATHER_ILP - 1) / (256 * GATHER_ILP);
     if (gblocks > 148 * 64) gblocks = 148 * 64;
     k_gather<P, V><<<(int)gblocks, 256, 0, s>>>(b.perm[1], n, b.x[cur], b.y[cur], b.z[cur],

@@ -34,7 +34,8 @@ KERNEL_KINDS = {"step": 0, "finalize": 1, "sort": 2, "probe": 3, "other": 4,
 # every symbol include/scaletrack.h declares
 EXPORTS = [
     "st_version", "st_last_error", "st_params_default", "st_create", "st_destroy",
-    "st_set_parcels", "st_get_parcels", "st_get_cells", "st_num_parcels", "st_num_cells",
+    "st_set_parcels", "st_get_parcels", "st_get_cells", "st_get_order", "st_num_parcels",
+    "st_num_cells",
     "st_set_fluid_velocity", "st_set_fluid_velocity_device", "st_step", "st_get_source",
     "st_source_device", "st_synchronize", "st_get_stream", "st_set_stream",
     "st_profile_enable", "st_profile_read", "st_launch_count", "st_setup", "st_default_handle",
@@ -112,6 +113,7 @@ def lib():
         "st_get_parcels": ([c_h, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                             ctypes.c_void_p], ctypes.c_int),
         "st_get_cells": ([c_h, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+        "st_get_order": ([c_h, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
         "st_num_parcels": ([c_h, ctypes.c_int], ctypes.c_int64),
         "st_num_cells": ([c_h], ctypes.c_int64),
         "st_set_fluid_velocity": ([c_h, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
@@ -335,6 +337,12 @@ class ParcelTracker:
         if check:
             _check(rc)
         return cells
+
+    def get_order(self, cloud=0):
+        """ids[k]: st_set_parcels index of the parcel at device position k."""
+        ids = np.empty(self.num_parcels(cloud), dtype=np.int32)
+        _check(lib().st_get_order(self._h, cloud, _dptr(ids)))
+        return ids
 
     def set_fluid_velocity(self, U):
         U = np.ascontiguousarray(U)

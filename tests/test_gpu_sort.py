@@ -1,0 +1,97 @@
+"""GPU tests of the periodic re-sort through the C ABI: after the set-up sort and after a
+re-sort during stepping, the device-side order (st_get_order) is a permutation that groups
+parcels by owning cell in key order (the Morton code of the cell on cuboid meshes up to 1024
+cells per axis, the linear cell index on wider ones, the owning tet on tet meshes).  Key ranges
+up to 2^24 values use the counting sort, wider ones the radix sort; both are covered.  Results
+do not depend on the order (the parity tests compare runs with and without re-sorting)."""
+import numpy as np
+import pytest
+
+import scaletrack as st
+import workload
+
+pytestmark = pytest.mark.gpu
+
+L = workload.L_BOX
+
+
+def _params(**kw):
+    return st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                     drag_model="schiller_naumann", precision="mixed", n_substeps=1, **kw)
+
+
+def _check_grouped(order, keys_by_id):
+    n = keys_by_id.shape[0]
+    assert np.array_equal(np.sort(order), np.arange(n, dtype=np.int32))
+    k = keys_by_id[order]
+    assert np.all(k[1:] >= k[:-1])
+
+
+def _morton_keys(cells, nx, ny):
+    i = cells % nx
+    j = (cells // nx) % ny
+    k = cells // (nx * ny)
+    return workload._morton3(i, j, k)
+
+
+@pytest.mark.parametrize("n", [32, 48])
+def test_cuboid_resort_groups_parcels_by_morton_key(n):
+    """Counting sort: 32^3 (15-bit keys) and 48^3 (18-bit keys, a Morton range wider than the
+    mesh).  The carrier field is scaled by 10 so that many parcels change cell between sorts
+    while every step stays shorter than a cell (the reference's relocation assumes that)."""
+    m = 200000
+    xyz, uvw, d = workload.parcels(m, 11)
+    U = workload.tgv_field(n)
+    with st.ParcelTracker(_params(sort_interval=5), st.mesh_desc(n, 0.0, L)) as h:
+        h.set_parcels(xyz, uvw, d)
+        c0 = h.get_cells()
+        _check_grouped(h.get_order(), _morton_keys(c0, n, n))
+        h.set_fluid_velocity(U)
+        for s in range(5):                         # the re-sort runs after the fifth step
+            h.step(workload.DT, 10.0)
+        h.synchronize()
+        c1 = h.get_cells()
+        assert np.count_nonzero(c1 != c0) > m // 50
+        _check_grouped(h.get_order(), _morton_keys(c1, n, n))
+        for s in range(2):                         # moved on since: still a permutation
+            h.step(workload.DT, 10.0)
+        order = h.get_order()
+        assert np.array_equal(np.sort(order), np.arange(m, dtype=np.int32))
+
+
+def test_wide_mesh_uses_the_radix_sort_by_linear_cell():
+    """1100 x 1100 x 14 cells (more than 2^24, wider than 1024): linear cell keys through the
+    radix sort."""
+    dims = (1100, 1100, 14)
+    m = 100000
+    rng = np.random.default_rng(3)
+    xyz = rng.uniform(0.0, L, (3, m))
+    uvw = np.zeros((3, m))
+    d = np.full(m, 2e-5)
+    mesh = st.mesh_desc(dims, 0.0, L)
+    with st.ParcelTracker(_params(sort_interval=3), mesh) as h:
+        h.set_parcels(xyz, uvw, d)
+        _check_grouped(h.get_order(), h.get_cells().astype(np.int64))
+        h.set_fluid_velocity(np.zeros((int(np.prod(dims)), 3), np.float32))
+        for s in range(3):
+            h.step(workload.DT, 1.0)
+        h.synchronize()
+        _check_grouped(h.get_order(), h.get_cells().astype(np.int64))
+
+
+def test_tet_resort_groups_parcels_by_owning_tet():
+    n, m = 10, 60000
+    verts, tets, nbr, hex_ijk = workload.kuhn_tet_mesh(n, L, 0.15, 1)
+    xyz, _, d = workload.parcels(m, 4)
+    rng = np.random.default_rng(8)
+    uvw = rng.normal(0.0, 2.0, (3, m)).astype(np.float32).astype(np.float64)
+    U = workload.tgv_at(workload.tet_centroids(verts, tets), U0=3.0)
+    desc = st.tet_mesh_desc(verts, tets, nbr, 0.0, L)
+    with st.ParcelTracker(_params(sort_interval=4), desc) as h:
+        h.set_parcels(xyz, uvw, d, hint=workload.tet_hints(xyz, hex_ijk, n, L))
+        _check_grouped(h.get_order(), h.get_cells().astype(np.int64))
+        h.set_fluid_velocity(U)
+        for s in range(4):
+            h.step(workload.DT, 1.0)
+        h.synchronize()
+        _check_grouped(h.get_order(), h.get_cells().astype(np.int64))
