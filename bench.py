@@ -554,7 +554,7 @@ def run_clouds(st, torch, local, dev):
 def run_tets(st, torch, local, dev, steps, npcl=None):
     """Configuration 2: 96^3 hexes split into 6 jittered tets (5,308,416 tets), 2e7 parcels,
     carrier field U0 = 3 m/s at the tet centroids, Schiller-Naumann, one substep, mixed
-    precision, greedy face walk after every position update, re-sort by owning tet every 20
+    precision, greedy face walk after every position update, re-sort by owning tet every 10
     steps."""
     c = workload.CONFIGS["c2_tets_96"]
     n, dt = c["n"], workload.DT
@@ -612,7 +612,7 @@ def run_tets(st, torch, local, dev, steps, npcl=None):
     walks = float(hops.sum())
     return {"workload": "BASELINE config 2: 96^3 x 6 jittered tets (5,308,416), 2e7 parcels, "
                         "U0 = 3 m/s, Schiller-Naumann, dt = 1e-4 s, 1 substep, mixed precision, "
-                        "face walk, re-sort by owning tet every 20 steps",
+                        "face walk, re-sort by owning tet every %d steps" % c["sort_interval"],
             "parcels": npcl, "tets": int(tets.shape[0]), "steps": steps,
             "particle_steps_per_s": npcl * steps / (ms / 1e3), "ms_per_step": ms / steps,
             "kernel_ms": {"step": round(step_avg, 5),

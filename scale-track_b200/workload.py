@@ -38,7 +38,7 @@ CONFIGS = {
     # 96^3 hexes x 6 tets, vertices jittered +-0.15 h (seed 1), 2e7 parcels, U0 = 3 m/s,
     # mixed precision, 200 steps, face-walk relocation
     "c2_tets_96": dict(n=96, nparcels=20_000_000, seed=0, mesh_seed=1, jitter=0.15,
-                       precision="mixed", steps=200, U0=3.0, sort_interval=20),
+                       precision="mixed", steps=200, U0=3.0, sort_interval=10),
     # adjoint: 128^3 hex, 1e6 parcels, 200 steps, checkpoints every 20 steps; the target
     # source comes from a forward run with drag multiplier 1.1 and diameters x 0.95
     "c4_adjoint_128": dict(n=128, nparcels=1_000_000, seed=3, precision="mixed", steps=200,
