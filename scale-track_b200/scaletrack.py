@@ -202,8 +202,10 @@ def tet_mesh_desc(vertices, tets, neighbors, origin, ending, hop_limit=0):
     verts = np.ascontiguousarray(vertices, dtype=np.float64)
     tt = np.ascontiguousarray(tets, dtype=np.int32)
     nb = np.ascontiguousarray(neighbors, dtype=np.int32)
-    assert verts.ndim == 2 and verts.shape[1] == 3
-    assert tt.shape == nb.shape and tt.ndim == 2 and tt.shape[1] == 4
+    if verts.ndim != 2 or verts.shape[1] != 3:
+        raise ValueError("vertices must be [nv][3]")
+    if tt.shape != nb.shape or tt.ndim != 2 or tt.shape[1] != 4:
+        raise ValueError("tets and neighbors must both be [nt][4]")
     m = TetMeshDesc()
     m.n_vertices = verts.shape[0]
     m.vertices = verts.ctypes.data
@@ -233,6 +235,12 @@ def params(**kw):
             raise TypeError(f"unknown parameter {k}")
         setattr(p, k, v)
     return p
+
+
+def _check_parcel_shapes(xyz, uvw, n):
+    if xyz.shape != (3, n) or uvw.shape != (3, n):
+        raise ValueError(f"xyz and uvw must be [3][{n}] (one column per parcel), got "
+                         f"{xyz.shape} and {uvw.shape}")
 
 
 def _dptr(a):
@@ -278,14 +286,16 @@ class ParcelTracker:
         uvw = np.ascontiguousarray(uvw, dtype=np.float64)
         d = np.ascontiguousarray(d, dtype=np.float64)
         n = d.shape[0]
-        assert xyz.shape == (3, n) and uvw.shape == (3, n)
+        _check_parcel_shapes(xyz, uvw, n)
         if self.tet:
             h = None if hint is None else np.ascontiguousarray(hint, dtype=np.int32)
-            assert h is None or h.shape == (n,)
+            if h is not None and h.shape != (n,):
+                raise ValueError("hint must hold one starting tet per parcel")
             _check(lib().st_set_parcels_tet(self._h, cloud, n, _dptr(xyz), _dptr(uvw),
                                             _dptr(d), _dptr(h)))
         else:
-            assert hint is None, "hint is for tet meshes"
+            if hint is not None:
+                raise ValueError("hint is for tet meshes")
             _check(lib().st_set_parcels(self._h, cloud, n, _dptr(xyz), _dptr(uvw), _dptr(d)))
 
     def hop_histogram(self, reset=False):
@@ -300,7 +310,7 @@ class ParcelTracker:
         uvw = np.ascontiguousarray(uvw, dtype=np.float64)
         d = np.ascontiguousarray(d, dtype=np.float64)
         m = d.shape[0]
-        assert xyz.shape == (3, m) and uvw.shape == (3, m)
+        _check_parcel_shapes(xyz, uvw, m)
         _check(lib().st_append_parcels(self._h, cloud, m, _dptr(xyz), _dptr(uvw), _dptr(d)))
 
     def init_parcels(self, n, seed, d_min, d_max, cloud=0):
@@ -318,7 +328,10 @@ class ParcelTracker:
         _check(lib().st_load_state(self._h, os.fsencode(path)))
 
     def num_parcels(self, cloud=0):
-        return int(lib().st_num_parcels(self._h, cloud))
+        n = int(lib().st_num_parcels(self._h, cloud))
+        if n < 0:
+            raise ScaleTrackError(ST_ERR_INVALID_ARGUMENT, f"cloud {cloud} out of range")
+        return n
 
     def get_parcels(self, cloud=0, check=True):
         n = self.num_parcels(cloud)
@@ -346,7 +359,9 @@ class ParcelTracker:
 
     def set_fluid_velocity(self, U):
         U = np.ascontiguousarray(U)
-        assert U.shape == (self.ncells, 3) and U.dtype in (np.float32, np.float64)
+        if U.shape != (self.ncells, 3) or U.dtype not in (np.float32, np.float64):
+            raise ValueError(f"U must be float32 or float64 [{self.ncells}][3], got "
+                             f"{U.dtype} {U.shape}")
         _check(lib().st_set_fluid_velocity(self._h, _dptr(U), U.dtype.itemsize))
 
     def set_fluid_velocity_device(self, ptr, elem_bytes):
@@ -405,7 +420,8 @@ class ParcelTracker:
         fs = None
         if fluid_scale is not None:
             fs = np.ascontiguousarray(fluid_scale, dtype=np.float64)
-            assert fs.shape == (n_steps,)
+            if fs.shape != (n_steps,):
+                raise ValueError("fluid_scale must hold one factor per step")
         desc = AdjointDesc(n_steps, checkpoint_interval, dt,
                            None if fs is None else fs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         return desc, fs

@@ -107,3 +107,15 @@ def test_exchange_mode_is_validated():
     assert st.lib().st_set_exchange_mode(7) == st.ST_ERR_INVALID_ARGUMENT
     assert "exchange mode" in st.last_error()
     st.set_exchange_mode("copy")
+
+
+def test_host_wrapper_rejects_malformed_tet_meshes():
+    """Shape errors are raised by the Python host before anything reaches the library."""
+    v = np.zeros((5, 3))
+    t = np.zeros((2, 4), np.int32)
+    with pytest.raises(ValueError):
+        st.tet_mesh_desc(np.zeros((5, 2)), t, t, 0.0, 1.0)
+    with pytest.raises(ValueError):
+        st.tet_mesh_desc(v, t, np.zeros((3, 4), np.int32), 0.0, 1.0)
+    d = st.tet_mesh_desc(v, t, t, 0.0, 1.0)
+    assert d.n_vertices == 5 and d.n_tets == 2
