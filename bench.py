@@ -394,7 +394,8 @@ def run_ours(args):
             t = torch.tensor([el], device=dev, dtype=torch.float64)
             pg.all_reduce(t, op=pg.ReduceOp.MAX)
             el = float(t.item())
-        assert np.isfinite(UT).all()
+        if not np.isfinite(UT).all():
+            raise RuntimeError("non-finite source from the coupling shim")
         st.finalize()
         e2e = {"value": ws * npcl * args.e2e_steps / el, "unit": UNIT,
                "h2d_bytes_per_step": ncells * 3 * 4, "d2h_bytes_per_step": ncells * 3 * 4,
@@ -419,7 +420,8 @@ def run_ours(args):
         for j in range(args.e2e_steps):
             st.evolve_cloud(dt)
         el = time.perf_counter() - t0
-        assert np.isfinite(UT).all()
+        if not np.isfinite(UT).all():
+            raise RuntimeError("non-finite source from the coupling shim")
         st.finalize()
         extras["e2e_mapped"] = {
             "value": npcl * args.e2e_steps / el, "unit": UNIT,
@@ -443,7 +445,8 @@ def run_ours(args):
         for j in range(args.e2e_steps):
             st.evolve_cloud_async(dt)
         el = time.perf_counter() - t0
-        assert np.isfinite(UT).all()
+        if not np.isfinite(UT).all():
+            raise RuntimeError("non-finite source from the coupling shim")
         st.finalize()
         extras["e2e_async"] = {
             "value": npcl * args.e2e_steps / el, "unit": UNIT,
