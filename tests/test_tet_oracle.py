@@ -71,6 +71,25 @@ def test_oracle_walk_finds_containing_tet():
     assert lam0.min() >= -1e-9
 
 
+def test_walk_on_unjittered_hexes_agrees_with_floor_locate():
+    """Known answer: on a uniform hex mesh split into tets (no jitter) the owning tet found by
+    the face walk lies in the hex that floor-locate gives, for positions off the faces."""
+    n = 7
+    verts, tets, nbr, hex_ijk = _mesh(n, jitter=0.0)
+    rng = np.random.default_rng(12)
+    m = 20000
+    x = rng.random((3, m)) * L
+    h = L / n
+    ijk = np.floor(x / h).astype(np.int64)
+    frac = x / h - ijk
+    off_faces = ((frac > 1e-9) & (frac < 1 - 1e-9)).all(axis=0)
+    cells, status = oracle.tet_locate((verts, tets, nbr), x, np.zeros(m, np.int32), 4096)
+    assert (status == 0).all()
+    found = hex_ijk[cells // 6].T                  # (i, j, k) of the hex of each owning tet
+    assert off_faces.sum() > 0.99 * m
+    assert np.array_equal(found[:, off_faces], ijk[:, off_faces])
+
+
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_tet_step_matches_cuboid_step_in_uniform_flow(precision):
     """Uniform U: positions, velocities and the total fixed-point source of the tet step must
