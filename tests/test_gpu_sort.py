@@ -16,8 +16,9 @@ L = workload.L_BOX
 
 
 def _params(**kw):
+    kw.setdefault("precision", "mixed")
     return st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
-                     drag_model="schiller_naumann", precision="mixed", n_substeps=1, **kw)
+                     drag_model="schiller_naumann", n_substeps=1, **kw)
 
 
 def _check_grouped(order, keys_by_id):
@@ -34,15 +35,18 @@ def _morton_keys(cells, nx, ny):
     return workload._morton3(i, j, k)
 
 
-@pytest.mark.parametrize("n", [32, 48])
-def test_cuboid_resort_groups_parcels_by_morton_key(n):
+@pytest.mark.parametrize("n,prec", [(32, "mixed"), (48, "mixed"), (32, "fp32"), (32, "fp64")])
+def test_cuboid_resort_groups_parcels_by_morton_key(n, prec):
     """Counting sort: 32^3 (15-bit keys) and 48^3 (18-bit keys, a Morton range wider than the
     mesh).  The carrier field is scaled by 10 so that many parcels change cell between sorts
     while every step stays shorter than a cell (the reference's relocation assumes that)."""
     m = 200000
     xyz, uvw, d = workload.parcels(m, 11)
     U = workload.tgv_field(n)
-    with st.ParcelTracker(_params(sort_interval=5), st.mesh_desc(n, 0.0, L)) as h:
+    if prec == "fp64":
+        U = U.astype(np.float64)
+    with st.ParcelTracker(_params(sort_interval=5, precision=prec),
+                          st.mesh_desc(n, 0.0, L)) as h:
         h.set_parcels(xyz, uvw, d)
         c0 = h.get_cells()
         _check_grouped(h.get_order(), _morton_keys(c0, n, n))
