@@ -1,6 +1,6 @@
 """Benchmark of the B200 Lagrangian parcel step (one JSON line on stdout, rank 0).
 
-Workload (BASELINE configuration 1): 128^3 uniform hex mesh (2,097,152 cells) on
+Workload: 128^3 uniform hex mesh (2,097,152 cells) on
 [0, 0.1 m]^3, 1e7 parcels, Schiller-Naumann drag with explicit Euler, dt = 1e-4 s, one
 substep, mixed precision (FP64 positions, FP32 drag/velocity, deterministic fixed-point
 source reduced to FP64), Morton re-sort every 20 steps, time-varying Taylor-Green-like
@@ -44,7 +44,7 @@ import workload  # noqa: E402
 
 METRIC = "particle-steps/s mixed vs FP64 on 1 B200 at src rel err<=1e-5; adjoint/fwd cost"
 UNIT = "particle-steps/s"
-CONFIG = workload.CONFIGS["c1_mixed_128"]
+CONFIG = workload.CONFIGS["hex128_mixed"]
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -64,11 +64,11 @@ def parse():
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the configuration-4 adjoint timing")
     ap.add_argument("--no-tets", dest="tets", action="store_false",
-                    help="skip configuration 2 (tet mesh)")
-    ap.add_argument("--tet-steps", type=int, default=workload.CONFIGS["c2_tets_96"]["steps"])
-    ap.add_argument("--tet-nparcels", type=int, default=workload.CONFIGS["c2_tets_96"]["nparcels"])
+                    help="skip the 96^3 x 6 jittered tet mesh workload")
+    ap.add_argument("--tet-steps", type=int, default=workload.CONFIGS["tets96x6_mixed"]["steps"])
+    ap.add_argument("--tet-nparcels", type=int, default=workload.CONFIGS["tets96x6_mixed"]["nparcels"])
     ap.add_argument("--tets-only", action="store_true",
-                    help="time configuration 2 alone and print its object (profiling runs)")
+                    help="time the tet mesh workload alone and print its object (profiling runs)")
     ap.add_argument("--no-clouds", dest="clouds", action="store_false",
                     help="skip the configuration-3 multi-cloud timing")
     return ap.parse_args()
@@ -455,15 +455,15 @@ def run_ours(args):
             "path": "st_evolve_cloud_async (the reference's default coupling): U H2D and the "
                     "extrapolated source D2H on a copy stream, overlapping the previous step"}
 
-    # ---- 64 clouds in one launch, graph replay, autotuned (BASELINE configuration 3) ----
+    # ---- 64 clouds in one launch, graph replay, autotuned ----
     if not args.no_extras and solo and args.clouds:
         extras["clouds"] = run_clouds(st, torch, local, dev)
 
-    # ---- face walk on the jittered tet mesh ----
+    # ---- face walk on the jittered 96^3 x 6 tet mesh ----
     if not args.no_extras and solo and args.tets:
         extras["tets"] = run_tets(st, torch, local, dev, args.tet_steps, args.tet_nparcels)
 
-    # ---- adjoint of the time-averaged source ----
+    # ---- adjoint of the time-averaged source (128^3 hex, 1e6 parcels) ----
     if not args.no_extras and solo and args.adjoint:
         extras["adjoint"] = run_adjoint(st, local)
 
@@ -486,7 +486,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 positions / f32 drag+velocity "
         "/ int64 fixed-point source -> f64",
         "data": "synthetic (seeded uniform parcels, lognormal diameters, analytic TGV field)",
-        "config": {"workload": "BASELINE config 1: 128^3 hex (2,097,152 cells), 1e7 parcels "
+        "config": {"workload": "128^3 hex (2,097,152 cells), 1e7 parcels "
                                "per GPU, Schiller-Naumann explicit, dt=1e-4 s, 1 substep, "
                                "mixed precision, Morton re-sort every 20 steps, "
                                "time-varying field",
@@ -502,10 +502,10 @@ def run_ours(args):
 
 
 def run_clouds(st, torch, local, dev):
-    """Configuration 3: 64 clouds with log-uniform sizes on a 64^3 mesh, each with its own
+    """64 clouds with log-uniform sizes on a 64^3 mesh, each with its own
     source, one persistent launch per step; block size and re-sort interval from the
     autotuner; the step sequence replayed from a captured CUDA graph."""
-    c = workload.CONFIGS["c3_clouds_64"]
+    c = workload.CONFIGS["clouds64_hex64"]
     sizes, dmed = workload.cloud_sizes(c)
     n = c["n"]
     U = workload.tgv_field(n, dtype=np.float32)
@@ -544,7 +544,7 @@ def run_clouds(st, torch, local, dev):
             h.graph_launch()
         ms_graph = timer.stop()
         h.synchronize()
-    return {"workload": "BASELINE config 3: 64 clouds, sizes log-uniform in [1e3, 2e6] (seed 2), "
+    return {"workload": "64 clouds, sizes log-uniform in [1e3, 2e6] (seed 2), "
                         "median diameter per cloud uniform in [5, 50] um, 64^3 mesh, one "
                         "source per cloud, mixed precision, 10 substeps inside one launch per "
                         "step",
@@ -555,11 +555,11 @@ def run_clouds(st, torch, local, dev):
 
 
 def run_tets(st, torch, local, dev, steps, npcl=None):
-    """Configuration 2: 96^3 hexes split into 6 jittered tets (5,308,416 tets), 2e7 parcels,
+    """96^3 hexes split into 6 jittered tets (5,308,416 tets), 2e7 parcels,
     carrier field U0 = 3 m/s at the tet centroids, Schiller-Naumann, one substep, mixed
     precision, greedy face walk after every position update, re-sort by owning tet every 10
     steps."""
-    c = workload.CONFIGS["c2_tets_96"]
+    c = workload.CONFIGS["tets96x6_mixed"]
     n, dt = c["n"], workload.DT
     npcl = npcl or c["nparcels"]
     verts, tets, nbr, hex_ijk = workload.kuhn_tet_mesh(n, workload.L_BOX, c["jitter"],
@@ -613,7 +613,7 @@ def run_tets(st, torch, local, dev, steps, npcl=None):
     step_avg = step_ms / max(nstep, 1)
     algo = workload.tet_step_kernel_bytes(c["precision"], npcl, tets.shape[0])
     walks = float(hops.sum())
-    return {"workload": "BASELINE config 2: 96^3 x 6 jittered tets (5,308,416), 2e7 parcels, "
+    return {"workload": "96^3 x 6 jittered tets (5,308,416), 2e7 parcels, "
                         "U0 = 3 m/s, Schiller-Naumann, dt = 1e-4 s, 1 substep, mixed precision, "
                         "face walk, re-sort by owning tet every %d steps" % c["sort_interval"],
             "parcels": npcl, "tets": int(tets.shape[0]), "steps": steps,
@@ -632,9 +632,9 @@ def run_tets(st, torch, local, dev, steps, npcl=None):
 
 
 def run_adjoint(st, device):
-    """Forward (objective) and pull-back (gradient) times of configuration 4: J = |Sbar -
+    """Forward (objective) and pull-back (gradient) times of the adjoint workload: J = |Sbar -
     S*|^2 over 200 steps, 1e6 parcels, 128^3 cells, checkpoints every 20 steps."""
-    c = workload.CONFIGS["c4_adjoint_128"]
+    c = workload.CONFIGS["adjoint_hex128"]
     n, npcl, T, C = c["n"], c["nparcels"], c["steps"], c["checkpoint"]
     xyz, uvw, d = workload.parcels(npcl, c["seed"])
     U = workload.tgv_field(n, dtype=np.float32)
@@ -667,7 +667,7 @@ def run_adjoint(st, device):
         h.profile(False)
     fwd = fwd_ms / reps
     bwd = bwd_ms / reps
-    return {"workload": "BASELINE config 4: 128^3 hex, 1e6 parcels, 200 steps, checkpoints every "
+    return {"workload": "adjoint, 128^3 hex, 1e6 parcels, 200 steps, checkpoints every "
                         "20 steps, mixed precision, J = |mean source - target|^2, target from "
                         "drag x1.1 and diameters x0.95",
             "forward_ms": round(fwd, 3), "pullback_ms": round(bwd, 3),
@@ -747,7 +747,7 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 positions / f32 drag+velocity",
         "data": "synthetic (seeded uniform parcels, lognormal diameters, analytic TGV field)",
-        "config": {"workload": "BASELINE config 1 on the host CPU: 128^3 hex, Schiller-Naumann "
+        "config": {"workload": "the 128^3 hex, 1e7-parcel step on the host CPU: 128^3 hex, Schiller-Naumann "
                                "explicit, dt=1e-4 s, mixed precision; bounded parcel sample",
                    "nparcels_sampled": sample, "ncells": n ** 3},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",

@@ -283,7 +283,7 @@ struct ProfScope {
 };
 
 /* Blocks per cloud of the finalize pass: four 256-thread blocks per SM over all clouds
- * (measured on configuration 1: 23 us against 28 us with eight), each thread looping over
+ * (measured at 128^3 cells: 23 us against 28 us with eight), each thread looping over
  * groups of four components. */
 int finalize_grid(const st_handle* h)
 {

@@ -1,6 +1,6 @@
 /*
  * st_tet.cu -- the parcel step on unstructured tetrahedral meshes with face-walk
- * relocation (configuration 2: 96^3 jittered hexes split into 6 tets; no counterpart in the
+ * relocation (the benchmark mesh: 96^3 jittered hexes split into 6 tets; no counterpart in the
  * reference, whose cuboid mesh is located by floor, A:663-697).
  *
  * Each parcel carries its owning tet.  After the drag update and the position update, a new

@@ -23,25 +23,25 @@ L_BOX = 0.1
 
 CONFIGS = {
     # 32^3 hex, 1e5 parcels, FP64, 100 steps (the CPU-runnable case)
-    "c0_fp64_32": dict(n=32, nparcels=100_000, seed=0, precision="fp64", steps=100,
+    "hex32_fp64": dict(n=32, nparcels=100_000, seed=0, precision="fp64", steps=100,
                        U0=1.0, time_varying=False, sort_interval=0),
     # 128^3 hex, 1e7 parcels, mixed precision, 500 steps, Morton re-sort every 20 steps,
     # time-varying field
-    "c1_mixed_128": dict(n=128, nparcels=10_000_000, seed=0, precision="mixed", steps=500,
+    "hex128_mixed": dict(n=128, nparcels=10_000_000, seed=0, precision="mixed", steps=500,
                          U0=1.0, time_varying=True, sort_interval=20),
     # 64 clouds, sizes log-uniform in [1e3, 2e6] (seed 2), per-cloud median diameter uniform
     # in [5, 50] um, one shared 64^3 mesh, own source per cloud, 100 steps.  Ten substeps of
     # dt/10 (the reference's nSteps): a 2 um parcel has tau_p ~ 1.2e-5 s, and explicit Euler
     # needs dt_sub / tau_p < 2
-    "c3_clouds_64": dict(n=64, nclouds=64, seed=2, precision="mixed", steps=100, substeps=10,
-                         size_min=1_000, size_max=2_000_000, dmed_min=5e-6, dmed_max=50e-6),
+    "clouds64_hex64": dict(n=64, nclouds=64, seed=2, precision="mixed", steps=100, substeps=10,
+                           size_min=1_000, size_max=2_000_000, dmed_min=5e-6, dmed_max=50e-6),
     # 96^3 hexes x 6 tets, vertices jittered +-0.15 h (seed 1), 2e7 parcels, U0 = 3 m/s,
     # mixed precision, 200 steps, face-walk relocation
-    "c2_tets_96": dict(n=96, nparcels=20_000_000, seed=0, mesh_seed=1, jitter=0.15,
-                       precision="mixed", steps=200, U0=3.0, sort_interval=10),
+    "tets96x6_mixed": dict(n=96, nparcels=20_000_000, seed=0, mesh_seed=1, jitter=0.15,
+                           precision="mixed", steps=200, U0=3.0, sort_interval=10),
     # adjoint: 128^3 hex, 1e6 parcels, 200 steps, checkpoints every 20 steps; the target
     # source comes from a forward run with drag multiplier 1.1 and diameters x 0.95
-    "c4_adjoint_128": dict(n=128, nparcels=1_000_000, seed=3, precision="mixed", steps=200,
+    "adjoint_hex128": dict(n=128, nparcels=1_000_000, seed=3, precision="mixed", steps=200,
                            checkpoint=20, U0=1.0, time_varying=False, target_alpha=1.1,
                            target_dscale=0.95),
 }

@@ -1,4 +1,5 @@
-"""GPU tests of the adjoint of the time-averaged source (configuration 4's method).
+"""GPU tests of the adjoint of the time-averaged source (the method of the 128^3, 1e6-parcel
+adjoint benchmark).
 
 The pull-back is checked (a) against the CPU adjoint of the same precision mode: the mean
 source and the per-parcel velocity cotangents bit for bit, the parameter gradients to FP64

@@ -1,4 +1,4 @@
-"""GPU tests of the multi-cloud path of configuration 3: one launch for all clouds, CUDA-graph
+"""GPU tests of the multi-cloud path (64 clouds of log-uniform sizes in the benchmark): one launch for all clouds, CUDA-graph
 replay of a step sequence and the autotuner.  Replays must give the same bits as st_step
 calls, and tuning must not change results (parcel order never changes a parcel's state or
 the fixed-point source)."""
@@ -15,7 +15,7 @@ N = 16
 
 
 def clouds(k=5, seed=2):
-    cfg = dict(workload.CONFIGS["c3_clouds_64"], nclouds=k, size_min=50, size_max=20000,
+    cfg = dict(workload.CONFIGS["clouds64_hex64"], nclouds=k, size_min=50, size_max=20000,
                seed=seed)
     sizes, dmed = workload.cloud_sizes(cfg)
     out = []

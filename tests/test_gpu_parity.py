@@ -317,12 +317,12 @@ def test_profile_counters_and_launch_count():
 
 
 @pytest.mark.slow
-def test_configuration_0_fp64_full_run():
+def test_hex32_fp64_1e5_parcels_100_steps_full_run():
     """The CPU-runnable configuration in full: 32^3 cells, 1e5 parcels, FP64, 100 steps of
     Schiller-Naumann drag with a frozen field.  Positions, velocities and cells bit-exact with
     the FP64 oracle after 100 steps; the two-limb source bit-exact with its fixed-point model
     and within 1e-14 of the FP64 sum of the same deposits."""
-    c = workload.CONFIGS["c0_fp64_32"]
+    c = workload.CONFIGS["hex32_fp64"]
     n, nparcels, steps = c["n"], c["nparcels"], c["steps"]
     xyz, uvw, d = workload.parcels(nparcels, c["seed"], dtype_v=np.float64)
     U = workload.tgv_field(n, U0=c["U0"], dtype=np.float64)
@@ -336,9 +336,9 @@ def test_configuration_0_fp64_full_run():
 
 @pytest.mark.slow
 def test_full_size_mixed_against_oracle():
-    """BASELINE configuration 1 sizes (128^3 cells, 1e7 parcels), a few steps: bit-exact
+    """The benchmark sizes (128^3 cells, 1e7 parcels), a few steps: bit-exact
     state and cells and fixed-point source against the (multi-threaded) oracle."""
-    cfgd = workload.CONFIGS["c1_mixed_128"]
+    cfgd = workload.CONFIGS["hex128_mixed"]
     n, nparcels = cfgd["n"], cfgd["nparcels"]
     xyz, uvw, d, U = bench_inputs(nparcels, n, cfgd["seed"], "mixed")
     fs = [workload.fluid_scale(s) for s in range(3)]

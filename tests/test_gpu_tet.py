@@ -154,7 +154,7 @@ def test_tet_graph_replay_equals_steps():
 @pytest.mark.slow
 def test_tet_full_mesh_subsample():
     """The 96^3 x 6 jittered mesh with U0 = 3 at the benchmark's time step, 1e6 parcels."""
-    cfg = workload.CONFIGS["c2_tets_96"]
+    cfg = workload.CONFIGS["tets96x6_mixed"]
     n, m = cfg["n"], 1_000_000
     mesh, xyz, uvw, d, U, hint = _setup(n, m, cfg["seed"], 0.0, 20e-6, U0=cfg["U0"])
     prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
