@@ -99,3 +99,23 @@ def test_tet_resort_groups_parcels_by_owning_tet():
             h.step(workload.DT, 1.0)
         h.synchronize()
         _check_grouped(h.get_order(), h.get_cells().astype(np.int64))
+
+
+def test_ragged_clouds_share_the_bins():
+    """Several clouds of ragged sizes (partial warps, a cloud of two) sorted one after the
+    other with the handle's shared counting bins: each cloud's order groups its own parcels."""
+    n = 16
+    sizes = [2, 33, 1000, 5]
+    prm = _params(n_clouds=len(sizes), sort_interval=3)
+    with st.ParcelTracker(prm, st.mesh_desc(n, 0.0, L)) as h:
+        for c, m in enumerate(sizes):
+            xyz, uvw, d = workload.parcels(m, 40 + c)
+            h.set_parcels(xyz, uvw, d, cloud=c)
+        for c in range(len(sizes)):
+            _check_grouped(h.get_order(c), _morton_keys(h.get_cells(c), n, n))
+        h.set_fluid_velocity(workload.tgv_field(n))
+        for s in range(3):
+            h.step(workload.DT, 10.0)
+        h.synchronize()
+        for c in range(len(sizes)):
+            _check_grouped(h.get_order(c), _morton_keys(h.get_cells(c), n, n))
