@@ -242,35 +242,12 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     extras = {}
-    # ---- accuracy: mixed vs all-FP64 on the same inputs (source of the last step) ----
+    # ---- accuracy: mixed vs all-FP64 on the same inputs ----
     # single-GPU extras run on one rank only when the job has one rank: with several ranks
     # the others would wait in a collective for minutes
     solo = ws == 1
     if not args.no_extras and solo:
-        S = {}
-        for prec, dep in (("mixed", "deterministic"), ("fp64", "deterministic")):
-            with st.ParcelTracker(make_params(st, prec, dep), mesh, device=local) as h:
-                h.set_parcels(xyz, uvw, d)
-                h.set_fluid_velocity(U.astype(np.float64 if prec == "fp64" else np.float32))
-                for k in range(args.accuracy_steps):
-                    h.step(dt, fs(k))
-                h.synchronize()
-                S[prec] = h.get_source()
-                if prec == "mixed":
-                    cells_m = h.get_cells()
-                    pos_m = h.get_parcels()[0]
-                else:
-                    cells_d = h.get_cells()
-                    pos_d = h.get_parcels()[0]
-        ref = S["fp64"]
-        extras["src_rel_err_mixed_vs_fp64"] = float(np.abs(S["mixed"] - ref).max() /
-                                                    np.abs(ref).max())
-        extras["src_rel_err_l2_mixed_vs_fp64"] = float(np.linalg.norm(S["mixed"] - ref) /
-                                                       np.linalg.norm(ref))
-        extras["pos_rel_err_mixed_vs_fp64"] = float(np.abs(pos_m - pos_d).max() /
-                                                    workload.L_BOX)
-        extras["cells_differing_mixed_vs_fp64"] = int(np.sum(cells_m != cells_d))
-        extras["accuracy_steps"] = args.accuracy_steps
+        extras.update(accuracy(st, xyz, uvw, d, U, mesh, local, args.accuracy_steps, dt, fs))
 
     # ---- headline: mixed deterministic step, device-resident ----
     h = st.ParcelTracker(make_params(st, "mixed"), mesh, device=local)
@@ -499,6 +476,60 @@ def run_ours(args):
     }
     line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+def source_errors(Sm, Sd):
+    """Source of the mixed step against the FP64 step's source S: max-norm and L2 relative to
+    S, and the per-cell relative error over the cells with |S_c| >= 1e-3 max |S|."""
+    mx = np.abs(Sd).max()
+    err = np.abs(Sm - Sd)
+    sel = np.abs(Sd) >= 1e-3 * mx
+    rel = err[sel] / np.abs(Sd[sel])
+    return {"max_norm": float(err.max() / mx),
+            "l2": float(np.linalg.norm(Sm - Sd) / np.linalg.norm(Sd)),
+            "per_cell_p99": float(np.percentile(rel, 99)),
+            "per_cell_max": float(rel.max()),
+            "per_cell_cells": int(sel.sum())}
+
+
+def accuracy(st, xyz, uvw, d, U, mesh, local, steps, dt, fs):
+    """Mixed against all-FP64 at the benchmark's size: (a) `steps` steps of both from the
+    same inputs (arithmetic plus trajectory divergence), (b) one step of both from the mixed
+    run's state after `steps` steps (the arithmetic alone, on relaxed parcels)."""
+    out = {}
+    S, state = {}, {}
+    for prec in ("mixed", "fp64"):
+        with st.ParcelTracker(make_params(st, prec), mesh, device=local) as h:
+            h.set_parcels(xyz, uvw, d)
+            h.set_fluid_velocity(U.astype(np.float64 if prec == "fp64" else np.float32))
+            for k in range(steps):
+                h.step(dt, fs(k))
+            h.synchronize()
+            S[prec] = h.get_source()
+            state[prec] = (h.get_parcels(), h.get_cells())
+    (pm, _, _), cm = state["mixed"]
+    (pd, _, _), cd = state["fp64"]
+    e = source_errors(S["mixed"], S["fp64"])
+    out["src_rel_err_mixed_vs_fp64"] = e["max_norm"]
+    out["src_rel_err_l2_mixed_vs_fp64"] = e["l2"]
+    out["pos_rel_err_mixed_vs_fp64"] = float(np.abs(pm - pd).max() / workload.L_BOX)
+    out["cells_differing_mixed_vs_fp64"] = int(np.sum(cm != cd))
+    out["accuracy_steps"] = steps
+    out["src_err_after_steps"] = dict(e, steps=steps, start="same inputs")
+    x1, u1, _ = state["mixed"][0]
+    S1, c1 = {}, {}
+    for prec in ("mixed", "fp64"):
+        with st.ParcelTracker(make_params(st, prec), mesh, device=local) as h:
+            h.set_parcels(x1, u1, d)
+            h.set_fluid_velocity(U.astype(np.float64 if prec == "fp64" else np.float32))
+            h.step(dt, fs(steps))
+            h.synchronize()
+            S1[prec] = h.get_source()
+            c1[prec] = h.get_cells()
+    out["src_err_one_step"] = dict(source_errors(S1["mixed"], S1["fp64"]),
+                                   start="mixed state after %d steps, one step of each" % steps,
+                                   cells_differing=int(np.sum(c1["mixed"] != c1["fp64"])))
+    return out
 
 
 def run_clouds(st, torch, local, dev):

@@ -223,6 +223,15 @@ typedef struct st_tune_result {
  * changes positions, velocities or the fixed-point source. */
 ST_API int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out);
 
+/* Step kernel of a handle with one cloud.  ST_STEP_KERNEL_RING (the default): a persistent
+ * block per SM streams block tiles of 1024 parcels through a shared-memory ring with bulk
+ * copies.  ST_STEP_KERNEL_WARP: every warp loads and steps its own 32 parcels.  Both give
+ * bit-identical positions, velocities, cells and sources; handles with several clouds, and
+ * the first (probe) pass of a run, always use the warp kernel.  No counterpart in the
+ * reference (one kernel, A:1258-1269). */
+enum { ST_STEP_KERNEL_RING = 0, ST_STEP_KERNEL_WARP = 1 };
+ST_API int st_set_step_kernel(st_handle* h, int kind);
+
 /* ---- instrumentation --------------------------------------------------------------- */
 enum { ST_KERNEL_STEP = 0, ST_KERNEL_FINALIZE = 1, ST_KERNEL_SORT = 2, ST_KERNEL_PROBE = 3,
        ST_KERNEL_OTHER = 4, ST_KERNEL_ADJ_FORWARD = 5, ST_KERNEL_ADJ_REVERSE = 6,
@@ -259,6 +268,34 @@ ST_API int st_mean_source_forward(st_handle* h, int cloud, const st_adjoint_desc
 ST_API int st_mean_source_pullback(st_handle* h, int cloud, const st_adjoint_desc* desc,
                                    const double* cotangent, double* d_drag_multiplier,
                                    double* d_diameter_scale, double* d_velocity0);
+
+/* Sets the drag multiplier and the diameter scale of an existing handle (the st_params
+ * fields of the same names), so that the parameters of the adjoint above can be arguments of
+ * the differentiated function.  Takes effect at the next step or forward pass; invalidates
+ * the last st_mean_source_forward.  Both must be finite and > 0. */
+ST_API int st_set_drag_parameters(st_handle* h, double drag_multiplier, double diameter_scale);
+
+/* ---- sharded steps: one cloud split over ranks (one handle per rank or GPU) ---------- */
+/* The reference sums the per-rank sources over MPI (asyncParallelTracking.jl:1156-1183);
+ * here the ranks combine the fixed-point accumulators before they are converted, so the
+ * source is bit-identical to one handle stepping every parcel, for any split and any
+ * reduction order (integer sums are exact).  Per step, on every rank:
+ *   if st_shard_needs_probe(h, dt):  st_shard_probe(h, dt, fs); max-reduce the exponents
+ *   st_shard_deposit(h, dt, fs);     sum-reduce the accumulators, max-reduce the exponents
+ *   st_shard_finish(h);              the source (identical on every rank), next scale
+ * The reductions act on the device buffers of st_shard_buffers (int64 accumulators, int32
+ * exponents) and must be ordered on the handle's stream (e.g. NCCL all-reduce on it).
+ * st_shard_set_total gives the parcel count of the cloud over all ranks, so that every rank
+ * uses the same fixed-point headroom; it needs the deterministic deposit.  No counterpart in
+ * the reference's one-GPU path. */
+ST_API int st_shard_set_total(st_handle* h, int cloud, int64_t n_parcels_all_ranks);
+ST_API int st_shard_buffers(st_handle* h, void** accumulators, int64_t* n_accumulators,
+                            int32_t** exponents, int32_t* n_exponents);
+/* 1 when the next step at this dt needs the probe phase, 0 when not, < 0 on error. */
+ST_API int st_shard_needs_probe(st_handle* h, double dt);
+ST_API int st_shard_probe(st_handle* h, double dt, double fluid_scale);
+ST_API int st_shard_deposit(st_handle* h, double dt, double fluid_scale);
+ST_API int st_shard_finish(st_handle* h);
 
 /* ---- shims with the reference's names and semantics -------------------------------- */
 /* Creates (or replaces) the process-wide default handle used by the two calls below, on

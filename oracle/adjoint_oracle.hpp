@@ -50,9 +50,10 @@ struct StepLocal {
  * from `fz` instead of being computed (frozen ownership for finite differences); otherwise
  * they are computed as in evolve_parcel and written to `fz`. */
 template <class P, class V>
-bool adj_forward_step(const Params<P, V>& pr, P dtP, V dtV, const double* U, V fs, P pos[3],
-                      V vel[3], V dIn, Frozen& fz, bool replay, StepLocal<V>& o)
+bool adj_forward_step(const Params<P, V>& pr, P dtP, V dtV, const double* U, V fs, V fs_lo,
+                      P pos[3], V vel[3], V dIn, Frozen& fz, bool replay, StepLocal<V>& o)
 {
+    constexpr bool MIX = mixed_mode<P, V>();
     const Mesh<P>& mesh = pr.mesh;
     const V d = dIn * pr.dscale;
     o.mB = ((pr.rhod_by_rhoc * (V)M_PI) * ((d * d) * d)) / (V)6;
@@ -65,18 +66,19 @@ bool adj_forward_step(const Params<P, V>& pr, P dtP, V dtV, const double* U, V f
         if (bad || l0.partitionI != 1) return false;
         posI = l0.posI;
     }
-    V uc[3];
-    for (int c = 0; c < 3; ++c) uc[c] = (V)U[3 * (int64_t)(posI - 1) + c] * fs;
     o.f = ((((V)18 * pr.mu) * dtV) / (pr.rho_d * (d * d))) * pr.alpha;
-    for (int c = 0; c < 3; ++c) o.du[c] = uc[c] - vel[c];
+    for (int c = 0; c < 3; ++c)
+        o.du[c] = slip_of<P, V>((V)U[3 * (int64_t)(posI - 1) + c], fs, fs_lo, vel[c]);
     o.mag2 = (o.du[0] * o.du[0] + o.du[1] * o.du[1]) + o.du[2] * o.du[2];
     V mag = std::sqrt(o.mag2);
     V Re = (mag * d) * pr.rnu;
     o.pw = (sizeof(V) == 4) ? (V)st_pow0687f((float)Re) : (V)st_pow0687((double)Re);
     o.g = o.f * ((V)1 + (V)0.15 * o.pw);
     P posNew[3];
+    V inc[3];
     for (int c = 0; c < 3; ++c) {
-        o.velNew[c] = vel[c] + o.g * o.du[c];
+        inc[c] = o.g * o.du[c];
+        o.velNew[c] = vel[c] + inc[c];
         posNew[c] = pos[c] + (P)o.velNew[c] * dtP;
     }
     V state0[3] = {vel[0], vel[1], vel[2]};
@@ -102,8 +104,11 @@ bool adj_forward_step(const Params<P, V>& pr, P dtP, V dtV, const double* U, V f
             state0[c] -= (V)2 * vel[c];
         }
     }
+    /* mixed precision deposits -m/rho_c times the increment, zero on a bounced component
+     * (the deposit forms of evolve_parcel) */
     for (int c = 0; c < 3; ++c) {
-        o.dep[c] = o.mB * (state0[c] - o.velNew[c]);
+        if (MIX) o.dep[c] = o.mB * ((b & (1 << c)) ? (V)0 : -inc[c]);
+        else o.dep[c] = o.mB * (state0[c] - o.velNew[c]);
         pos[c] = posNew[c];
         vel[c] = o.velNew[c];
     }
@@ -113,15 +118,15 @@ bool adj_forward_step(const Params<P, V>& pr, P dtP, V dtV, const double* U, V f
 /* Reverse of one step.  `vel` is the velocity at the start of the step, `a` the cotangent
  * of the velocity after the step (in) and before it (out). */
 template <class P, class V>
-void adj_reverse_step(const Params<P, V>& pr, P dtP, V dtV, const double* U, V fs, V vel[3],
-                      V dIn, const Frozen& fz, const V G[3], V a[3], double& dalpha,
+void adj_reverse_step(const Params<P, V>& pr, P dtP, V dtV, const double* U, V fs, V fs_lo,
+                      V vel[3], V dIn, const Frozen& fz, const V G[3], V a[3], double& dalpha,
                       double& dscale)
 {
     P pos[3] = {(P)0, (P)0, (P)0};
     V v[3] = {vel[0], vel[1], vel[2]};
     Frozen f2 = fz;
     StepLocal<V> o;
-    adj_forward_step<P, V>(pr, dtP, dtV, U, fs, pos, v, dIn, f2, true, o);
+    adj_forward_step<P, V>(pr, dtP, dtV, U, fs, fs_lo, pos, v, dIn, f2, true, o);
     const uint8_t b = fz.bounce;
     V w[3];
     V Sw = (V)0;

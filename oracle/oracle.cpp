@@ -38,6 +38,8 @@ typedef struct oracle_cfg {
     int32_t quant_limbs;  /* 1 or 2: fixed-point model of the deterministic deposit */
     double drag_multiplier;
     double diameter_scale;
+    int64_t deposit_bound;  /* parcels whose deposits share one fixed-point sum (all ranks of
+                               a sharded run); 0: the parcels of this call */
 } oracle_cfg;
 
 }  // extern "C"
@@ -113,7 +115,8 @@ struct AccSink : Sink<V> {
 template <class P, class V>
 int run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const double* d,
         const double* U, int nsteps, double dt, const double* fscale, double* src_seq,
-        double* src_quant, int32_t* cells, int32_t* scale_io, int64_t* stats, int nthreads)
+        double* src_quant, int32_t* cells, int32_t* scale_io, int64_t* stats, int nthreads,
+        int64_t* acc_out)
 {
     Params<P, V> pr = make_params<P, V>(cfg->n, cfg->origin, cfg->ending, cfg->mu_c, cfg->rho_c,
                                         cfg->rho_d, cfg->drag, cfg->n_substeps,
@@ -141,9 +144,14 @@ int run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const doubl
         else { hi.assign(3 * nC, 0); lo.assign(3 * nC, 0); }
     }
     seq.assign(src_seq ? 3 * nC : 0, 0.0);
-    const int64_t nbound = std::max<int64_t>(2, np * (int64_t)cfg->n_substeps);
+    const int64_t nbound =
+        std::max<int64_t>(2, std::max<int64_t>(np, cfg->deposit_bound) * (int64_t)cfg->n_substeps);
     const int H = quant_headroom(limbs, nbound);
     int L = scale_io ? *scale_io : INT_MIN;
+    int emax_last = EXP_NONE;
+    /* nsteps == 0 with scale INT_MIN: the probe of the next step only (its exponent in
+     * stats[3]); the state is not advanced */
+    const bool probe_only = (nsteps == 0 && quant && L == INT_MIN);
     int64_t lost = 0, overflow = 0;
 
 #ifdef _OPENMP
@@ -151,8 +159,9 @@ int run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const doubl
 #endif
     const bool par = nthreads != 1;
 
-    for (int s = 0; s < nsteps; ++s) {
-        const V fs = fscale ? (V)fscale[s] : (V)1;
+    for (int s = 0; s < (probe_only ? 1 : nsteps); ++s) {
+        V fs, fs_lo;
+        split_factor<P, V>(fscale, s, fs, fs_lo);
         if (quant && L == INT_MIN) {
             /* probe: the deposits of this step without committing the state */
             Acc pa;
@@ -163,10 +172,14 @@ int run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const doubl
                 AccSink<V> sk(&pa, true);
                 P x = X[i], y = Y[i], z = Z[i];
                 V u = Uu[i], v = Vv[i], w = Ww[i];
-                evolve_parcel<P, V>(pr, dtP, dtV, U, fs, x, y, z, u, v, w, D[i], sk);
+                evolve_parcel<P, V>(pr, dtP, dtV, U, fs, fs_lo, x, y, z, u, v, w, D[i], sk);
                 emax = std::max(emax, sk.emax);
             }
             L = (emax == EXP_NONE) ? -H : emax - H;
+            if (probe_only) {
+                emax_last = emax;
+                break;
+            }
         }
         const bool last = (s == nsteps - 1);
         Acc acc;
@@ -184,8 +197,8 @@ int run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const doubl
 #pragma omp parallel for schedule(static) reduction(max : emax) reduction(+ : lost_s, ovf_s) if (par)
         for (int64_t i = 0; i < np; ++i) {
             AccSink<V> sk(&acc, quant);
-            if (!evolve_parcel<P, V>(pr, dtP, dtV, U, fs, X[i], Y[i], Z[i], Uu[i], Vv[i], Ww[i],
-                                     D[i], sk))
+            if (!evolve_parcel<P, V>(pr, dtP, dtV, U, fs, fs_lo, X[i], Y[i], Z[i], Uu[i], Vv[i],
+                                     Ww[i], D[i], sk))
                 ++lost_s;
             emax = std::max(emax, sk.emax);
             ovf_s += sk.overflow;
@@ -205,6 +218,17 @@ int run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const doubl
                 src_quant[j] = ldexp2(v, L);
             }
         }
+        if (last && quant && acc_out) {
+            for (int64_t j = 0; j < 3 * nC; ++j) {
+                if (limbs == 1) {
+                    acc_out[j] = q1[j];
+                } else {  /* the library's two-limb layout: [hi, lo] per component */
+                    acc_out[2 * j] = hi[j];
+                    acc_out[2 * j + 1] = (int64_t)lo[j];
+                }
+            }
+        }
+        emax_last = emax;
         if (quant && emax != EXP_NONE) L = emax - H;
     }
     if (src_seq) std::memcpy(src_seq, seq.data(), sizeof(double) * 3 * nC);
@@ -219,7 +243,7 @@ int run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const doubl
             cells[i] = (bad || l.partitionI != 1) ? -1 : l.posI - 1;
         }
     }
-    if (stats) { stats[0] = lost; stats[1] = overflow; stats[2] = H; }
+    if (stats) { stats[0] = lost; stats[1] = overflow; stats[2] = H; stats[3] = emax_last; }
     return (int)(lost > 0 ? 1 : 0) | (overflow > 0 ? 2 : 0);
 }
 
@@ -235,22 +259,27 @@ extern "C" {
  *  src_quant: [nCells][3] fixed-point model of the library's deterministic deposit, or NULL
  *  cells    : [np] 0-based owning cell after the last step (-1 if lost), or NULL
  *  scale_io : in: scale exponent for the first step (INT_MIN: probe); out: for the next step
- *  stats    : [3] lost parcels, overflowing deposits, headroom bits H (or NULL)
+ *  stats    : [4] lost parcels, overflowing deposits, headroom bits H, largest-deposit
+ *             exponent of the last step (or of the probe when nsteps == 0), or NULL
+ *  acc_out  : raw fixed-point accumulators of the last step (int64 [nCells*3], two limbs:
+ *             [nCells*3][hi, lo]), or NULL
+ * nsteps == 0 with *scale_io == INT_MIN runs the probe of the first step only.
  * Returns 0, or a bit set: 1 = some parcel could not be located, 2 = deposit overflow. */
 int oracle_run(const oracle_cfg* cfg, int64_t np, double* xyz, double* uvw, const double* d,
                const double* U, int nsteps, double dt, const double* fscale, double* src_seq,
-               double* src_quant, int32_t* cells, int32_t* scale_io, int64_t* stats, int nthreads)
+               double* src_quant, int32_t* cells, int32_t* scale_io, int64_t* stats, int nthreads,
+               int64_t* acc_out)
 {
     switch (cfg->precision) {
     case 0:
         return run<float, float>(cfg, np, xyz, uvw, d, U, nsteps, dt, fscale, src_seq, src_quant,
-                                 cells, scale_io, stats, nthreads);
+                                 cells, scale_io, stats, nthreads, acc_out);
     case 1:
         return run<double, float>(cfg, np, xyz, uvw, d, U, nsteps, dt, fscale, src_seq, src_quant,
-                                  cells, scale_io, stats, nthreads);
+                                  cells, scale_io, stats, nthreads, acc_out);
     case 2:
         return run<double, double>(cfg, np, xyz, uvw, d, U, nsteps, dt, fscale, src_seq,
-                                   src_quant, cells, scale_io, stats, nthreads);
+                                   src_quant, cells, scale_io, stats, nthreads, acc_out);
     default:
         return -1;
     }
@@ -326,8 +355,10 @@ int adjoint_run(const oracle_cfg* cfg, int64_t np, const double* xyz, const doub
         V vel[3] = {(V)uvw[i], (V)uvw[np + i], (V)uvw[2 * np + i]};
         Frozen f = replay ? fz[i] : Frozen{0, 0};
         StepLocal<V> o;
-        if (!adj_forward_step<P, V>(pr, dtP, dtV, U, fscale ? (V)fscale[0] : (V)1, pos, vel,
-                                    (V)d[i], f, replay != 0, o))
+        V fs, fs_lo;
+        split_factor<P, V>(fscale, 0, fs, fs_lo);
+        if (!adj_forward_step<P, V>(pr, dtP, dtV, U, fs, fs_lo, pos, vel, (V)d[i], f,
+                                    replay != 0, o))
             return -1;
         for (int c = 0; c < 3; ++c) {
             double dv = (double)o.dep[c];
@@ -346,8 +377,10 @@ int adjoint_run(const oracle_cfg* cfg, int64_t np, const double* xyz, const doub
                 for (int c = 0; c < 3; ++c) vrec[((size_t)n * np + i) * 3 + c] = vel[c];
             Frozen& f = fz[(size_t)n * np + i];
             StepLocal<V> o;
-            if (!adj_forward_step<P, V>(pr, dtP, dtV, U, fscale ? (V)fscale[n] : (V)1, pos,
-                                        vel, (V)d[i], f, replay != 0, o))
+            V fs, fs_lo;
+            split_factor<P, V>(fscale, n, fs, fs_lo);
+            if (!adj_forward_step<P, V>(pr, dtP, dtV, U, fs, fs_lo, pos, vel, (V)d[i], f,
+                                        replay != 0, o))
                 return -1;
             for (int c = 0; c < 3; ++c) {
                 double dv = (double)o.dep[c];
@@ -401,8 +434,9 @@ int adjoint_run(const oracle_cfg* cfg, int64_t np, const double* xyz, const doub
             for (int c = 0; c < 3; ++c) vel[c] = vrec[((size_t)n * np + i) * 3 + c];
             V Gc[3];
             for (int c = 0; c < 3; ++c) Gc[c] = (V)G[3 * (int64_t)f.cell + c];
-            adj_reverse_step<P, V>(pr, dtP, dtV, U, fscale ? (V)fscale[n] : (V)1, vel, (V)d[i],
-                                   f, Gc, a, da, ds);
+            V fs, fs_lo;
+            split_factor<P, V>(fscale, n, fs, fs_lo);
+            adj_reverse_step<P, V>(pr, dtP, dtV, U, fs, fs_lo, vel, (V)d[i], f, Gc, a, da, ds);
         }
         if (dv0)
             for (int c = 0; c < 3; ++c) dv0[c * np + i] = (double)a[c];
@@ -476,7 +510,8 @@ int tet_run(const oracle_cfg* cfg, const TetMesh& mesh, int64_t np, double* xyz,
         D[i] = (V)d[i];
     }
     for (int s = 0; s < nsteps; ++s) {
-        const V fs = fscale ? (V)fscale[s] : (V)1;
+        V fs, fs_lo;
+        split_factor<double, V>(fscale, s, fs, fs_lo);
         if (quant && L == INT_MIN) {
             Acc pa;
             pa.limbs = limbs; pa.L = 0; pa.H = 1 << 20;
@@ -485,8 +520,8 @@ int tet_run(const oracle_cfg* cfg, const TetMesh& mesh, int64_t np, double* xyz,
                 double x[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
                 V v[3] = {Vv[3 * i], Vv[3 * i + 1], Vv[3 * i + 2]};
                 int32_t c = cells[i];
-                evolve_parcel_tet<V>(mesh, pr, dtP, dtV, U, fs, x, v, c, D[i], hop_limit, sk,
-                                     nullptr);
+                evolve_parcel_tet<V>(mesh, pr, dtP, dtV, U, fs, fs_lo, x, v, c, D[i], hop_limit,
+                                     sk, nullptr);
             }
             L = (sk.emax == EXP_NONE) ? -H : sk.emax - H;
         }
@@ -502,8 +537,8 @@ int tet_run(const oracle_cfg* cfg, const TetMesh& mesh, int64_t np, double* xyz,
         }
         AccSink<V> sk(&acc, quant);
         for (int64_t i = 0; i < np; ++i) {
-            if (!evolve_parcel_tet<V>(mesh, pr, dtP, dtV, U, fs, &P[3 * i], &Vv[3 * i], cells[i],
-                                      D[i], hop_limit, sk, hop_hist))
+            if (!evolve_parcel_tet<V>(mesh, pr, dtP, dtV, U, fs, fs_lo, &P[3 * i], &Vv[3 * i],
+                                      cells[i], D[i], hop_limit, sk, hop_hist))
                 ++lost;
         }
         ovf += sk.overflow;

@@ -31,6 +31,7 @@ class OracleCfg(ctypes.Structure):
         ("quant_limbs", ctypes.c_int32),
         ("drag_multiplier", ctypes.c_double),
         ("diameter_scale", ctypes.c_double),
+        ("deposit_bound", ctypes.c_int64),
     ]
 
 
@@ -52,7 +53,7 @@ def lib():
             P(OracleCfg), ctypes.c_int64, P(ctypes.c_double), P(ctypes.c_double),
             P(ctypes.c_double), P(ctypes.c_double), ctypes.c_int, ctypes.c_double,
             P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_int32),
-            P(ctypes.c_int32), P(ctypes.c_int64), ctypes.c_int,
+            P(ctypes.c_int32), P(ctypes.c_int64), ctypes.c_int, P(ctypes.c_int64),
         ]
         L.oracle_run.restype = ctypes.c_int
         L.oracle_locate.argtypes = [P(OracleCfg), ctypes.c_int64, P(ctypes.c_double),
@@ -95,7 +96,8 @@ def _ptr(a, ctype):
 
 
 def make_cfg(n, origin, ending, mu_c, rho_c, rho_d, drag="sn_explicit", precision="mixed",
-             n_substeps=1, quant_limbs=1, drag_multiplier=1.0, diameter_scale=1.0):
+             n_substeps=1, quant_limbs=1, drag_multiplier=1.0, diameter_scale=1.0,
+             deposit_bound=0):
     c = OracleCfg()
     n = [n] * 3 if np.isscalar(n) else list(n)
     origin = [origin] * 3 if np.isscalar(origin) else list(origin)
@@ -110,14 +112,18 @@ def make_cfg(n, origin, ending, mu_c, rho_c, rho_d, drag="sn_explicit", precisio
     c.quant_limbs = quant_limbs
     c.drag_multiplier = drag_multiplier
     c.diameter_scale = diameter_scale
+    c.deposit_bound = deposit_bound
     return c
 
 
 def run(cfg, xyz, uvw, d, U, nsteps, dt, fscale=None, want_seq=True, want_quant=True,
-        scale=INT_MIN, nthreads=1):
+        scale=INT_MIN, nthreads=1, want_acc=False):
     """Runs nsteps steps.  xyz/uvw are [3, np] float64 (copied), d [np], U [ncells, 3].
+    nsteps=0 with scale=INT_MIN runs the first step's probe only (its exponent in "emax").
 
-    Returns dict(xyz, uvw, cells, src_seq, src_quant, scale, lost, overflow, H, status)."""
+    Returns dict(xyz, uvw, cells, src_seq, src_quant, scale, lost, overflow, H, emax, acc,
+    status); emax is the largest-deposit exponent of the last step, acc (want_acc) its raw
+    int64 fixed-point accumulators."""
     xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
     uvw = np.ascontiguousarray(uvw, dtype=np.float64).copy()
     d = np.ascontiguousarray(d, dtype=np.float64)
@@ -130,18 +136,19 @@ def run(cfg, xyz, uvw, d, U, nsteps, dt, fscale=None, want_seq=True, want_quant=
     src_q = np.zeros(3 * ncells) if want_quant else None
     cells = np.zeros(npcl, dtype=np.int32)
     sc = np.array([scale], dtype=np.int32)
-    stats = np.zeros(3, dtype=np.int64)
+    stats = np.zeros(4, dtype=np.int64)
+    acc = np.zeros(3 * ncells * cfg.quant_limbs, dtype=np.int64) if want_acc else None
     st = lib().oracle_run(ctypes.byref(cfg), npcl, _ptr(xyz, ctypes.c_double),
                           _ptr(uvw, ctypes.c_double), _ptr(d, ctypes.c_double),
                           _ptr(U, ctypes.c_double), nsteps, dt, _ptr(fs, ctypes.c_double),
                           _ptr(src_seq, ctypes.c_double), _ptr(src_q, ctypes.c_double),
                           _ptr(cells, ctypes.c_int32), _ptr(sc, ctypes.c_int32),
-                          _ptr(stats, ctypes.c_int64), nthreads)
+                          _ptr(stats, ctypes.c_int64), nthreads, _ptr(acc, ctypes.c_int64))
     return dict(xyz=xyz, uvw=uvw, cells=cells,
                 src_seq=None if src_seq is None else src_seq.reshape(ncells, 3),
                 src_quant=None if src_q is None else src_q.reshape(ncells, 3),
                 scale=int(sc[0]), lost=int(stats[0]), overflow=int(stats[1]), H=int(stats[2]),
-                status=st)
+                emax=int(stats[3]), acc=acc, status=st)
 
 
 def locate(cfg, xyz):

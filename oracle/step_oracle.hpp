@@ -142,13 +142,44 @@ struct Sink {
     virtual ~Sink() {}
 };
 
+/* Mixed precision (P = double, V = float) is project-defined: the reference computes in
+ * Float32 only.  Two of its operations are arranged so that the result stays close to the
+ * all-FP64 step when a parcel has nearly relaxed to the carrier:
+ *   slip   u_c - v = fma(U, fs_hi, -v) + U * fs_lo, with fs = fs_hi + fs_lo the fluid
+ *          factor split into a float and its FP64 remainder (the product U*fs_hi is exact
+ *          inside the fma);
+ *   source D = state0 - v is carried instead of state0: every substep subtracts its velocity
+ *          increment, a component that bounces keeps its D, and a deposit is m/rho_c * D.
+ * P = V (FP32 reference mode and all-FP64) follow the reference's form exactly. */
+template <class P, class V>
+constexpr bool mixed_mode() { return sizeof(P) == 8 && sizeof(V) == 4; }
+
+template <class P, class V>
+inline V slip_of(V U, V fs, V fs_lo, V v)
+{
+    if (mixed_mode<P, V>()) return std::fma(U, fs, -v) + U * fs_lo;
+    return U * fs - v;
+}
+
+/* The fluid factor of step s (1 when there is none) as a V value and, in mixed precision,
+ * its FP64 remainder. */
+template <class P, class V>
+inline void split_factor(const double* fscale, int s, V& hi, V& lo)
+{
+    const double f = fscale ? fscale[s] : 1.0;
+    hi = (V)f;
+    lo = mixed_mode<P, V>() ? (V)(f - (double)hi) : (V)0;
+}
+
 /* evolve_particle! (A:1271-1365) for one parcel over one call of the step.
  * Returns false if the parcel could not be located (the reference would index out of
- * bounds or throw); the state is then left unchanged and nothing is deposited. */
+ * bounds or throw); the state is then left unchanged and nothing is deposited.
+ * fscale_lo is the FP64 remainder of the fluid factor (mixed precision; 0 otherwise). */
 template <class P, class V>
 bool evolve_parcel(const Params<P, V>& pr, P dtP, V dtV, const double* U, V fscale,
-                   P& X, P& Y, P& Z, V& Uv, V& Vv, V& Wv, V dIn, Sink<V>& sink)
+                   V fscale_lo, P& X, P& Y, P& Z, V& Uv, V& Vv, V& Wv, V dIn, Sink<V>& sink)
 {
+    constexpr bool MIX = mixed_mode<P, V>();
     const Mesh<P>& mesh = pr.mesh;
     const V d = dIn * pr.dscale;
     /* mᵈByρᶜ = ρᵈByρᶜ*π*⌀^3/6 (A:1280): left fold, ⌀^3 = ⌀*⌀*⌀ (literal_pow), π rounded to V */
@@ -163,27 +194,41 @@ bool evolve_parcel(const Params<P, V>& pr, P dtP, V dtV, const double* U, V fsca
     if (bad || L0.partitionI != 1 || L0.posI < 1 || L0.posI > mesh.nCells) return false;
     int32_t posI = L0.posI;
     int32_t partitionI = L0.partitionI;
-    V uc[3];
-    for (int c = 0; c < 3; ++c) uc[c] = (V)U[3 * (int64_t)(posI - 1) + c] * fscale;  /* A:1288 */
+    V Ur[3];                                                          /* A:1288 (raw U) */
+    for (int c = 0; c < 3; ++c) Ur[c] = (V)U[3 * (int64_t)(posI - 1) + c];
     V state0[3] = {vel[0], vel[1], vel[2]};                          /* A:1289 */
+    V D[3] = {0, 0, 0};                                              /* mixed: state0 - vel */
 
     /* dragFactor = 18*μᶜ*Δt/(ρᵈ*⌀^2) (A:1294) */
     const V f = ((((V)18 * pr.mu) * dtV) / (pr.rho_d * (d * d))) * pr.alpha;
 
     for (int t = 1; t <= pr.nsub; ++t) {                            /* A:1291 */
+        V inc[3] = {0, 0, 0};
         if (pr.drag == DRAG_STOKES_IMPLICIT) {
-            /* velNew = (vel + f*uᶜ)/(1 + f) (A:1295) */
-            for (int c = 0; c < 3; ++c) velNew[c] = (vel[c] + f * uc[c]) / ((V)1 + f);
+            if (MIX) {
+                /* the same update as an increment: v' = v + f (u - v)/(1 + f) */
+                for (int c = 0; c < 3; ++c) {
+                    inc[c] = (f * slip_of<P, V>(Ur[c], fscale, fscale_lo, vel[c])) / ((V)1 + f);
+                    velNew[c] = vel[c] + inc[c];
+                }
+            } else {
+                /* velNew = (vel + f*uᶜ)/(1 + f), uᶜ = U*fscale (A:1288, A:1295) */
+                for (int c = 0; c < 3; ++c)
+                    velNew[c] = (vel[c] + f * (Ur[c] * fscale)) / ((V)1 + f);
+            }
         } else {
             /* Schiller-Naumann, explicit Euler (project-defined; no reference code):
              * v' = v + f (1 + 0.15 Re^0.687) (u - v), Re = |u - v| d (1/nu) */
             V du[3];
-            for (int c = 0; c < 3; ++c) du[c] = uc[c] - vel[c];
+            for (int c = 0; c < 3; ++c) du[c] = slip_of<P, V>(Ur[c], fscale, fscale_lo, vel[c]);
             V mag = std::sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
             V Re = (mag * d) * pr.rnu;
             V pw = (sizeof(V) == 4) ? (V)st_pow0687f((float)Re) : (V)st_pow0687((double)Re);
             V g = f * ((V)1 + (V)0.15 * pw);
-            for (int c = 0; c < 3; ++c) velNew[c] = vel[c] + g * du[c];
+            for (int c = 0; c < 3; ++c) {
+                inc[c] = g * du[c];
+                velNew[c] = vel[c] + inc[c];
+            }
         }
         /* posNew = pos + velNew*Δt (A:1296) */
         for (int c = 0; c < 3; ++c) posNew[c] = pos[c] + (P)velNew[c] * dtP;
@@ -193,42 +238,59 @@ bool evolve_parcel(const Params<P, V>& pr, P dtP, V dtV, const double* U, V fsca
         int32_t posNewI = Ln.posI;
         int32_t partitionNewI = Ln.partitionI;
 
+        bool bnc[3] = {false, false, false};
         if (posNewI != posI || partitionNewI != partitionI) {          /* A:1306 */
-            bool bx = (Ln.I < 0) || (Ln.I >= mesh.N[0]);               /* A:1309-1311 */
-            bool by = (Ln.J < 0) || (Ln.J >= mesh.N[1]);
-            bool bz = (Ln.K < 0) || (Ln.K >= mesh.N[2]);
+            bnc[0] = (Ln.I < 0) || (Ln.I >= mesh.N[0]);               /* A:1309-1311 */
+            bnc[1] = (Ln.J < 0) || (Ln.J >= mesh.N[1]);
+            bnc[2] = (Ln.K < 0) || (Ln.K >= mesh.N[2]);
             /* hold the position component, mirror the OLD velocity, correct state0
              * by -2*vel (update_at_boundary!, A:731-736; A:1313-1329) */
-            if (bx) { posNew[0] = pos[0]; velNew[0] = -vel[0]; state0[0] -= (V)2 * vel[0]; }
-            if (by) { posNew[1] = pos[1]; velNew[1] = -vel[1]; state0[1] -= (V)2 * vel[1]; }
-            if (bz) { posNew[2] = pos[2]; velNew[2] = -vel[2]; state0[2] -= (V)2 * vel[2]; }
-            if (bx || by || bz) {                                        /* A:1333-1335 */
+            for (int c = 0; c < 3; ++c) {
+                if (bnc[c]) {
+                    posNew[c] = pos[c];
+                    velNew[c] = -vel[c];
+                    if (!MIX) state0[c] -= (V)2 * vel[c];
+                }
+            }
+            if (bnc[0] || bnc[1] || bnc[2]) {                            /* A:1333-1335 */
                 Ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);
                 if (bad) return false;
                 posNewI = Ln.posI;
                 partitionNewI = Ln.partitionI;
             }
             /* A:1337-1340 re-points to eulerianArr[partitionI] (the old one): a no-op
-             * with a single partition. */
-            if (t != pr.nsub && posNewI != posI) {                       /* A:1342-1348 */
-                if (partitionNewI != 1 || posNewI < 1 || posNewI > mesh.nCells) return false;
+             * with a single partition.  partitionI keeps its initial value: the reference
+             * never reassigns it. */
+        }
+        if (MIX)
+            for (int c = 0; c < 3; ++c)
+                if (!bnc[c]) D[c] -= inc[c];
+        if (t != pr.nsub && posNewI != posI) {                           /* A:1342-1348 */
+            if (partitionNewI != 1 || posNewI < 1 || posNewI > mesh.nCells) return false;
+            if (MIX)
+                sink.deposit(posI, mByRho * D[0], mByRho * D[1], mByRho * D[2]);
+            else
                 sink.deposit(posI, mByRho * (state0[0] - velNew[0]),
                              mByRho * (state0[1] - velNew[1]),
                              mByRho * (state0[2] - velNew[2]));
-                for (int c = 0; c < 3; ++c) state0[c] = velNew[c];
-                for (int c = 0; c < 3; ++c) uc[c] = (V)U[3 * (int64_t)(posNewI - 1) + c] * fscale;
-                posI = posNewI;
+            for (int c = 0; c < 3; ++c) {
+                state0[c] = velNew[c];
+                D[c] = 0;
             }
-            /* partitionI keeps its initial value: the reference never reassigns it. */
+            for (int c = 0; c < 3; ++c) Ur[c] = (V)U[3 * (int64_t)(posNewI - 1) + c];
+            posI = posNewI;
         }
         for (int c = 0; c < 3; ++c) { vel[c] = velNew[c]; pos[c] = posNew[c]; }
     }
 
     X = posNew[0]; Y = posNew[1]; Z = posNew[2];                        /* A:1355-1360 */
     Uv = velNew[0]; Vv = velNew[1]; Wv = velNew[2];
-    sink.deposit(posI, mByRho * (state0[0] - velNew[0]),              /* A:1361 */
-                 mByRho * (state0[1] - velNew[1]),
-                 mByRho * (state0[2] - velNew[2]));
+    if (MIX)                                                            /* A:1361 */
+        sink.deposit(posI, mByRho * D[0], mByRho * D[1], mByRho * D[2]);
+    else
+        sink.deposit(posI, mByRho * (state0[0] - velNew[0]),
+                     mByRho * (state0[1] - velNew[1]),
+                     mByRho * (state0[2] - velNew[2]));
     return true;
 }
 

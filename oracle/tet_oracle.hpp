@@ -113,12 +113,15 @@ inline int32_t tet_walk(const TetMesh& m, int32_t t, const double x[3], int hop_
 }
 
 /* One call of the step for one parcel on a tet mesh (positions in double).  Returns false
- * if the parcel was lost (walk exit or hop limit); the state is then unchanged. */
+ * if the parcel was lost (walk exit or hop limit); the state is then unchanged.  The velocity
+ * update and deposit forms are those of evolve_parcel in step_oracle.hpp (mixed precision:
+ * compensated slip and the carried D = state0 - v). */
 template <class V>
 bool evolve_parcel_tet(const TetMesh& m, const Params<double, V>& pr, double dtP, V dtV,
-                       const double* U, V fscale, double pos0[3], V vel0[3], int32_t& cell,
-                       V dIn, int hop_limit, Sink<V>& sink, int64_t* hop_hist)
+                       const double* U, V fscale, V fscale_lo, double pos0[3], V vel0[3],
+                       int32_t& cell, V dIn, int hop_limit, Sink<V>& sink, int64_t* hop_hist)
 {
+    constexpr bool MIX = mixed_mode<double, V>();
     const V d = dIn * pr.dscale;
     const V mByRho = ((pr.rhod_by_rhoc * (V)M_PI) * ((d * d) * d)) / (V)6;
     double pos[3] = {pos0[0], pos0[1], pos0[2]};
@@ -126,29 +129,44 @@ bool evolve_parcel_tet(const TetMesh& m, const Params<double, V>& pr, double dtP
     double posNew[3] = {pos[0], pos[1], pos[2]};
     V velNew[3] = {vel[0], vel[1], vel[2]};
     int32_t cur = cell;
-    V uc[3];
-    for (int c = 0; c < 3; ++c) uc[c] = (V)U[3 * (int64_t)cur + c] * fscale;
+    V Ur[3];
+    for (int c = 0; c < 3; ++c) Ur[c] = (V)U[3 * (int64_t)cur + c];
     V state0[3] = {vel[0], vel[1], vel[2]};
+    V D[3] = {0, 0, 0};
     const V f = ((((V)18 * pr.mu) * dtV) / (pr.rho_d * (d * d))) * pr.alpha;
     int32_t tNew = cur;
     for (int t = 1; t <= pr.nsub; ++t) {
+        V inc[3] = {0, 0, 0};
         if (pr.drag == DRAG_STOKES_IMPLICIT) {
-            for (int c = 0; c < 3; ++c) velNew[c] = (vel[c] + f * uc[c]) / ((V)1 + f);
+            if (MIX) {
+                for (int c = 0; c < 3; ++c) {
+                    inc[c] = (f * slip_of<double, V>(Ur[c], fscale, fscale_lo, vel[c])) / ((V)1 + f);
+                    velNew[c] = vel[c] + inc[c];
+                }
+            } else {
+                for (int c = 0; c < 3; ++c)
+                    velNew[c] = (vel[c] + f * (Ur[c] * fscale)) / ((V)1 + f);
+            }
         } else {
             V du[3];
-            for (int c = 0; c < 3; ++c) du[c] = uc[c] - vel[c];
+            for (int c = 0; c < 3; ++c) du[c] = slip_of<double, V>(Ur[c], fscale, fscale_lo, vel[c]);
             V mag = std::sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
             V Re = (mag * d) * pr.rnu;
             V pw = (sizeof(V) == 4) ? (V)st_pow0687f((float)Re) : (V)st_pow0687((double)Re);
             V g = f * ((V)1 + (V)0.15 * pw);
-            for (int c = 0; c < 3; ++c) velNew[c] = vel[c] + g * du[c];
+            for (int c = 0; c < 3; ++c) {
+                inc[c] = g * du[c];
+                velNew[c] = vel[c] + inc[c];
+            }
         }
         for (int c = 0; c < 3; ++c) posNew[c] = pos[c] + (double)velNew[c] * dtP;
         for (int c = 0; c < 3; ++c) {
             if (posNew[c] < m.origin[c] || posNew[c] > m.ending[c]) {
                 posNew[c] = pos[c];
                 velNew[c] = -vel[c];
-                state0[c] -= (V)2 * vel[c];
+                if (!MIX) state0[c] -= (V)2 * vel[c];
+            } else if (MIX) {
+                D[c] -= inc[c];
             }
         }
         int status = WALK_OK, hops = 0;
@@ -156,16 +174,25 @@ bool evolve_parcel_tet(const TetMesh& m, const Params<double, V>& pr, double dtP
         if (status != WALK_OK) return false;
         if (hop_hist) ++hop_hist[hops < 7 ? hops : 7];
         if (t != pr.nsub && tNew != cur) {
-            sink.deposit(cur + 1, mByRho * (state0[0] - velNew[0]),
-                         mByRho * (state0[1] - velNew[1]), mByRho * (state0[2] - velNew[2]));
-            for (int c = 0; c < 3; ++c) state0[c] = velNew[c];
-            for (int c = 0; c < 3; ++c) uc[c] = (V)U[3 * (int64_t)tNew + c] * fscale;
+            if (MIX)
+                sink.deposit(cur + 1, mByRho * D[0], mByRho * D[1], mByRho * D[2]);
+            else
+                sink.deposit(cur + 1, mByRho * (state0[0] - velNew[0]),
+                             mByRho * (state0[1] - velNew[1]), mByRho * (state0[2] - velNew[2]));
+            for (int c = 0; c < 3; ++c) {
+                state0[c] = velNew[c];
+                D[c] = 0;
+            }
+            for (int c = 0; c < 3; ++c) Ur[c] = (V)U[3 * (int64_t)tNew + c];
             cur = tNew;
         }
         for (int c = 0; c < 3; ++c) { vel[c] = velNew[c]; pos[c] = posNew[c]; }
     }
-    sink.deposit(cur + 1, mByRho * (state0[0] - velNew[0]), mByRho * (state0[1] - velNew[1]),
-                 mByRho * (state0[2] - velNew[2]));
+    if (MIX)
+        sink.deposit(cur + 1, mByRho * D[0], mByRho * D[1], mByRho * D[2]);
+    else
+        sink.deposit(cur + 1, mByRho * (state0[0] - velNew[0]), mByRho * (state0[1] - velNew[1]),
+                     mByRho * (state0[2] - velNew[2]));
     for (int c = 0; c < 3; ++c) { pos0[c] = posNew[c]; vel0[c] = velNew[c]; }
     cell = tNew;
     return true;

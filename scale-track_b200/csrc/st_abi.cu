@@ -22,6 +22,7 @@
 #include <cstring>
 #include <cstdint>
 #include <climits>
+#include <cmath>
 #include <mutex>
 #include <new>
 #include <string>
@@ -68,6 +69,7 @@ void st::st_set_last_error(const char* msg) { g_err = msg ? msg : ""; }
 /* ------------------------------------------------------------------------------------ */
 struct CloudBufs {
     int64_t n = 0;
+    int64_t shard_total = 0;   /* parcels of this cloud over all ranks of a sharded run */
     int64_t cap = 0;
     void* x[2] = {nullptr, nullptr};
     void* y[2] = {nullptr, nullptr};
@@ -144,6 +146,9 @@ struct st_handle {
     int steps_since_sort = 0;
     int block = 256;
     int grid = 0;
+    bool ring = true;      /* ST_STEP_KERNEL_RING for single-cloud steps */
+    int32_t* dexp = nullptr;   /* [nclouds] largest-deposit exponents of a sharded step */
+    bool shard_probed = false; /* st_shard_probe ran; its exponents are in dexp */
     int key_bits = 32;
     bool morton = true;
     int64_t total_tiles = 0;
@@ -314,15 +319,21 @@ int check_device_errors(st_handle* h)
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
     unsigned long long lost = 0, ovf = 0;
+    int fault = 0;
     for (int c = 0; c < nc; ++c) {
         lost += ctl[c].lost;
         ovf += ctl[c].overflow;
+        fault |= ctl[c].fault;
     }
-    if (lost || ovf) {
-        for (int c = 0; c < nc; ++c) ctl[c].lost = ctl[c].overflow = 0;
+    if (lost || ovf || fault) {
+        for (int c = 0; c < nc; ++c) ctl[c].lost = ctl[c].overflow = ctl[c].fault = 0;
         CK(cudaMemcpyAsync(h->dctl, ctl.data(), sizeof(CloudCtl) * nc, cudaMemcpyHostToDevice,
                            h->stream));
         CK(cudaStreamSynchronize(h->stream));
+        if (fault)
+            return fail(ST_ERR_CUDA,
+                        "a step kernel gave up waiting on its shared-memory pipeline (fault "
+                        "bits %d); that step's results are incomplete", fault);
         /* lost parcels take precedence in the status; the message counts both */
         if (lost)
             return fail(ST_ERR_PARCEL_OUTSIDE,
@@ -414,15 +425,99 @@ int do_sort_all(st_handle* h)
     return ST_OK;
 }
 
+/* Phases of one step.  PH_ALL is st_step.  A sharded step (one handle per rank, parcels
+ * split over the ranks) runs PH_PROBE (first step only), PH_DEPOSIT and PH_FINISH as separate
+ * calls, and the caller combines the ranks' exponents (max) and accumulators (sum) between
+ * them; the exponents travel through the contiguous buffer h->dexp. */
+enum StepPhase { PH_ALL = 0, PH_PROBE = 1, PH_DEPOSIT = 2, PH_FINISH = 3 };
+
+/* The launch sequence shared by hex and tet meshes: `launch(dep)` launches the step kernel
+ * of the mesh with deposit mode dep (DEP_PROBE for the read-only pass), `sort()` re-sorts
+ * every cloud. */
+template <class L, class S>
+int step_phases(st_handle* h, double dt, int phase, bool empty, L&& launch, S&& sort)
+{
+    const bool det = (h->dep == DEP_DET1 || h->dep == DEP_DET2);
+    const int nc = h->p.n_clouds;
+    if (phase != PH_ALL && !det)
+        return fail(ST_ERR_INVALID_ARGUMENT,
+                    "sharded steps need the deterministic deposit (integer accumulators)");
+    if (phase == PH_ALL && empty) return ST_OK;
+    if (phase == PH_PROBE) {
+        if (!empty) {
+            ProfScope ps(h, ST_KERNEL_PROBE);
+            CK(launch(DEP_PROBE));
+            h->launches += 1;
+        }
+        CK(launch_ctl_exponents(h->dctl, h->dexp, nc, false, h->stream));
+        h->shard_probed = true;
+        h->last_dt = dt;
+        return ST_OK;
+    }
+    if (phase != PH_FINISH) {
+        if (det && phase == PH_DEPOSIT && h->shard_probed) {
+            /* the first-step scale from the exponents every rank agreed on */
+            CK(launch_ctl_exponents(h->dctl, h->dexp, nc, true, h->stream));
+            CK(launch_set_scale(h->dctl, nc, h->stream));
+            h->launches += 1;
+            h->shard_probed = false;
+            h->need_probe = false;
+        } else if (det && (h->need_probe || dt != h->last_dt)) {
+            if (phase == PH_DEPOSIT)
+                return fail(ST_ERR_INVALID_ARGUMENT,
+                            "st_shard_probe must precede the first sharded step (and a new dt)");
+            {
+                ProfScope ps(h, ST_KERNEL_PROBE);
+                CK(launch(DEP_PROBE));
+            }
+            {
+                ProfScope ps(h, ST_KERNEL_OTHER);
+                CK(launch_set_scale(h->dctl, nc, h->stream));
+            }
+            h->launches += 2;
+            h->need_probe = false;
+        }
+        h->last_dt = dt;
+        if (!det) {
+            ProfScope ps(h, ST_KERNEL_OTHER);
+            CK(launch_zero_f64(h->dsrc, (int64_t)nc * h->stride, h->stream));
+            h->launches += 1;
+        }
+        if (!empty) {
+            ProfScope ps(h, ST_KERNEL_STEP);
+            CK(launch(h->dep));
+            h->launches += 1;
+        }
+        if (phase == PH_DEPOSIT) {
+            CK(launch_ctl_exponents(h->dctl, h->dexp, nc, false, h->stream));
+            return ST_OK;
+        }
+    }
+    if (det) {
+        if (phase == PH_FINISH) CK(launch_ctl_exponents(h->dctl, h->dexp, nc, true, h->stream));
+        {
+            ProfScope ps(h, ST_KERNEL_FINALIZE);
+            CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter, nc, h->stride,
+                               finalize_grid(h), h->stream));
+            h->launches += 1;
+        }
+        CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * nc * h->limbs * 8, h->stream));
+    }
+    h->steps += 1;
+    h->steps_since_sort += 1;
+    if (h->p.sort_interval > 0 && h->steps_since_sort >= h->p.sort_interval) return sort();
+    return ST_OK;
+}
+
 template <class V>
-int do_step_tet(st_handle* h, double dt, double fscale);
+int do_step_tet(st_handle* h, double dt, double fscale, int phase);
 
 template <class P, class V>
-int do_step(st_handle* h, double dt, double fscale)
+int do_step(st_handle* h, double dt, double fscale, int phase = PH_ALL)
 {
     int rc;
     if constexpr (std::is_same<P, double>::value) {
-        if (h->tet) return do_step_tet<V>(h, dt, fscale);
+        if (h->tet) return do_step_tet<V>(h, dt, fscale, phase);
     }
     if (!h->capturing && h->clouds_dirty && (rc = upload_clouds<P, V>(h)) != ST_OK) return rc;
     StepArgs<P, V> a;
@@ -430,7 +525,7 @@ int do_step(st_handle* h, double dt, double fscale)
     a.phys = phys_k<V>(h);
     a.dtP = (P)dt / (P)h->p.n_substeps;
     a.dtV = (V)a.dtP;
-    a.fscale = (V)fscale;
+    split_fluid_scale<P, V>(fscale, a.fscale, a.fscale_lo);
     a.nclouds = h->p.n_clouds;
     a.U = (const V*)h->dU;
     a.clouds = h->capturing
@@ -445,58 +540,24 @@ int do_step(st_handle* h, double dt, double fscale)
     } else {
         memset(&a.one, 0, sizeof a.one);
     }
-    if (a.total_tiles == 0) return ST_OK;
     int grid = h->grid;
     const int64_t warps_per_block = h->block / 32;
     const int64_t need = (a.total_tiles + warps_per_block - 1) / warps_per_block;
     if (grid > need) grid = (int)need;
     if (grid < 1) grid = 1;
-
-    const bool det = (h->dep == DEP_DET1 || h->dep == DEP_DET2);
-    if (det && (h->need_probe || dt != h->last_dt)) {
-        {
-            ProfScope ps(h, ST_KERNEL_PROBE);
-            CK(launch_step<P, V>(a, DEP_PROBE, grid, h->block, h->stream));
-        }
-        {
-            ProfScope ps(h, ST_KERNEL_OTHER);
-            CK(launch_set_scale(h->dctl, h->p.n_clouds, h->stream));
-        }
-        h->launches += 2;
-        h->need_probe = false;
-    }
-    h->last_dt = dt;
-    if (!det) {
-        ProfScope ps(h, ST_KERNEL_OTHER);
-        CK(launch_zero_f64(h->dsrc, (int64_t)h->p.n_clouds * h->stride, h->stream));
-        h->launches += 1;
-    }
-    {
-        ProfScope ps(h, ST_KERNEL_STEP);
-        CK(launch_step<P, V>(a, h->dep, grid, h->block, h->stream));
-        h->launches += 1;
-    }
-    if (det) {
-        {
-            ProfScope ps(h, ST_KERNEL_FINALIZE);
-            CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter,
-                               h->p.n_clouds, h->stride, finalize_grid(h), h->stream));
-            h->launches += 1;
-        }
-        CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * h->p.n_clouds * h->limbs * 8,
-                           h->stream));
-    }
-    h->steps += 1;
-    h->steps_since_sort += 1;
-    if (h->p.sort_interval > 0 && h->steps_since_sort >= h->p.sort_interval)
-        return do_sort_all<P, V>(h);
-    return ST_OK;
+    auto launch = [&](int dep) -> cudaError_t {
+        if (dep != DEP_PROBE && h->ring && ring_eligible<P, V>(a, dep))
+            return launch_step_ring<P, V>(a, dep, h->nsm, h->stream);
+        return launch_step<P, V>(a, dep, grid, h->block, h->stream);
+    };
+    return step_phases(h, dt, phase, a.total_tiles == 0, launch,
+                       [&] { return do_sort_all<P, V>(h); });
 }
 
-/* The step on a tetrahedral mesh: same launch sequence as do_step with the face-walk
- * kernel (st_tet.cu). */
+/* The step on a tetrahedral mesh: the launch sequence of do_step with the face-walk kernel
+ * (st_tet.cu). */
 template <class V>
-int do_step_tet(st_handle* h, double dt, double fscale)
+int do_step_tet(st_handle* h, double dt, double fscale, int phase)
 {
     int rc;
     if (!h->capturing && h->clouds_dirty && (rc = upload_clouds<double, V>(h)) != ST_OK) return rc;
@@ -505,7 +566,7 @@ int do_step_tet(st_handle* h, double dt, double fscale)
     a.phys = phys_k<V>(h);
     a.dtP = dt / (double)h->p.n_substeps;
     a.dtV = (V)a.dtP;
-    a.fscale = (V)fscale;
+    split_fluid_scale<double, V>(fscale, a.fscale, a.fscale_lo);
     a.nclouds = h->p.n_clouds;
     a.U = (const V*)h->dU;
     a.clouds = h->capturing
@@ -514,50 +575,15 @@ int do_step_tet(st_handle* h, double dt, double fscale)
     a.ctl = h->dctl;
     a.total_tiles = h->total_tiles;
     a.hop_hist = h->d_hops;
-    if (a.total_tiles == 0) return ST_OK;
     int grid = h->grid;
     const int64_t need = (a.total_tiles + h->block / 32 - 1) / (h->block / 32);
     if (grid > need) grid = (int)need;
     if (grid < 1) grid = 1;
-    const bool det = (h->dep == DEP_DET1 || h->dep == DEP_DET2);
-    if (det && (h->need_probe || dt != h->last_dt)) {
-        {
-            ProfScope ps(h, ST_KERNEL_PROBE);
-            CK(launch_step_tet<V>(a, DEP_PROBE, grid, h->block, h->stream));
-        }
-        {
-            ProfScope ps(h, ST_KERNEL_OTHER);
-            CK(launch_set_scale(h->dctl, h->p.n_clouds, h->stream));
-        }
-        h->launches += 2;
-        h->need_probe = false;
-    }
-    h->last_dt = dt;
-    if (!det) {
-        ProfScope ps(h, ST_KERNEL_OTHER);
-        CK(launch_zero_f64(h->dsrc, (int64_t)h->p.n_clouds * h->stride, h->stream));
-        h->launches += 1;
-    }
-    {
-        ProfScope ps(h, ST_KERNEL_STEP);
-        CK(launch_step_tet<V>(a, h->dep, grid, h->block, h->stream));
-        h->launches += 1;
-    }
-    if (det) {
-        {
-            ProfScope ps(h, ST_KERNEL_FINALIZE);
-            CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter,
-                               h->p.n_clouds, h->stride, finalize_grid(h), h->stream));
-            h->launches += 1;
-        }
-        CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * h->p.n_clouds * h->limbs * 8,
-                           h->stream));
-    }
-    h->steps += 1;
-    h->steps_since_sort += 1;
-    if (h->p.sort_interval > 0 && h->steps_since_sort >= h->p.sort_interval)
-        return do_sort_all<double, V>(h);
-    return ST_OK;
+    auto launch = [&](int dep) -> cudaError_t {
+        return launch_step_tet<V>(a, dep, grid, h->block, h->stream);
+    };
+    return step_phases(h, dt, phase, a.total_tiles == 0, launch,
+                       [&] { return do_sort_all<double, V>(h); });
 }
 
 /* Parcels generated on the device instead of uploaded (st_init_parcels). */
@@ -936,7 +962,7 @@ int graph_capture(st_handle* h, int n, double dt, const double* fs)
         a.phys = phys_k<V>(h);
         a.dtP = (P)dt / (P)h->p.n_substeps;
         a.dtV = (V)a.dtP;
-        a.fscale = (V)(fs ? fs[0] : 1.0);
+        split_fluid_scale<P, V>(fs ? fs[0] : 1.0, a.fscale, a.fscale_lo);
         a.nclouds = h->p.n_clouds;
         a.U = (const V*)h->dU;
         a.clouds = (const CloudK<P, V>*)h->dclouds;
@@ -1046,7 +1072,7 @@ int adj_prepare(st_handle* h, int cloud, const st_adjoint_desc* d)
     const size_t o_G = carve((size_t)h->stride * sizeof(double));
     const size_t o_av = carve((size_t)3 * n * sizeof(V));
     const size_t o_pa = carve((size_t)nseg * (grid > 0 ? grid : 1) * 2 * sizeof(double));
-    const size_t o_fs = carve((size_t)T * sizeof(V));
+    const size_t o_fs = carve((size_t)2 * T * sizeof(V));   /* fs, then fs_lo */
     const size_t o_mean = carve((size_t)h->stride * sizeof(double));
     const size_t o_ctl = carve(sizeof(CloudCtl));
     const size_t o_acc = carve((size_t)h->stride * limbs * 8);
@@ -1073,9 +1099,10 @@ int adj_prepare(st_handle* h, int cloud, const st_adjoint_desc* d)
     t.fs.assign(T, 1.0);
     if (d->fluid_scale)
         for (int k = 0; k < T; ++k) t.fs[k] = d->fluid_scale[k];
-    std::vector<V> fsv(T);
-    for (int k = 0; k < T; ++k) fsv[k] = (V)t.fs[k];
-    CK(cudaMemcpyAsync(t.fsd, fsv.data(), T * sizeof(V), cudaMemcpyHostToDevice, h->stream));
+    std::vector<V> fsv(2 * (size_t)T);
+    for (int k = 0; k < T; ++k) split_fluid_scale<P, V>(t.fs[k], fsv[k], fsv[T + k]);
+    CK(cudaMemcpyAsync(t.fsd, fsv.data(), 2 * (size_t)T * sizeof(V), cudaMemcpyHostToDevice,
+                       h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return ST_OK;
 }
@@ -1096,6 +1123,7 @@ AdjArgs<P, V> adj_args(st_handle* h)
     a.d = (const V*)c.d[c.cur];
     a.U = (const V*)h->dU;
     a.fs = (const V*)t.fsd;
+    a.fs_lo = (const V*)t.fsd + t.T;
     a.acc = t.acc; a.ctl = t.ctl;
     a.ck_x = (P*)t.ck_x; a.ck_v = (V*)t.ck_v;
     a.rec_v = (V*)t.rec_v; a.rec_c = t.rec_c; a.rec_b = t.rec_b;
@@ -1312,6 +1340,7 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
         (e = cudaMalloc((void**)&h->dctl, sizeof(CloudCtl) * p->n_clouds)) != cudaSuccess ||
         (e = cudaMalloc((void**)&h->dcounter, sizeof(unsigned int))) != cudaSuccess ||
         (e = cudaMalloc((void**)&h->dcount, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->dexp, sizeof(int32_t) * p->n_clouds)) != cudaSuccess ||
         (e = cudaMalloc(&h->dclouds, 256 * (size_t)p->n_clouds)) != cudaSuccess)
         return bail(fail(e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA,
                          "device allocation: %s", cudaGetErrorString(e)));
@@ -1336,7 +1365,7 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
             c.L = 0;
             c.emax = EXP_NONE;
             c.H = 0;
-            c.pad = 0;
+            c.fault = 0;
             c.lost = 0;
             c.overflow = 0;
         }
@@ -1485,7 +1514,7 @@ int st_destroy(st_handle* h)
     if (h->graph) cudaGraphDestroy(h->graph);
     void* arrs[] = {h->dU, h->dsrc, h->dacc, h->dctl, h->dcounter, h->dcount, h->dclouds,
                     h->dstage, h->adj.mem, h->dclouds2, h->d_verts, h->d_tets, h->d_planes, h->d_nbr,
-                    h->d_hops, h->dbins, h->doffs, h->dscan};
+                    h->d_hops, h->dbins, h->doffs, h->dscan, h->dexp};
     for (void* p : arrs)
         if (p) cudaFree(p);
     for (auto& r : h->recs) {
@@ -1515,7 +1544,9 @@ static int update_headroom(st_handle* h)
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
     for (int c = 0; c < h->p.n_clouds; ++c) {
-        int64_t bound = h->clouds[c].n * (int64_t)h->p.n_substeps;
+        /* a sharded cloud sums the deposits of every rank: its headroom covers all of them */
+        const int64_t np = std::max(h->clouds[c].n, h->clouds[c].shard_total);
+        int64_t bound = np * (int64_t)h->p.n_substeps;
         if (bound < 2) bound = 2;
         ctl[c].H = h->limbs == 1 ? 62 - QUANT_GROWTH_BITS - quant_nbits(bound)
                                  : 62 - QUANT_GROWTH_BITS;
@@ -1814,6 +1845,94 @@ int st_profile_read(st_handle* h, int kind, int64_t* launches, double* ms, int r
 }
 
 int64_t st_launch_count(st_handle* h) { return h ? h->launches : -1; }
+
+int st_set_drag_parameters(st_handle* h, double drag_multiplier, double diameter_scale)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (!(drag_multiplier > 0.0 && drag_multiplier < INFINITY) ||
+        !(diameter_scale > 0.0 && diameter_scale < INFINITY))
+        return fail(ST_ERR_INVALID_ARGUMENT,
+                    "st_set_drag_parameters: drag_multiplier and diameter_scale must be finite "
+                    "and > 0 (got %g, %g)", drag_multiplier, diameter_scale);
+    h->p.drag_multiplier = drag_multiplier;
+    h->p.diameter_scale = diameter_scale;
+    h->need_probe = true;      /* the deposits change size: new first-step scale */
+    h->adj.valid = false;      /* the pull-back needs the forward of these parameters */
+    return ST_OK;
+}
+
+int st_shard_set_total(st_handle* h, int cloud, int64_t n_parcels_all_ranks)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    if (n_parcels_all_ranks < 0 || n_parcels_all_ranks > ((int64_t)1 << 40))
+        return fail(ST_ERR_INVALID_ARGUMENT, "st_shard_set_total: count out of range");
+    if (h->dep != DEP_DET1 && h->dep != DEP_DET2)
+        return fail(ST_ERR_INVALID_ARGUMENT,
+                    "sharded steps need the deterministic deposit (integer accumulators)");
+    h->clouds[cloud].shard_total = n_parcels_all_ranks;
+    DeviceGuard g(h->device);
+    if ((rc = update_headroom(h))) return rc;
+    h->need_probe = true;
+    return ST_OK;
+}
+
+int st_shard_buffers(st_handle* h, void** accumulators, int64_t* n_accumulators,
+                     int32_t** exponents, int32_t* n_exponents)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (accumulators) *accumulators = h->dacc;
+    if (n_accumulators) *n_accumulators = h->stride * h->p.n_clouds * h->limbs;
+    if (exponents) *exponents = h->dexp;
+    if (n_exponents) *n_exponents = h->p.n_clouds;
+    return ST_OK;
+}
+
+int st_shard_needs_probe(st_handle* h, double dt)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    return (h->need_probe || dt != h->last_dt) ? 1 : 0;
+}
+
+static int shard_phase(st_handle* h, double dt, double fs, int phase)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (h->capturing) return fail(ST_ERR_INVALID_ARGUMENT, "sharded steps cannot be captured");
+    if (phase != PH_FINISH && !(dt > 0.0 && dt < INFINITY))
+        return fail(ST_ERR_INVALID_ARGUMENT, "dt must be finite and > 0");
+    DeviceGuard g(h->device);
+    return DISPATCH(h, do_step, h, dt, fs, phase);
+}
+
+int st_shard_probe(st_handle* h, double dt, double fluid_scale)
+{
+    return shard_phase(h, dt, fluid_scale, PH_PROBE);
+}
+
+int st_shard_deposit(st_handle* h, double dt, double fluid_scale)
+{
+    return shard_phase(h, dt, fluid_scale, PH_DEPOSIT);
+}
+
+int st_shard_finish(st_handle* h)
+{
+    int rc;
+    return shard_phase(h, h ? h->last_dt : 0.0, 1.0, PH_FINISH);
+}
+
+int st_set_step_kernel(st_handle* h, int kind)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (kind != ST_STEP_KERNEL_RING && kind != ST_STEP_KERNEL_WARP)
+        return fail(ST_ERR_INVALID_ARGUMENT, "st_set_step_kernel: unknown kind %d", kind);
+    h->ring = (kind == ST_STEP_KERNEL_RING);
+    return ST_OK;
+}
 
 int st_mean_source_forward(st_handle* h, int cloud, const st_adjoint_desc* desc,
                            double* mean_source)

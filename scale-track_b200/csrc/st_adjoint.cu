@@ -26,8 +26,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "st_internal.h"
-#include "st_pow.h"
+#include "st_device.cuh"
 
 namespace st {
 
@@ -79,8 +78,10 @@ struct AdjLocal {
 /* One forward step (evolve_particle!, nSteps = 1).  Returns false if the parcel is lost. */
 template <class P, class V>
 __device__ __forceinline__ bool adj_step(const AdjArgs<P, V>& a, P pos[3], V vel[3], V d,
-                                         V fs, int32_t& cell, uint8_t& bounce, AdjLocal<V>& o)
+                                         V fs, V fs_lo, int32_t& cell, uint8_t& bounce,
+                                         AdjLocal<V>& o)
 {
+    constexpr bool MIX = is_mixed<P, V>;
     const MeshK<P>& m = a.mesh;
     const PhysK<V>& ph = a.phys;
     bool bad = false;
@@ -89,10 +90,9 @@ __device__ __forceinline__ bool adj_step(const AdjArgs<P, V>& a, P pos[3], V vel
     if (bad || part != 1) return false;
     o.mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
     const V* Uc = a.U + 3 * (int64_t)(posI - 1);
-    V uc[3] = {__ldg(Uc) * fs, __ldg(Uc + 1) * fs, __ldg(Uc + 2) * fs};
     o.f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) o.du[k] = uc[k] - vel[k];
+    for (int k = 0; k < 3; ++k) o.du[k] = slip<MIX>(__ldg(Uc + k), fs, fs_lo, vel[k]);
     o.mag2 = (o.du[0] * o.du[0] + o.du[1] * o.du[1]) + o.du[2] * o.du[2];
     const V mag = adj_sqrt(o.mag2);
     const V Re = (mag * d) * ph.rnu;
@@ -100,10 +100,11 @@ __device__ __forceinline__ bool adj_step(const AdjArgs<P, V>& a, P pos[3], V vel
     else o.pw = (V)st_pow0687((double)Re);
     o.g = o.f * ((V)1 + (V)0.15 * o.pw);
     P posNew[3];
-    V velNew[3];
+    V velNew[3], inc[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        velNew[k] = vel[k] + o.g * o.du[k];
+        inc[k] = o.g * o.du[k];
+        velNew[k] = vel[k] + inc[k];
         posNew[k] = pos[k] + (P)velNew[k] * a.dtP;
     }
     uint8_t b = 0;
@@ -124,9 +125,12 @@ __device__ __forceinline__ bool adj_step(const AdjArgs<P, V>& a, P pos[3], V vel
             state0[k] -= (V)2 * vel[k];
         }
     }
+    /* deposit forms of the step kernel (st_kernels.cu evolve_one): mixed precision deposits
+     * -m/rho_c times the velocity increment, zero on a bounced component */
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        o.dep[k] = o.mB * (state0[k] - velNew[k]);
+        if constexpr (MIX) o.dep[k] = o.mB * ((b & (1 << k)) ? (V)0 : -inc[k]);
+        else o.dep[k] = o.mB * (state0[k] - velNew[k]);
         pos[k] = posNew[k];
         vel[k] = velNew[k];
     }
@@ -139,17 +143,18 @@ __device__ __forceinline__ bool adj_step(const AdjArgs<P, V>& a, P pos[3], V vel
  * and before it (out). */
 template <class P, class V>
 __device__ __forceinline__ void adj_reverse(const AdjArgs<P, V>& a, const V vel[3], V d, V fs,
+                                            V fs_lo,
                                             int32_t cell, uint8_t b, V av[3], double& dalpha,
                                             double& dscale)
 {
+    constexpr bool MIX = is_mixed<P, V>;
     const PhysK<V>& ph = a.phys;
     AdjLocal<V> o;
     o.mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
     const V* Uc = a.U + 3 * (int64_t)cell;
-    V uc[3] = {__ldg(Uc) * fs, __ldg(Uc + 1) * fs, __ldg(Uc + 2) * fs};
     o.f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) o.du[k] = uc[k] - vel[k];
+    for (int k = 0; k < 3; ++k) o.du[k] = slip<MIX>(__ldg(Uc + k), fs, fs_lo, vel[k]);
     o.mag2 = (o.du[0] * o.du[0] + o.du[1] * o.du[1]) + o.du[2] * o.du[2];
     const V mag = adj_sqrt(o.mag2);
     const V Re = (mag * d) * ph.rnu;
@@ -159,13 +164,15 @@ __device__ __forceinline__ void adj_reverse(const AdjArgs<P, V>& a, const V vel[
     V velNew[3], state0[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        velNew[k] = vel[k] + o.g * o.du[k];
+        const V inc = o.g * o.du[k];
+        velNew[k] = vel[k] + inc;
         state0[k] = vel[k];
         if (b & (1 << k)) {
             velNew[k] = -vel[k];
             state0[k] -= (V)2 * vel[k];
         }
-        o.dep[k] = o.mB * (state0[k] - velNew[k]);
+        if constexpr (MIX) o.dep[k] = o.mB * ((b & (1 << k)) ? (V)0 : -inc);
+        else o.dep[k] = o.mB * (state0[k] - velNew[k]);
     }
     const double* Gd = a.G + 3 * (int64_t)cell;
     const V G[3] = {(V)__ldg(Gd), (V)__ldg(Gd + 1), (V)__ldg(Gd + 2)};
@@ -228,7 +235,7 @@ __global__ void __launch_bounds__(256) k_adj_forward(const AdjArgs<P, V> a)
             int32_t cell;
             uint8_t b;
             AdjLocal<V> o;
-            if (adj_step<P, V>(a, pos, vel, d, a.fs[n], cell, b, o)) {
+            if (adj_step<P, V>(a, pos, vel, d, a.fs[n], a.fs_lo[n], cell, b, o)) {
                 key = cell;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) dep[k] = o.dep[k];
@@ -346,7 +353,9 @@ __global__ void __launch_bounds__(256) k_adj_reverse(const AdjArgs<P, V> a, int 
             int32_t cell = -1;
             uint8_t b = 0;
             AdjLocal<V> o;
-            if (ok && !adj_step<P, V>(a, pos, vel, d, a.fs[n0 + t], cell, b, o)) ok = false;
+            if (ok && !adj_step<P, V>(a, pos, vel, d, a.fs[n0 + t], a.fs_lo[n0 + t], cell, b,
+                                      o))
+                ok = false;
             a.rec_c[(int64_t)t * a.n + i] = ok ? cell : -1;
             a.rec_b[(int64_t)t * a.n + i] = b;
         }
@@ -356,8 +365,8 @@ __global__ void __launch_bounds__(256) k_adj_reverse(const AdjArgs<P, V> a, int 
             if (cell < 0) continue;
             const V* rv = a.rec_v + (int64_t)t * 3 * a.n;
             const V vn[3] = {rv[i], rv[a.n + i], rv[2 * a.n + i]};
-            adj_reverse<P, V>(a, vn, d, a.fs[n0 + t], cell, a.rec_b[(int64_t)t * a.n + i], av,
-                              dalpha, dscale);
+            adj_reverse<P, V>(a, vn, d, a.fs[n0 + t], a.fs_lo[n0 + t], cell,
+                              a.rec_b[(int64_t)t * a.n + i], av, dalpha, dscale);
         }
         a.adj_v[i] = av[0]; a.adj_v[a.n + i] = av[1]; a.adj_v[2 * a.n + i] = av[2];
     }

@@ -24,6 +24,19 @@ __device__ __forceinline__ double st_sqrt(double v) { return __dsqrt_rn(v); }
 __device__ __forceinline__ int32_t st_floor_int(float v) { return __float2int_rd(v); }
 __device__ __forceinline__ int32_t st_floor_int(double v) { return __double2int_rd(v); }
 
+/* Slip velocity u_c - v of one component, from the raw cell value Ur and the fluid factor
+ * fs = fs_hi + fs_lo.  In mixed precision the product Ur*fs_hi stays exact inside one fma and
+ * the low part of the FP64 factor is added, so the slip carries about one rounding of its
+ * own size, also when the parcel has nearly relaxed to the carrier (|u - v| << |u|); the
+ * FP32 and FP64 modes round u_c = U*fs to the velocity type first, as the reference does
+ * (A:1288, A:1295). */
+template <bool MIX, class V>
+__device__ __forceinline__ V slip(V Ur, V fs_hi, V fs_lo, V vel)
+{
+    if constexpr (MIX) return __fmaf_rn(Ur, fs_hi, -vel) + Ur * fs_lo;
+    else return Ur * fs_hi - vel;
+}
+
 /* floor(label, v) (A:668-670); values outside int32 mark the parcel as lost.  floor(v) lies
  * in [-2^31, 2^31) exactly when v does (both bounds are integers), so the range test is made
  * on v and one round-down conversion gives the label. */

@@ -28,6 +28,19 @@ constexpr int QUANT_GROWTH_BITS = 8;   /* deposits may grow 2^8 x between steps 
 
 enum DepMode { DEP_DET1 = 0, DEP_DET2 = 1, DEP_ATOMIC = 2, DEP_PROBE = 3 };
 
+/* Mixed precision: FP64 positions with FP32 drag and velocities. */
+template <class P, class V>
+constexpr bool is_mixed = sizeof(P) == 8 && sizeof(V) == 4;
+
+/* The fluid factor rounded to the velocity type; mixed precision also carries the FP64
+ * remainder, which the slip velocity adds back (st_device.cuh slip). */
+template <class P, class V>
+inline void split_fluid_scale(double fs, V& hi, V& lo)
+{
+    hi = (V)fs;
+    lo = is_mixed<P, V> ? (V)(fs - (double)hi) : (V)0;
+}
+
 template <class P>
 struct MeshK {
     int32_t N[3];
@@ -56,7 +69,8 @@ struct CloudCtl {
     int32_t L;                   /* fixed-point scale exponent of the current step        */
     int32_t emax;                /* max frexp exponent of this step's deposits            */
     int32_t H;                   /* headroom bits: first step maps 2^emax to 2^H          */
-    int32_t pad;
+    int32_t fault;               /* bit 0: the ring kernel's producer, bit 1: a consumer gave
+                                    up waiting on a pipeline barrier (sticky)              */
     unsigned long long lost;     /* parcels that could not be located (sticky)            */
     unsigned long long overflow; /* deposits beyond the fixed-point range (sticky)        */
 };
@@ -84,6 +98,7 @@ struct StepArgs {
     P dtP;                      /* substep for positions  */
     V dtV;                      /* substep for drag       */
     V fscale;                   /* factor on U            */
+    V fscale_lo;                /* mixed precision: FP64 factor - fscale, else 0 */
     int32_t nclouds;
     const V* U;                 /* [nCells*3] */
     const CloudK<P, V>* clouds; /* [nclouds] device array */
@@ -110,6 +125,7 @@ struct TetStepArgs {
     double dtP;
     V dtV;
     V fscale;
+    V fscale_lo;                         /* mixed precision: FP64 factor - fscale, else 0 */
     int32_t nclouds;
     const V* U;                          /* [nt*3] */
     const CloudK<double, V>* clouds;
@@ -152,6 +168,7 @@ struct AdjArgs {
     const V* d;
     const V* U;                 /* [nCells*3] */
     const V* fs;                /* [T] fluid factor per step */
+    const V* fs_lo;             /* [T] mixed precision: FP64 factor - fs, else zeros */
     unsigned long long* acc;    /* [ncomp*limbs] mean-source accumulator */
     CloudCtl* ctl;              /* scale and counters of the adjoint run */
     P* ck_x;                    /* checkpoints [nseg][3][n] */
@@ -181,11 +198,20 @@ template <class P, class V>
 cudaError_t launch_step(const StepArgs<P, V>& a, int dep, int grid, int block, cudaStream_t s);
 template <class P, class V>
 int step_max_active_blocks(int dep, int block);
+/* The step of a single cloud as a persistent shared-memory ring (st_ring.cu); deposits
+ * DEP_DET1, DEP_DET2 or DEP_ATOMIC.  Every parcel array must be 16-byte aligned. */
+template <class P, class V>
+cudaError_t launch_step_ring(const StepArgs<P, V>& a, int dep, int nsm, cudaStream_t s);
+/* true when launch_step_ring can run this step */
+template <class P, class V>
+bool ring_eligible(const StepArgs<P, V>& a, int dep);
 
 cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, CloudCtl* ctl,
                             unsigned int* counter, int nclouds, int64_t stride, int grid_x,
                             cudaStream_t s);
 cudaError_t launch_set_scale(CloudCtl* ctl, int nclouds, cudaStream_t s);
+cudaError_t launch_ctl_exponents(CloudCtl* ctl, int32_t* e, int nclouds, bool to_ctl,
+                                 cudaStream_t s);
 cudaError_t launch_zero_f64(double* p, int64_t n, cudaStream_t s);
 cudaError_t launch_f64_to_f32(const double* in, float* out, int64_t n, cudaStream_t s);
 cudaError_t launch_f32_to_f64(const float* in, double* out, int64_t n, cudaStream_t s);

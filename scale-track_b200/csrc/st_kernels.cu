@@ -24,53 +24,9 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "st_device.cuh"
+#include "st_step.cuh"
 
 namespace st {
-
-/* ------------------------------------------------------------------------------------ */
-/* relocation                                                                           */
-/* ------------------------------------------------------------------------------------ */
-
-struct LocK {
-    int32_t I, J, K;
-    int32_t posI;   /* 1-based linear cell index */
-    int32_t part;   /* 1-based partition index (one partition) */
-};
-
-/* divrem(i, n) truncating toward zero; most parcels are inside, where it is (0, i). */
-__device__ __forceinline__ void divrem_label(int32_t i, int32_t n, int32_t& q, int32_t& r)
-{
-    if ((uint32_t)i < (uint32_t)n) {
-        q = 0;
-        r = i;
-    } else {
-        q = i / n;
-        r = i - q * n;
-    }
-}
-
-template <class P>
-__device__ __forceinline__ LocK locate(const MeshK<P>& m, P x, P y, P z, bool& bad)
-{
-    LocK r;
-    r.I = floor_label((x - m.origin[0]) * m.rD[0], bad);
-    r.J = floor_label((y - m.origin[1]) * m.rD[1], bad);
-    r.K = floor_label((z - m.origin[2]) * m.rD[2], bad);
-    if ((uint32_t)r.I < (uint32_t)m.N[0] && (uint32_t)r.J < (uint32_t)m.N[1] &&
-        (uint32_t)r.K < (uint32_t)m.N[2]) {  /* inside: divrem is (0, i) on every axis */
-        r.part = 1;
-        r.posI = r.K * m.NxNy + r.J * m.N[0] + r.I + 1;
-        return r;
-    }
-    int32_t iP, iL, jP, jL, kP, kL;
-    divrem_label(r.I, m.N[0], iP, iL);
-    divrem_label(r.J, m.N[1], jP, jL);
-    divrem_label(r.K, m.N[2], kP, kL);
-    r.part = abs(kP) + abs(jP) + abs(iP) + 1;
-    r.posI = abs(kL) * m.NxNy + abs(jL) * m.N[0] + abs(iL) + 1;
-    return r;
-}
 
 /* ------------------------------------------------------------------------------------ */
 /* the step kernel                                                                      */
@@ -89,151 +45,6 @@ __device__ __forceinline__ int find_cloud(const StepArgs<P, V>& a, int64_t tile)
         else hi = mid - 1;
     }
     return lo;
-}
-
-/* One parcel through all substeps (A:1271-1365) after its start cell has been located and
- * the cell velocity gathered.  pos/vel are updated in place; the final deposit is returned
- * in (key, dep) for the warp-level reduction; intermediate deposits on cell change
- * (A:1342-1348, only with substeps > 1) go straight to memory. */
-template <class P, class V, int DEP>
-__device__ __forceinline__ void evolve_parcel(const StepArgs<P, V>& a, P pos[3], V vel[3], V d,
-                                              int32_t posI, V uc[3], unsigned long long* acc,
-                                              double* src, const Quant& qp, AmaxT<V>& amax,
-                                              unsigned& ovf, bool& lost, int32_t& key,
-                                              V dep[3])
-{
-    const MeshK<P>& mesh = a.mesh;
-    const PhysK<V>& ph = a.phys;
-    const P dtP = a.dtP;
-    /* mᵈ/ρᶜ = ρᵈ/ρᶜ·π·⌀³/6 (A:1280) */
-    const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
-    /* drag factor 18 μ Δt/(ρᵈ ⌀²) (A:1294), times the drag multiplier */
-    const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
-    P posNew[3] = {pos[0], pos[1], pos[2]};
-    V velNew[3] = {vel[0], vel[1], vel[2]};
-    V state0[3] = {vel[0], vel[1], vel[2]};                          /* A:1289 */
-    bool bad = false;
-    for (int t = 1; t <= ph.nsub; ++t) {                             /* A:1291 */
-        if (ph.drag == 0) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) velNew[k] = (vel[k] + f * uc[k]) / ((V)1 + f); /* A:1295 */
-        } else {
-            V du[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) du[k] = uc[k] - vel[k];
-            V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
-            V Re = (mag * d) * ph.rnu;
-            V pw;
-            if (sizeof(V) == 4) pw = (V)st_pow0687f((float)Re);
-            else pw = (V)st_pow0687((double)Re);
-            V g = f * ((V)1 + (V)0.15 * pw);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) velNew[k] = vel[k] + g * du[k];
-        }
-#pragma unroll
-        for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (P)velNew[k] * dtP;  /* A:1296 */
-
-        LocK ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);          /* A:1303 */
-        if (bad) { lost = true; return; }
-        if (ln.posI != posI || ln.part != 1) {                                   /* A:1306 */
-            const bool bx = (ln.I < 0) || (ln.I >= mesh.N[0]);
-            const bool by = (ln.J < 0) || (ln.J >= mesh.N[1]);
-            const bool bz = (ln.K < 0) || (ln.K >= mesh.N[2]);
-            /* hold position, mirror the old velocity, state0 -= 2 vel (A:1313-1329) */
-            if (bx) { posNew[0] = pos[0]; velNew[0] = -vel[0]; state0[0] -= (V)2 * vel[0]; }
-            if (by) { posNew[1] = pos[1]; velNew[1] = -vel[1]; state0[1] -= (V)2 * vel[1]; }
-            if (bz) { posNew[2] = pos[2]; velNew[2] = -vel[2]; state0[2] -= (V)2 * vel[2]; }
-            if (bx || by || bz) {                                                /* A:1333-1335 */
-                ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);
-                if (bad) { lost = true; return; }
-            }
-            if (t != ph.nsub && ln.posI != posI) {                               /* A:1342-1348 */
-                if (ln.part != 1 || ln.posI < 1 || ln.posI > mesh.nCells) { lost = true; return; }
-                V di[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k) di[k] = mB * (state0[k] - velNew[k]);
-                if (DEP == DEP_PROBE) {
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) track_max(di[k], amax);
-                } else {
-                    deposit_direct<DEP, V>(di, (int64_t)(posI - 1), acc, src, qp, amax, ovf);
-                }
-#pragma unroll
-                for (int k = 0; k < 3; ++k) state0[k] = velNew[k];
-                const V* Un = a.U + 3 * (int64_t)(ln.posI - 1);
-                uc[0] = __ldg(Un) * a.fscale;
-                uc[1] = __ldg(Un + 1) * a.fscale;
-                uc[2] = __ldg(Un + 2) * a.fscale;
-                posI = ln.posI;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 3; ++k) { vel[k] = velNew[k]; pos[k] = posNew[k]; }
-    }
-    key = posI - 1;                                                              /* A:1361 */
-#pragma unroll
-    for (int k = 0; k < 3; ++k) dep[k] = mB * (state0[k] - velNew[k]);
-}
-
-/* One substep (the benchmark configurations): evolve_particle! (A:1271-1365) with
- * nSteps = 1, where no intermediate deposit can happen and the final deposit goes to the
- * start cell.  A new position inside the mesh cannot meet a wall, so the reference's
- * relocation test (A:1303-1335) is only evaluated in full when the position left the index
- * range of some axis. */
-template <class P, class V>
-__device__ __forceinline__ void evolve_one(const StepArgs<P, V>& a, P pos[3], V vel[3], V d,
-                                           int32_t posI, const V uc[3], bool& lost, V dep[3])
-{
-    const MeshK<P>& mesh = a.mesh;
-    const PhysK<V>& ph = a.phys;
-    const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;  /* A:1280 */
-    const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha; /* A:1294 */
-    V velNew[3];
-    if (ph.drag == 0) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) velNew[k] = (vel[k] + f * uc[k]) / ((V)1 + f);  /* A:1295 */
-    } else {
-        V du[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) du[k] = uc[k] - vel[k];
-        V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
-        V Re = (mag * d) * ph.rnu;
-        V pw;
-        if (sizeof(V) == 4) pw = (V)st_pow0687f((float)Re);
-        else pw = (V)st_pow0687((double)Re);
-        V g = f * ((V)1 + (V)0.15 * pw);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) velNew[k] = vel[k] + g * du[k];
-    }
-    P posNew[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (P)velNew[k] * a.dtP;              /* A:1296 */
-    V state0[3] = {vel[0], vel[1], vel[2]};
-    /* floor(t) lies in [0, N) exactly when t does, so the fractional cell coordinates decide
-     * whether the new position is inside without converting them */
-    const P tx = (posNew[0] - mesh.origin[0]) * mesh.rD[0];
-    const P ty = (posNew[1] - mesh.origin[1]) * mesh.rD[1];
-    const P tz = (posNew[2] - mesh.origin[2]) * mesh.rD[2];
-    if (!(tx >= (P)0 && tx < (P)mesh.N[0] && ty >= (P)0 && ty < (P)mesh.N[1] && tz >= (P)0 &&
-          tz < (P)mesh.N[2])) {
-        bool bad = false;
-        LocK ln = locate(mesh, posNew[0], posNew[1], posNew[2], bad);                  /* A:1303 */
-        if (bad) { lost = true; return; }
-        if (ln.posI != posI || ln.part != 1) {                                          /* A:1306 */
-            const bool bx = (ln.I < 0) || (ln.I >= mesh.N[0]);
-            const bool by = (ln.J < 0) || (ln.J >= mesh.N[1]);
-            const bool bz = (ln.K < 0) || (ln.K >= mesh.N[2]);
-            if (bx) { posNew[0] = pos[0]; velNew[0] = -vel[0]; state0[0] -= (V)2 * vel[0]; }
-            if (by) { posNew[1] = pos[1]; velNew[1] = -vel[1]; state0[1] -= (V)2 * vel[1]; }
-            if (bz) { posNew[2] = pos[2]; velNew[2] = -vel[2]; state0[2] -= (V)2 * vel[2]; }
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        pos[k] = posNew[k];
-        vel[k] = velNew[k];
-        dep[k] = mB * (state0[k] - velNew[k]);                                          /* A:1361 */
-    }
 }
 
 /* The step kernel.  A warp owns a tile of SLICES x 32 consecutive parcels (lane l holds
@@ -323,9 +134,10 @@ __global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArg
             Uv[s] = R.Uv[s]; Vv[s] = R.Vv[s]; Wv[s] = R.Wv[s]; D[s] = R.D[s];
         }
         R = RN;
-        /* phase 2: start cells (A:1286) and cell velocities (A:1288) */
+        /* phase 2: start cells (A:1286) and raw cell velocities (A:1288; the fluid factor is
+         * applied in the slip) */
         int32_t pI[SLICES];
-        V uc[SLICES][3];
+        V Ur[SLICES][3];
 #pragma unroll
         for (int s = 0; s < SLICES; ++s) {
             pI[s] = 0;
@@ -335,9 +147,9 @@ __global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArg
                 if (!bad && l0.part == 1) {
                     pI[s] = l0.posI;
                     const V* Uc = a.U + 3 * (int64_t)(l0.posI - 1);
-                    uc[s][0] = __ldg(Uc) * a.fscale;
-                    uc[s][1] = __ldg(Uc + 1) * a.fscale;
-                    uc[s][2] = __ldg(Uc + 2) * a.fscale;
+                    Ur[s][0] = __ldg(Uc);
+                    Ur[s][1] = __ldg(Uc + 1);
+                    Ur[s][2] = __ldg(Uc + 2);
                 } else {
                     ++nlost;
                 }
@@ -354,10 +166,10 @@ __global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArg
                 V vel[3] = {Uv[s], Vv[s], Wv[s]};
                 bool lost = false;
                 if (ONE) {
-                    evolve_one<P, V>(a, pos, vel, D[s] * a.phys.dscale, pI[s], uc[s], lost, dep);
+                    evolve_one<P, V>(a, pos, vel, D[s] * a.phys.dscale, pI[s], Ur[s], lost, dep);
                     key = pI[s] - 1;
                 } else {
-                    evolve_parcel<P, V, DEP>(a, pos, vel, D[s] * a.phys.dscale, pI[s], uc[s],
+                    evolve_parcel<P, V, DEP>(a, pos, vel, D[s] * a.phys.dscale, pI[s], Ur[s],
                                              acc, src, qp, amax, ovf, lost, key, dep);
                 }
                 if (lost) {
@@ -520,6 +332,24 @@ __global__ void k_set_scale(CloudCtl* ctl, int nclouds)
         ctl[k].L = (em == EXP_NONE) ? -ctl[k].H : em - ctl[k].H;
         ctl[k].emax = EXP_NONE;
     }
+}
+
+/* Copies every cloud's largest-deposit exponent between the control blocks and a contiguous
+ * array (to_ctl: array -> blocks), the buffer a sharded run max-reduces across ranks. */
+__global__ void k_ctl_exponents(CloudCtl* ctl, int32_t* e, int nclouds, int to_ctl)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nclouds) {
+        if (to_ctl) ctl[k].emax = e[k];
+        else e[k] = ctl[k].emax;
+    }
+}
+
+cudaError_t launch_ctl_exponents(CloudCtl* ctl, int32_t* e, int nclouds, bool to_ctl,
+                                 cudaStream_t s)
+{
+    k_ctl_exponents<<<(nclouds + 127) / 128, 128, 0, s>>>(ctl, e, nclouds, to_ctl ? 1 : 0);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_set_scale(CloudCtl* ctl, int nclouds, cudaStream_t s)

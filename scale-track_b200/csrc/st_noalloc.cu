@@ -182,7 +182,7 @@ ST_API int st_step_noalloc(const st_params* p, const st_mesh_desc* m, int64_t n,
     a.phys.nsub = p->n_substeps;
     a.dtP = dt / (double)p->n_substeps;
     a.dtV = (float)a.dtP;
-    a.fscale = (float)fluid_scale;
+    split_fluid_scale<double, float>(fluid_scale, a.fscale, a.fscale_lo);
     a.nclouds = 1;
     a.U = U;
     a.clouds = cloud;

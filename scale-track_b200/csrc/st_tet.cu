@@ -176,21 +176,37 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
             asm volatile("prefetch.global.L1 [%0];" ::"l"(a.mesh.planes + 4 * (int64_t)cur));
             const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
             const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
+            constexpr bool MIX = is_mixed<double, V>;
             const V* Uc = a.U + 3 * (int64_t)cur;
-            V uc[3] = {__ldg(Uc) * a.fscale, __ldg(Uc + 1) * a.fscale, __ldg(Uc + 2) * a.fscale};
+            V Ur[3] = {__ldg(Uc), __ldg(Uc + 1), __ldg(Uc + 2)};
+            /* deposit forms of the hex step (st_kernels.cu evolve_parcel): FP32/FP64 carry
+             * state0, mixed precision carries D = state0 - v */
             V state0[3] = {vel[0], vel[1], vel[2]};
+            V D[3] = {(V)0, (V)0, (V)0};
             double posNew[3] = {pos[0], pos[1], pos[2]};
             V velNew[3] = {vel[0], vel[1], vel[2]};
             int32_t tNew = cur;
             bool lost = false;
             for (int t = 1; t <= nsub; ++t) {
+                V inc[3];
                 if (ph.drag == 0) {
+                    if constexpr (MIX) {
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) velNew[k] = (vel[k] + f * uc[k]) / ((V)1 + f);
+                        for (int k = 0; k < 3; ++k) {
+                            inc[k] = (f * slip<MIX>(Ur[k], a.fscale, a.fscale_lo, vel[k])) /
+                                     ((V)1 + f);
+                            velNew[k] = vel[k] + inc[k];
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            velNew[k] = (vel[k] + f * (Ur[k] * a.fscale)) / ((V)1 + f);
+                    }
                 } else {
                     V du[3];
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) du[k] = uc[k] - vel[k];
+                    for (int k = 0; k < 3; ++k)
+                        du[k] = slip<MIX>(Ur[k], a.fscale, a.fscale_lo, vel[k]);
                     V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
                     V Re = (mag * d) * ph.rnu;
                     V pw;
@@ -198,7 +214,10 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
                     else pw = (V)st_pow0687((double)Re);
                     V g = f * ((V)1 + (V)0.15 * pw);
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) velNew[k] = vel[k] + g * du[k];
+                    for (int k = 0; k < 3; ++k) {
+                        inc[k] = g * du[k];
+                        velNew[k] = vel[k] + inc[k];
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (double)velNew[k] * a.dtP;
@@ -207,7 +226,9 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
                     if (posNew[k] < a.mesh.origin[k] || posNew[k] > a.mesh.ending[k]) {
                         posNew[k] = pos[k];
                         velNew[k] = -vel[k];
-                        state0[k] -= (V)2 * vel[k];
+                        if constexpr (!MIX) state0[k] -= (V)2 * vel[k];
+                    } else if constexpr (MIX) {
+                        D[k] -= inc[k];
                     }
                 }
                 int status = TWALK_OK, hops = 0;
@@ -217,7 +238,8 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
                 if (t != nsub && tNew != cur) {
                     V di[3];
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) di[k] = mB * (state0[k] - velNew[k]);
+                    for (int k = 0; k < 3; ++k)
+                        di[k] = MIX ? mB * D[k] : mB * (state0[k] - velNew[k]);
                     if (DEP == DEP_PROBE) {
 #pragma unroll
                         for (int k = 0; k < 3; ++k) track_max(di[k], amax);
@@ -225,11 +247,14 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
                         deposit_direct<DEP, V>(di, (int64_t)cur, acc, src, qp, amax, ovf);
                     }
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) state0[k] = velNew[k];
+                    for (int k = 0; k < 3; ++k) {
+                        state0[k] = velNew[k];
+                        D[k] = (V)0;
+                    }
                     const V* Un = a.U + 3 * (int64_t)tNew;
-                    uc[0] = __ldg(Un) * a.fscale;
-                    uc[1] = __ldg(Un + 1) * a.fscale;
-                    uc[2] = __ldg(Un + 2) * a.fscale;
+                    Ur[0] = __ldg(Un);
+                    Ur[1] = __ldg(Un + 1);
+                    Ur[2] = __ldg(Un + 2);
                     cur = tNew;
                 }
 #pragma unroll
@@ -249,7 +274,8 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
                 }
                 key = cur;
 #pragma unroll
-                for (int k = 0; k < 3; ++k) dep[k] = mB * (state0[k] - velNew[k]);
+                for (int k = 0; k < 3; ++k)
+                    dep[k] = MIX ? mB * D[k] : mB * (state0[k] - velNew[k]);
             }
         }
         deposit_warp<DEP, V>(key, dep, acc, src, qp, lane, amax, ovf);

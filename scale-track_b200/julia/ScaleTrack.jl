@@ -108,15 +108,38 @@ function desc(T::Integer, C::Integer, dt::Real, fs::Union{Nothing,Vector{Float64
     StAdjointDesc(T, C, dt, fs === nothing ? Ptr{Float64}(C_NULL) : pointer(fs))
 end
 
-"""
-    mean_source(t, T, C, dt; fluid_scale) -> Sbar (3 × nCells)
+# the parcels of one cloud in st_set_parcels order: xyz, uvw as (n, 3), d as (n,)
+function get_parcels(t::Tracker; cloud::Integer = 0)
+    n = Int(ccall((:st_num_parcels, libscaletrack), Int64, (Ptr{Cvoid}, Cint), t.h, cloud))
+    xyz = Matrix{Float64}(undef, n, 3)
+    uvw = Matrix{Float64}(undef, n, 3)
+    d = Vector{Float64}(undef, n)
+    check(ccall((:st_get_parcels, libscaletrack), Cint,
+                (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                t.h, cloud, xyz, uvw, d))
+    return xyz, uvw, d
+end
 
-Time-averaged momentum source over `T` steps from the tracker's current state (the state
-is not modified).  Differentiable with respect to the drag multiplier, the diameter scale
-and the initial velocities through `rrule` (cell ownership frozen at the forward pass).
+set_drag_parameters!(t::Tracker, drag_multiplier::Real, diameter_scale::Real) =
+    check(ccall((:st_set_drag_parameters, libscaletrack), Cint, (Ptr{Cvoid}, Cdouble, Cdouble),
+                t.h, drag_multiplier, diameter_scale))
+
 """
-function mean_source(t::Tracker, T::Integer, C::Integer, dt::Real;
-                     fluid_scale::Union{Nothing,Vector{Float64}} = nothing, cloud::Integer = 0)
+    mean_source(t, α, s, v0, T, C, dt; fluid_scale, cloud) -> Sbar (3 × nCells)
+
+Time-averaged momentum source over `T` steps of one cloud, starting from its current
+positions and diameters with drag multiplier `α`, diameter scale `s` and initial velocities
+`v0` (n × 3, st_set_parcels order).  The tracker's positions are not advanced; `α`, `s` and
+`v0` stay set on it.  Differentiable in `α`, `s` and `v0` through `rrule` (cell ownership
+and wall bounces frozen at the forward pass); `t`, `T`, `C` and `dt` are not differentiated.
+"""
+function mean_source(t::Tracker, α::Real, s::Real, v0::Matrix{Float64}, T::Integer,
+                     C::Integer, dt::Real; fluid_scale::Union{Nothing,Vector{Float64}} = nothing,
+                     cloud::Integer = 0)
+    set_drag_parameters!(t, α, s)
+    xyz, _, d = get_parcels(t; cloud)
+    @assert size(v0) == size(xyz)
+    set_parcels!(t, xyz, v0, d; cloud)
     S = Matrix{Float64}(undef, 3, t.ncells)
     GC.@preserve fluid_scale begin
         check(ccall((:st_mean_source_forward, libscaletrack), Cint,
@@ -126,25 +149,24 @@ function mean_source(t::Tracker, T::Integer, C::Integer, dt::Real;
     return S
 end
 
-function ChainRulesCore.rrule(::typeof(mean_source), t::Tracker, T::Integer, C::Integer,
-                              dt::Real; fluid_scale = nothing, cloud::Integer = 0)
-    S = mean_source(t, T, C, dt; fluid_scale, cloud)
+function ChainRulesCore.rrule(::typeof(mean_source), t::Tracker, α::Real, s::Real,
+                              v0::Matrix{Float64}, T::Integer, C::Integer, dt::Real;
+                              fluid_scale = nothing, cloud::Integer = 0)
+    S = mean_source(t, α, s, v0, T, C, dt; fluid_scale, cloud)
     function mean_source_pullback(Sbar)
         cot = Matrix{Float64}(unthunk(Sbar))
-        da = Ref{Float64}(0.0)
+        dα = Ref{Float64}(0.0)
         ds = Ref{Float64}(0.0)
-        n = Int(ccall((:st_num_parcels, libscaletrack), Int64, (Ptr{Cvoid}, Cint), t.h, cloud))
-        dv0 = Matrix{Float64}(undef, n, 3)
+        dv0 = similar(v0)    # (n, 3) column-major = the [3][n] layout of the C side
         GC.@preserve fluid_scale begin
             check(ccall((:st_mean_source_pullback, libscaletrack), Cint,
                         (Ptr{Cvoid}, Cint, Ref{StAdjointDesc}, Ptr{Float64}, Ref{Float64},
                          Ref{Float64}, Ptr{Float64}),
-                        t.h, cloud, desc(T, C, dt, fluid_scale), cot, da, ds, dv0))
+                        t.h, cloud, desc(T, C, dt, fluid_scale), cot, dα, ds, dv0))
         end
-        # the tracker carries the differentiable parameters: return them as a Tangent
-        dt_tracker = Tangent{Tracker}(; drag_multiplier = da[], diameter_scale = ds[],
-                                      velocity0 = dv0)
-        return (NoTangent(), dt_tracker, NoTangent(), NoTangent(), NoTangent())
+        # one tangent per positional argument: (mean_source, t, α, s, v0, T, C, dt)
+        return (NoTangent(), NoTangent(), dα[], ds[], dv0, NoTangent(), NoTangent(),
+                NoTangent())
     end
     return S, mean_source_pullback
 end

@@ -38,7 +38,10 @@ EXPORTS = [
     "st_num_cells",
     "st_set_fluid_velocity", "st_set_fluid_velocity_device", "st_step", "st_get_source",
     "st_source_device", "st_synchronize", "st_get_stream", "st_set_stream",
-    "st_profile_enable", "st_profile_read", "st_launch_count", "st_setup", "st_default_handle",
+    "st_profile_enable", "st_profile_read", "st_launch_count", "st_set_step_kernel", "st_setup",
+    "st_set_drag_parameters", "st_shard_set_total", "st_shard_buffers", "st_shard_needs_probe",
+    "st_shard_probe", "st_shard_deposit", "st_shard_finish",
+    "st_default_handle",
     "st_allocate_array", "st_evolve_cloud", "st_finalize", "st_step_noalloc",
     "st_noalloc_max_cells", "st_mean_source_forward", "st_mean_source_pullback",
     "st_graph_capture", "st_graph_launch", "st_graph_release", "st_autotune",
@@ -128,6 +131,15 @@ def lib():
         "st_profile_read": ([c_h, ctypes.c_int, P(ctypes.c_int64), P(ctypes.c_double),
                              ctypes.c_int], ctypes.c_int),
         "st_launch_count": ([c_h], ctypes.c_int64),
+        "st_set_step_kernel": ([c_h, ctypes.c_int], ctypes.c_int),
+        "st_set_drag_parameters": ([c_h, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+        "st_shard_set_total": ([c_h, ctypes.c_int, ctypes.c_int64], ctypes.c_int),
+        "st_shard_buffers": ([c_h, P(ctypes.c_void_p), P(ctypes.c_int64), P(ctypes.c_void_p),
+                              P(ctypes.c_int32)], ctypes.c_int),
+        "st_shard_needs_probe": ([c_h, ctypes.c_double], ctypes.c_int),
+        "st_shard_probe": ([c_h, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+        "st_shard_deposit": ([c_h, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+        "st_shard_finish": ([c_h], ctypes.c_int),
         "st_setup": ([P(Params), P(MeshDesc)], ctypes.c_int),
         "st_default_handle": ([], c_h),
         "st_allocate_array": ([ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int],
@@ -399,6 +411,42 @@ class ParcelTracker:
 
     def launch_count(self):
         return int(lib().st_launch_count(self._h))
+
+    # ---- sharded steps (one cloud split over ranks) -------------------------------
+    def shard_set_total(self, n_parcels_all_ranks, cloud=0):
+        _check(lib().st_shard_set_total(self._h, cloud, int(n_parcels_all_ranks)))
+
+    def shard_buffers(self):
+        """(accumulator device pointer, int64 count, exponent device pointer, int32 count)"""
+        acc, nacc = ctypes.c_void_p(), ctypes.c_int64()
+        ex, nex = ctypes.c_void_p(), ctypes.c_int32()
+        _check(lib().st_shard_buffers(self._h, ctypes.byref(acc), ctypes.byref(nacc),
+                                      ctypes.byref(ex), ctypes.byref(nex)))
+        return acc.value, nacc.value, ex.value, nex.value
+
+    def shard_needs_probe(self, dt):
+        r = lib().st_shard_needs_probe(self._h, dt)
+        if r < 0:
+            _check(r)
+        return bool(r)
+
+    def shard_probe(self, dt, fluid_scale=1.0):
+        _check(lib().st_shard_probe(self._h, dt, fluid_scale))
+
+    def shard_deposit(self, dt, fluid_scale=1.0):
+        _check(lib().st_shard_deposit(self._h, dt, fluid_scale))
+
+    def shard_finish(self):
+        _check(lib().st_shard_finish(self._h))
+
+    def set_drag_parameters(self, drag_multiplier, diameter_scale):
+        _check(lib().st_set_drag_parameters(self._h, drag_multiplier, diameter_scale))
+
+    def set_step_kernel(self, kind):
+        """'ring' (default: shared-memory ring of block tiles) or 'warp' (per-warp tiles);
+        both give bit-identical results."""
+        k = {"ring": 0, "warp": 1}[kind] if isinstance(kind, str) else int(kind)
+        _check(lib().st_set_step_kernel(self._h, k))
 
     def graph_capture(self, n_steps, dt, fluid_scale=None):
         fs = None if fluid_scale is None else np.ascontiguousarray(fluid_scale, dtype=np.float64)

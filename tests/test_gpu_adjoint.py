@@ -121,3 +121,35 @@ def test_pullback_requires_matching_forward():
         h.mean_source_forward(T, C, workload.DT)
         with pytest.raises(st.ScaleTrackError):
             h.mean_source_pullback(np.zeros((N ** 3, 3)), T + 1, C, workload.DT)
+
+
+def test_drag_parameters_as_arguments():
+    """The call sequence of the Julia rrule: drag multiplier, diameter scale and initial
+    velocities set on an existing handle (st_set_drag_parameters, st_set_parcels) give the
+    same mean source and gradients as a handle created with them."""
+    xyz, uvw, d = inputs()
+    U = workload.tgv_field(N, dtype=np.float32)
+    v0 = np.random.default_rng(11).standard_normal(uvw.shape).astype(np.float32) * 0.01
+    cot = np.random.default_rng(12).standard_normal((N ** 3, 3)) * 1e-12
+    alpha, s = 1.07, 0.96
+    with st.ParcelTracker(gpu_params("mixed", alpha, s), st.mesh_desc(N, 0.0, workload.L_BOX)) as h:
+        h.set_parcels(xyz, v0.astype(np.float64), d)
+        h.set_fluid_velocity(U)
+        S_ref = h.mean_source_forward(T, C, workload.DT)
+        g_ref = h.mean_source_pullback(cot, T, C, workload.DT)
+    with st.ParcelTracker(gpu_params("mixed"), st.mesh_desc(N, 0.0, workload.L_BOX)) as h:
+        h.set_parcels(xyz, uvw, d)
+        h.set_fluid_velocity(U)
+        h.mean_source_forward(T, C, workload.DT)
+        h.set_drag_parameters(alpha, s)
+        with pytest.raises(st.ScaleTrackError):   # the forward of the old parameters is gone
+            h.mean_source_pullback(cot, T, C, workload.DT)
+        x1, _, d1 = h.get_parcels()
+        h.set_parcels(x1, v0.astype(np.float64), d1)
+        S = h.mean_source_forward(T, C, workload.DT)
+        g = h.mean_source_pullback(cot, T, C, workload.DT)
+        with pytest.raises(st.ScaleTrackError):
+            h.set_drag_parameters(0.0, 1.0)
+    assert np.array_equal(S, S_ref)
+    assert g[0] == g_ref[0] and g[1] == g_ref[1]
+    assert np.array_equal(g[2], g_ref[2])
