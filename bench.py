@@ -20,7 +20,8 @@ parcel (including the source finalize and, every 20th step, the re-sort).
              order, never re-sorted, three FP64 atomics per parcel
 --impl reference times the CPU restatement of the reference's path with all host threads.
 Multi-GPU (torchrun): every rank steps its own 1e7 parcels (weak scaling) against the
-replicated U, and the per-cell source is summed over ranks with an NCCL all-reduce.
+replicated U; the ranks sum their int64 fixed-point accumulators with an NCCL all-reduce and
+agree on one scale (the sharded step, st_shard_*), so the source is exact.
 """
 import argparse
 import json
@@ -46,6 +47,17 @@ METRIC = "particle-steps/s mixed vs FP64 on 1 B200 at src rel err<=1e-5; adjoint
 UNIT = "particle-steps/s"
 CONFIG = workload.CONFIGS["hex128_mixed"]
 FALLBACK_HBM_GBS = 6650.0
+
+
+def bench_config(npcl, ncells, ws):
+    """The workload both arms name in their JSON line (the reference arm steps a bounded
+    sample of it on the host cores and says so in cpu_baseline.sample)."""
+    return {"workload": "128^3 hex (2,097,152 cells), 1e7 parcels per GPU, Schiller-Naumann "
+                        "explicit, dt=1e-4 s, 1 substep, mixed precision, Morton re-sort every "
+                        "20 steps, time-varying field",
+            "nparcels_per_gpu": npcl, "ncells": ncells, "sort_interval": CONFIG["sort_interval"],
+            "l2": "inputs larger than L2: parcel state %d MB per GPU" % (npcl * 40 // 10**6),
+            "parallelism": "dp%d (parcels sharded, U replicated, source summed exactly)" % ws}
 
 
 def parse():
@@ -176,6 +188,17 @@ def ncu_traffic_per_parcel(precision):
         return None
 
 
+def ncu_instructions_per_parcel_substep(workload_name):
+    """Warp instructions per parcel and substep of a step kernel, from a committed ncu
+    summary (profiles/instructions.json), or None."""
+    p = os.path.join(ROOT, "profiles", "instructions.json")
+    try:
+        with open(p) as f:
+            return json.load(f)[workload_name]
+    except Exception:
+        return None
+
+
 def make_params(st, precision, deposit="deterministic", sort_interval=None):
     return st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
                      drag_model="schiller_naumann", precision=precision, n_substeps=1,
@@ -253,11 +276,25 @@ def run_ours(args):
     h = st.ParcelTracker(make_params(st, "mixed"), mesh, device=local)
     h.set_parcels(xyz, uvw, d)
     h.set_fluid_velocity(U)
-    src_view = None
+    step = h.step
     if pg is not None:
-        src_view = torch.as_tensor(DevArray(h.source_device_ptr(0), 3 * ncells), device=dev)
-        # one stream for the library and the collective
+        # sharded step: one stream for the library and the collectives; the ranks sum their
+        # fixed-point accumulators exactly (int64) and agree on one scale (max exponent), so
+        # the source is the same as one GPU stepping every parcel
         st.lib().st_set_stream(h.handle, torch.cuda.current_stream(dev).cuda_stream)
+        h.shard_set_total(ws * npcl)
+        acc_p, nacc, exp_p, nexp = h.shard_buffers()
+        acc_v = torch.as_tensor(DevArray(acc_p, nacc, "<i8"), device=dev)
+        exp_v = torch.as_tensor(DevArray(exp_p, nexp, "<i4"), device=dev)
+
+        def step(dt_, fs_):
+            if h.shard_needs_probe(dt_):
+                h.shard_probe(dt_, fs_)
+                pg.all_reduce(exp_v, op=pg.ReduceOp.MAX)
+            h.shard_deposit(dt_, fs_)
+            pg.all_reduce(acc_v)
+            pg.all_reduce(exp_v, op=pg.ReduceOp.MAX)
+            h.shard_finish()
     timer = DeviceTimer(torch, h.stream(), dev)
     k = 0
     # the clock sampler starts before the warm-up: nvidia-smi's start-up must not overlap
@@ -265,9 +302,7 @@ def run_ours(args):
     clk = ClockSampler(local).__enter__()
     time.sleep(1.5)
     for _ in range(args.warmup):
-        h.step(dt, fs(k))
-        if src_view is not None:
-            pg.all_reduce(src_view)
+        step(dt, fs(k))
         k += 1
     h.synchronize()
     barrier_sync()
@@ -277,9 +312,7 @@ def run_ours(args):
     w0 = time.time()
     timer.start()
     for _ in range(args.steps):
-        h.step(dt, fs(k))
-        if src_view is not None:
-            pg.all_reduce(src_view)
+        step(dt, fs(k))
         k += 1
     ms = timer.stop()
     w1 = time.time()
@@ -463,14 +496,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 positions / f32 drag+velocity "
         "/ int64 fixed-point source -> f64",
         "data": "synthetic (seeded uniform parcels, lognormal diameters, analytic TGV field)",
-        "config": {"workload": "128^3 hex (2,097,152 cells), 1e7 parcels "
-                               "per GPU, Schiller-Naumann explicit, dt=1e-4 s, 1 substep, "
-                               "mixed precision, Morton re-sort every 20 steps, "
-                               "time-varying field",
-                   "nparcels_per_gpu": npcl, "ncells": ncells,
-                   "sort_interval": CONFIG["sort_interval"],
-                   "l2": "inputs larger than L2: parcel state %d MB per GPU" % (npcl * 40 // 10**6),
-                   "parallelism": "dp%d (parcels sharded, U replicated, source all-reduced)" % ws},
+        "config": bench_config(npcl, ncells, ws),
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "gpu_launches": launches,
     }
@@ -558,10 +584,14 @@ def run_clouds(st, torch, local, dev):
             h.step(workload.DT)
         h.synchronize()
         steps = (c["steps"] // chunk) * chunk
+        h.profile(True)
+        h.profile_read("step", reset=True)
         timer.start()
         for _ in range(steps):
             h.step(workload.DT)
         ms_plain = timer.stop()
+        nst, st_ms = h.profile_read("step")
+        h.profile(False)
         # captured graph (capture right after a re-sort: run up to the next one first)
         h.synchronize()
         extra = (si - (3 + steps) % si) % si if si else 0
@@ -575,11 +605,30 @@ def run_clouds(st, torch, local, dev):
             h.graph_launch()
         ms_graph = timer.stop()
         h.synchronize()
+    peak, peak_src = measured_hbm_peak()
+    step_avg = st_ms / max(nst, 1)
+    algo = workload.step_kernel_bytes("mixed", total, n ** 3)
+    inst = ncu_instructions_per_parcel_substep("clouds64_hex64")
+    roof = {"bound": "issue: ten substeps of the parcel arithmetic per parcel in registers "
+                     "for each load and store of its state",
+            "kernel": "k_step<double,float,DET1,substeps,clouds> (all 64 clouds, one launch)",
+            "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(step_avg, 5),
+            "achieved": round(algo / (step_avg / 1e3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+            "peak_source": peak_src,
+            "frac": round(algo / (step_avg / 1e3) / 1e9 / peak, 4)}
+    if inst is not None:
+        # warp instructions issued per second against 4 per SM and clock (148 SMs, 1965 MHz)
+        rate = inst["warp_instructions_per_parcel_substep"] * total * c["substeps"] / \
+            (step_avg / 1e3)
+        roof["issue"] = {"warp_instructions_per_s": rate,
+                         "peak_warp_instructions_per_s": 148 * 4 * 1.965e9,
+                         "frac": round(rate / (148 * 4 * 1.965e9), 4),
+                         "instructions_from": inst["summary"]}
     return {"workload": "64 clouds, sizes log-uniform in [1e3, 2e6] (seed 2), "
                         "median diameter per cloud uniform in [5, 50] um, 64^3 mesh, one "
                         "source per cloud, mixed precision, 10 substeps inside one launch per "
                         "step",
-            "parcels": total, "steps": steps, "autotune": tune,
+            "parcels": total, "steps": steps, "autotune": tune, "roofline": roof,
             "particle_steps_per_s_graph": total * steps / (ms_graph / 1e3),
             "particle_steps_per_s_launches": total * steps / (ms_plain / 1e3),
             "ms_per_step_graph": ms_graph / steps, "ms_per_step_launches": ms_plain / steps}
@@ -778,9 +827,7 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 positions / f32 drag+velocity",
         "data": "synthetic (seeded uniform parcels, lognormal diameters, analytic TGV field)",
-        "config": {"workload": "the 128^3 hex, 1e7-parcel step on the host CPU: 128^3 hex, Schiller-Naumann "
-                               "explicit, dt=1e-4 s, mixed precision; bounded parcel sample",
-                   "nparcels_sampled": sample, "ncells": n ** 3},
+        "config": bench_config(npcl, n ** 3, ws),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

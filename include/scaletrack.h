@@ -120,6 +120,13 @@ ST_API int st_append_parcels(st_handle* h, int cloud, int64_t m, const double* x
 ST_API int st_get_parcels(st_handle* h, int cloud, double* xyz, double* uvw, double* d);
 /* 0-based owning cell of each parcel (locate, A:680-693), order as st_set_parcels. */
 ST_API int st_get_cells(st_handle* h, int cloud, int32_t* cells);
+/* A sample of one cloud's parcels by their st_set_parcels index (ids[m], each in [0, n)):
+ * positions and velocities as FP64 [3][m] each, and the owning cell [m] (tet meshes: the
+ * tracked tet; cuboid meshes: the located cell, -1 outside).  Any output may be NULL.
+ * Copies 56 bytes per sampled parcel instead of the whole cloud; synchronises the stream.
+ * No counterpart in the reference. */
+ST_API int st_get_parcel_sample(st_handle* h, int cloud, int64_t m, const int32_t* ids,
+                                double* xyz, double* uvw, int32_t* cells);
 /* Device-side order of a cloud: ids[k] = index (in the order given to st_set_parcels) of the
  * parcel stored at position k of the device arrays, which the periodic re-sort groups by
  * owning cell.  Diagnostic; no counterpart in the reference. */
@@ -349,11 +356,13 @@ ST_API int st_finalize(void);
  * library routine is called.  Meshes above ST_NOALLOC_MAX_CELLS cells are rejected with
  * ST_ERR_INVALID_ARGUMENT.  Runs on the current device and `stream` (a cudaStream_t, NULL
  * for the default stream) and returns after the stream has finished, with device-side
- * errors reported.  The first call on a device looks up the scratch array's address: make
- * it before any stream capture.  All calls share the one array: calls that overlap on the
- * GPU race.  Each call chooses its fixed-point scale from its own deposits, so the source
- * agrees with st_step's to the fixed-point resolution and positions and velocities are
- * bit-identical. */
+ * errors reported: it synchronises the stream, so it cannot be captured into a CUDA graph,
+ * and a call on a capturing stream is rejected with ST_ERR_INVALID_ARGUMENT before anything
+ * is launched.  The first call on a device looks up the scratch array's address and keeps
+ * it for the life of the process: do not call it on a device after cudaDeviceReset.  All
+ * calls share the one array: calls that overlap on the GPU race.  Each call chooses its
+ * fixed-point scale from its own deposits, so the source agrees with st_step's to the
+ * fixed-point resolution and positions and velocities are bit-identical. */
 ST_API int st_step_noalloc(const st_params* p, const st_mesh_desc* mesh, int64_t n, double* x,
                            double* y, double* z, float* u, float* v, float* w, const float* d,
                            const float* U, double* source, double dt, double fluid_scale,

@@ -148,6 +148,8 @@ struct st_handle {
     int grid = 0;
     bool ring = true;      /* ST_STEP_KERNEL_RING for single-cloud steps */
     int32_t* dexp = nullptr;   /* [nclouds] largest-deposit exponents of a sharded step */
+    float* dsrc32 = nullptr;   /* when set, the finalize also writes the FP32 source here
+                                  ([nclouds][stride]; the coupling's 4-byte exchange) */
     bool shard_probed = false; /* st_shard_probe ran; its exponents are in dexp */
     int key_bits = 32;
     bool morton = true;
@@ -172,6 +174,7 @@ struct st_handle {
     double* d_verts = nullptr;
     int32_t* d_tets = nullptr;
     double4* d_planes = nullptr;            /* [nt][4] face planes */
+    float4* d_planes32 = nullptr;           /* [nt][4] the same in FP32 */
     int32_t* d_nbr = nullptr;
     unsigned long long* d_hops = nullptr;   /* walk-length histogram [8] */
     /* CUDA-graph replay of a step sequence */
@@ -497,8 +500,8 @@ int step_phases(st_handle* h, double dt, int phase, bool empty, L&& launch, S&& 
         if (phase == PH_FINISH) CK(launch_ctl_exponents(h->dctl, h->dexp, nc, true, h->stream));
         {
             ProfScope ps(h, ST_KERNEL_FINALIZE);
-            CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dctl, h->dcounter, nc, h->stride,
-                               finalize_grid(h), h->stream));
+            CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dsrc32, h->dctl, h->dcounter, nc,
+                               h->stride, finalize_grid(h), h->stream));
             h->launches += 1;
         }
         CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * nc * h->limbs * 8, h->stream));
@@ -864,6 +867,40 @@ int do_get_cells(st_handle* h, int cloud, int32_t* cells)
         h->launches += 1;
     }
     CK(cudaMemcpyAsync(cells, c.keys[0], n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ST_OK;
+}
+
+template <class P, class V>
+int do_get_sample(st_handle* h, int cloud, int64_t m, const int32_t* ids, double* xyz,
+                  double* uvw, int32_t* cells)
+{
+    CloudBufs& c = h->clouds[cloud];
+    const size_t b_ids = ((size_t)m * sizeof(int32_t) + 255) / 256 * 256;
+    const size_t b_out = (size_t)m * 6 * sizeof(double);
+    int rc;
+    if ((rc = ensure_stage(h, b_ids + b_out + (size_t)m * sizeof(int32_t)))) return rc;
+    char* st = static_cast<char*>(h->dstage);
+    int32_t* d_ids = reinterpret_cast<int32_t*>(st);
+    double* d_out = reinterpret_cast<double*>(st + b_ids);
+    int32_t* d_cells = reinterpret_cast<int32_t*>(st + b_ids + b_out);
+    CK(cudaMemcpyAsync(d_ids, ids, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       h->stream));
+    SortBufs<P, V> b = sort_bufs<P, V>(h, c);
+    {
+        ProfScope ps(h, ST_KERNEL_OTHER);
+        CK(sample_cloud<P, V>(b, c.cur, c.n, mesh_k<P>(h), d_ids, m, d_out, d_cells, h->stream));
+        h->launches += 2;
+    }
+    if (xyz)
+        CK(cudaMemcpyAsync(xyz, d_out, (size_t)m * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->stream));
+    if (uvw)
+        CK(cudaMemcpyAsync(uvw, d_out + 3 * m, (size_t)m * 3 * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream));
+    if (cells)
+        CK(cudaMemcpyAsync(cells, d_cells, (size_t)m * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                           h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return ST_OK;
 }
@@ -1379,6 +1416,7 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
         if ((e = cudaMalloc((void**)&h->d_verts, nv * 3 * sizeof(double))) != cudaSuccess ||
             (e = cudaMalloc((void**)&h->d_tets, nt * 4 * sizeof(int32_t))) != cudaSuccess ||
             (e = cudaMalloc((void**)&h->d_planes, nt * 4 * sizeof(double4))) != cudaSuccess ||
+            (e = cudaMalloc((void**)&h->d_planes32, nt * 4 * sizeof(float4))) != cudaSuccess ||
             (e = cudaMalloc((void**)&h->d_nbr, nt * 4 * sizeof(int32_t))) != cudaSuccess ||
             (e = cudaMalloc((void**)&h->d_hops, 8 * sizeof(unsigned long long))) != cudaSuccess)
             return bail(fail(e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA,
@@ -1392,7 +1430,7 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
             (e = cudaMemsetAsync(h->d_hops, 0, 8 * sizeof(unsigned long long), h->stream)) !=
                 cudaSuccess ||
             (e = launch_tet_planes(h->d_verts, h->d_tets, (int64_t)nt, h->d_planes,
-                                   h->stream)) != cudaSuccess ||
+                                   h->d_planes32, h->stream)) != cudaSuccess ||
             (e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
             return bail(fail(ST_ERR_CUDA, "tet mesh set-up: %s", cudaGetErrorString(e)));
         h->launches += 1;
@@ -1403,12 +1441,20 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
         h->d_tets = nullptr;
         TetMeshK& k = h->tmesh;
         k.planes = h->d_planes;
+        k.planes32 = h->d_planes32;
         k.nbr = h->d_nbr;
         k.nt = (int64_t)nt;
+        double xm = 0.0;
         for (int a = 0; a < 3; ++a) {
             k.origin[a] = tm->origin[a];
             k.ending[a] = tm->ending[a];
+            xm = std::max(xm, std::max(std::fabs(tm->origin[a]), std::fabs(tm->ending[a])));
         }
+        /* rounded up to FP32: the pre-check's bound needs |x_i| <= xmax */
+        float xf = (float)xm;
+        if ((double)xf < xm) xf = std::nextafter(xf, INFINITY);
+        k.xmax = xf;
+        k.pad0 = 0;
         k.hop_limit = tm->hop_limit > 0 ? tm->hop_limit : 64;
         k.pad = 0;
     }
@@ -1421,6 +1467,8 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
                      : DISPATCH(h, step_max_active_blocks, h->dep, h->block);
     if (occ < 1) occ = 1;
     h->grid = p->grid_blocks > 0 ? p->grid_blocks : nsm * occ;
+    if (!h->tet && (e = DISPATCH(h, ring_prepare)) != cudaSuccess)
+        return bail(fail(ST_ERR_CUDA, "ring kernel set-up: %s", cudaGetErrorString(e)));
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
         return bail(fail(ST_ERR_CUDA, "set-up: %s", cudaGetErrorString(e)));
     *out = h;
@@ -1513,7 +1561,7 @@ int st_destroy(st_handle* h)
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
     void* arrs[] = {h->dU, h->dsrc, h->dacc, h->dctl, h->dcounter, h->dcount, h->dclouds,
-                    h->dstage, h->adj.mem, h->dclouds2, h->d_verts, h->d_tets, h->d_planes, h->d_nbr,
+                    h->dstage, h->adj.mem, h->dclouds2, h->d_verts, h->d_tets, h->d_planes, h->d_planes32, h->d_nbr,
                     h->d_hops, h->dbins, h->doffs, h->dscan, h->dexp};
     for (void* p : arrs)
         if (p) cudaFree(p);
@@ -1678,6 +1726,26 @@ int st_get_cells(st_handle* h, int cloud, int32_t* cells)
                                               : do_get_cells<double>(h, cloud, cells);
     });
     return rc ? rc : err;
+}
+
+int st_get_parcel_sample(st_handle* h, int cloud, int64_t m, const int32_t* ids, double* xyz,
+                         double* uvw, int32_t* cells)
+{
+    int rc;
+    if ((rc = check_handle(h)) || (rc = check_cloud(h, cloud))) return rc;
+    const int64_t n = h->clouds[cloud].n;
+    if (m < 0 || (m > 0 && !ids))
+        return fail(ST_ERR_INVALID_ARGUMENT, "st_get_parcel_sample: bad sample size or ids");
+    for (int64_t j = 0; j < m; ++j)
+        if (ids[j] < 0 || ids[j] >= n)
+            return fail(ST_ERR_INVALID_ARGUMENT,
+                        "st_get_parcel_sample: ids[%lld] = %d is not a parcel index (n = %lld)",
+                        (long long)j, ids[j], (long long)n);
+    if (m == 0) return ST_OK;
+    DeviceGuard g(h->device);
+    return guard_host_alloc("st_get_parcel_sample", [&] {
+        return DISPATCH(h, do_get_sample, h, cloud, m, ids, xyz, uvw, cells);
+    });
 }
 
 int st_get_order(st_handle* h, int cloud, int32_t* ids)
@@ -1920,7 +1988,6 @@ int st_shard_deposit(st_handle* h, double dt, double fluid_scale)
 
 int st_shard_finish(st_handle* h)
 {
-    int rc;
     return shard_phase(h, h ? h->last_dt : 0.0, 1.0, PH_FINISH);
 }
 
@@ -2445,6 +2512,20 @@ int st_evolve_cloud(double dt)
         else
             CK(launch_f32_to_f64((const float*)h->dstage, (double*)h->dU, ncomp, h->stream));
         h->launches += 1;
+    }
+    if (is->second.tbytes == 4) {
+        /* the finalize writes the 4-byte source next to the FP64 one: no conversion pass */
+        const size_t b32 = (size_t)h->stride * h->p.n_clouds * sizeof(float);
+        if ((rc = ensure_stage(h, b32 > (size_t)ncomp * 8 ? b32 : (size_t)ncomp * 8))) return rc;
+        h->dsrc32 = static_cast<float*>(h->dstage);
+        rc = DISPATCH(h, do_step, h, dt, 1.0);
+        h->dsrc32 = nullptr;
+        if (rc) return rc;
+        /* source device -> host (A:1148-1152) */
+        CK(cudaMemcpyAsync(is->second.ptr, h->dstage, ncomp * 4, cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return check_device_errors(h);
     }
     if ((rc = DISPATCH(h, do_step, h, dt, 1.0))) return rc;
     /* source device -> host (A:1148-1152) */

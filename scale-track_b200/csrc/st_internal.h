@@ -110,6 +110,9 @@ struct StepArgs {
 /* Unstructured tetrahedral mesh (st_tet.cu). */
 struct TetMeshK {
     const double4* planes;      /* [nt][4] outward face planes (n0, n1, n2, c), s = n.x - c */
+    const float4* planes32;     /* the same planes rounded to FP32 (the walk's pre-check) */
+    float xmax;                 /* max |coordinate| of any point of the box, rounded up */
+    int32_t pad0;
     const int32_t* nbr;         /* [nt][4] tet across the face opposite local vertex k, or -1 */
     int64_t nt;
     double origin[3];
@@ -143,7 +146,7 @@ int step_tet_max_active_blocks(int dep, int block);
  * cells[i] = tet or -1, and `outside` counts failures. */
 /* Face planes of every tet (canonical vertex order) from vertices and vertex ids. */
 cudaError_t launch_tet_planes(const double* verts, const int32_t* tets, int64_t nt,
-                              double4* planes, cudaStream_t s);
+                              double4* planes, float4* planes32, cudaStream_t s);
 cudaError_t launch_tet_locate(const TetMeshK& m, const double* x, const double* y,
                               const double* z, const int32_t* hint, int64_t n, int32_t* cells,
                               unsigned long long* outside, cudaStream_t s);
@@ -202,13 +205,18 @@ int step_max_active_blocks(int dep, int block);
  * DEP_DET1, DEP_DET2 or DEP_ATOMIC.  Every parcel array must be 16-byte aligned. */
 template <class P, class V>
 cudaError_t launch_step_ring(const StepArgs<P, V>& a, int dep, int nsm, cudaStream_t s);
+/* Shared-memory opt-in of the ring kernels of a precision on the current device. */
+template <class P, class V>
+cudaError_t ring_prepare();
 /* true when launch_step_ring can run this step */
 template <class P, class V>
 bool ring_eligible(const StepArgs<P, V>& a, int dep);
 
-cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, CloudCtl* ctl,
-                            unsigned int* counter, int nclouds, int64_t stride, int grid_x,
-                            cudaStream_t s);
+/* Fixed point -> FP64 source [nclouds][stride] (and, when src32 is not null, its FP32
+ * rounding in the same layout), next scale per cloud. */
+cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, float* src32,
+                            CloudCtl* ctl, unsigned int* counter, int nclouds, int64_t stride,
+                            int grid_x, cudaStream_t s);
 cudaError_t launch_set_scale(CloudCtl* ctl, int nclouds, cudaStream_t s);
 cudaError_t launch_ctl_exponents(CloudCtl* ctl, int32_t* e, int nclouds, bool to_ctl,
                                  cudaStream_t s);
@@ -259,6 +267,12 @@ template <class P, class V>
 cudaError_t unpermute_cloud(SortBufs<P, V>& b, int cur, int64_t n, cudaStream_t s);
 cudaError_t cells_unpermute(const int32_t* id, const int32_t* cell, int64_t n, int32_t* out,
                             cudaStream_t s);
+/* State ([6][m] FP64) and owning cells of the parcels ids[0..m) (st_set_parcels indices,
+ * each in [0, n)); uses b.perm[0] as scratch. */
+template <class P, class V>
+cudaError_t sample_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& mesh,
+                         const int32_t* ids, int64_t m, double* out, int32_t* cells_out,
+                         cudaStream_t s);
 template <class P>
 cudaError_t cells_cloud(const P* x, const P* y, const P* z, const int32_t* id, int64_t n,
                         const MeshK<P>& mesh, int32_t* cells_out, unsigned long long* outside,

@@ -254,7 +254,8 @@ template int step_max_active_blocks<double, double>(int, int);
 
 template <int LIMBS>
 __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict__ acc,
-                                                  double* __restrict__ src, CloudCtl* ctl,
+                                                  double* __restrict__ src,
+                                                  float* __restrict__ src32, CloudCtl* ctl,
                                                   unsigned int* counter, int nclouds,
                                                   int64_t stride)
 {
@@ -264,6 +265,7 @@ __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict
     const int L = ctl[c].L;
     const ulonglong2* a = reinterpret_cast<const ulonglong2*>(acc + (int64_t)c * stride * LIMBS);
     double2* s = reinterpret_cast<double2*>(src + (int64_t)c * stride);
+    float4* s32 = src32 ? reinterpret_cast<float4*>(src32 + (int64_t)c * stride) : nullptr;
     const int64_t ngroups = stride / 4;
     const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
     /* read-only pass: the accumulators are cleared afterwards by a memset, which costs less
@@ -290,8 +292,12 @@ __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict
                 v[k] = (double)hi * 4294967296.0 + (double)lo;
             }
         }
-        __stcs(s + 2 * g, make_double2(ldexp2(v[0], L), ldexp2(v[1], L)));
-        __stcs(s + 2 * g + 1, make_double2(ldexp2(v[2], L), ldexp2(v[3], L)));
+        const double o[4] = {ldexp2(v[0], L), ldexp2(v[1], L), ldexp2(v[2], L),
+                             ldexp2(v[3], L)};
+        __stcs(s + 2 * g, make_double2(o[0], o[1]));
+        __stcs(s + 2 * g + 1, make_double2(o[2], o[3]));
+        /* a 4-byte copy for an FP32 exchange array, rounded once from the FP64 source */
+        if (s32) __stcs(s32 + g, make_float4((float)o[0], (float)o[1], (float)o[2], (float)o[3]));
     }
     /* the last block to finish moves every cloud to the scale of its largest deposit */
     __syncthreads();
@@ -312,14 +318,16 @@ __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict
     }
 }
 
-cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, CloudCtl* ctl,
-                            unsigned int* counter, int nclouds, int64_t stride, int grid_x,
-                            cudaStream_t s)
+cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, float* src32,
+                            CloudCtl* ctl, unsigned int* counter, int nclouds, int64_t stride,
+                            int grid_x, cudaStream_t s)
 {
     if (stride % 4) return cudaErrorInvalidValue;
     dim3 grid(grid_x, nclouds);
-    if (limbs == 1) k_finalize<1><<<grid, 256, 0, s>>>(acc, src, ctl, counter, nclouds, stride);
-    else k_finalize<2><<<grid, 256, 0, s>>>(acc, src, ctl, counter, nclouds, stride);
+    if (limbs == 1)
+        k_finalize<1><<<grid, 256, 0, s>>>(acc, src, src32, ctl, counter, nclouds, stride);
+    else
+        k_finalize<2><<<grid, 256, 0, s>>>(acc, src, src32, ctl, counter, nclouds, stride);
     return cudaGetLastError();
 }
 

@@ -11,10 +11,14 @@
  *
  * The scratch array lives in every GPU that loads this library until the process exits.
  * Its device address is looked up once per device, on the first call made on that device
- * (cudaGetSymbolAddress with that device current); make that first call before any stream
- * capture.  All calls share the one array and it keeps the last call's contents: each call
- * clears the accumulator and control block it needs before use, and calls that overlap on
- * the GPU (other streams or host threads) race on the array.
+ * (cudaGetSymbolAddress with that device current), and kept for the life of the process: a
+ * cudaDeviceReset of that device makes the kept address stale, so the entry point must not
+ * be called on a device after it was reset.  Every call ends by reading the control block
+ * back and synchronising the stream, so a call cannot be recorded into a CUDA graph: one
+ * made on a capturing stream is rejected before anything is launched.  All calls share the
+ * one array and it keeps the last call's contents: each call clears the accumulator and
+ * control block it needs before use, and calls that overlap on the GPU (other streams or
+ * host threads) race on the array.
  */
 #include <climits>
 #include <cstdint>
@@ -131,6 +135,16 @@ ST_API int st_step_noalloc(const st_params* p, const st_mesh_desc* m, int64_t n,
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
         return fail(ST_ERR_CUDA, "no current CUDA device");
+    {
+        /* the call synchronises the stream at its end, which a capture does not allow */
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        const cudaError_t e = cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cs);
+        if (e != cudaSuccess) return fail(ST_ERR_CUDA, cudaGetErrorString(e));
+        if (cs != cudaStreamCaptureStatusNone)
+            return fail(ST_ERR_INVALID_ARGUMENT,
+                        "st_step_noalloc synchronises its stream and cannot be captured into a "
+                        "CUDA graph");
+    }
     unsigned char* base;
     {
         std::lock_guard<std::mutex> lk(g_mu);

@@ -375,27 +375,48 @@ __global__ void __launch_bounds__(RING_THREADS, 1) k_step_ring(const StepArgs<P,
 /* host side                                                                            */
 /* ------------------------------------------------------------------------------------ */
 
+/* The shared-memory opt-in of one kernel instance on the current device, made once per
+ * device (remembered in a bit mask per instance). */
 template <class P, class V, int DEP, bool ONE>
-static cudaError_t launch_ring_t(const StepArgs<P, V>& a, int nsm, cudaStream_t s)
+static cudaError_t ring_attr()
 {
-    using R = RingGeom<P, V>;
-    /* the shared-memory opt-in is per device: remembered in a bit mask per instantiation */
     static std::atomic<unsigned long long> ready{0};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     const unsigned long long bit = 1ULL << (dev & 63);
-    if (!(ready.load() & bit)) {
-        e = cudaFuncSetAttribute(k_step_ring<P, V, DEP, ONE>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R::SMEM);
-        if (e != cudaSuccess) return e;
-        ready.fetch_or(bit);
-    }
+    if (ready.load() & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_step_ring<P, V, DEP, ONE>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)RingGeom<P, V>::SMEM);
+    if (e == cudaSuccess) ready.fetch_or(bit);
+    return e;
+}
+
+template <class P, class V, int DEP, bool ONE>
+static cudaError_t launch_ring_t(const StepArgs<P, V>& a, int nsm, cudaStream_t s)
+{
+    cudaError_t e = ring_attr<P, V, DEP, ONE>();
+    if (e != cudaSuccess) return e;
     const int64_t nfull = a.one.n / RING_BT;
     int64_t grid = nfull < nsm ? nfull : nsm;
     if (grid < 1) grid = 1;
-    k_step_ring<P, V, DEP, ONE><<<(int)grid, RING_THREADS, R::SMEM, s>>>(a);
+    k_step_ring<P, V, DEP, ONE><<<(int)grid, RING_THREADS, RingGeom<P, V>::SMEM, s>>>(a);
     return cudaGetLastError();
+}
+
+/* Makes every ring kernel instance of a precision launchable on the current device (called
+ * when a handle is created, outside any stream capture). */
+template <class P, class V>
+cudaError_t ring_prepare()
+{
+    const cudaError_t r[6] = {ring_attr<P, V, DEP_DET1, true>(), ring_attr<P, V, DEP_DET1, false>(),
+                              ring_attr<P, V, DEP_DET2, true>(), ring_attr<P, V, DEP_DET2, false>(),
+                              ring_attr<P, V, DEP_ATOMIC, true>(),
+                              ring_attr<P, V, DEP_ATOMIC, false>()};
+    for (cudaError_t e : r)
+        if (e != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 template <class P, class V>
@@ -428,6 +449,9 @@ cudaError_t launch_step_ring(const StepArgs<P, V>& a, int dep, int nsm, cudaStre
 template cudaError_t launch_step_ring<float, float>(const StepArgs<float, float>&, int, int, cudaStream_t);
 template cudaError_t launch_step_ring<double, float>(const StepArgs<double, float>&, int, int, cudaStream_t);
 template cudaError_t launch_step_ring<double, double>(const StepArgs<double, double>&, int, int, cudaStream_t);
+template cudaError_t ring_prepare<float, float>();
+template cudaError_t ring_prepare<double, float>();
+template cudaError_t ring_prepare<double, double>();
 template bool ring_eligible<float, float>(const StepArgs<float, float>&, int);
 template bool ring_eligible<double, float>(const StepArgs<double, float>&, int);
 template bool ring_eligible<double, double>(const StepArgs<double, double>&, int);

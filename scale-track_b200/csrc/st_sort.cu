@@ -7,7 +7,8 @@
  * warps gather neighbouring cells of U (L2 locality).  Keys are the Morton code of the cell
  * (i, j, k) (the linear cell index for meshes wider than 1024 cells, the owning tet on tet
  * meshes).  Key ranges of at most 2^24 values are ranked by a counting sort: per-key counts
- * with warp-aggregated atomics, an exclusive scan, then each warp claims its slots of each
+ * with warp-aggregated atomics, an exclusive scan of the counts (two kernels of this file),
+ * then each warp claims its slots of each
  * key with one atomic.  Parcels of one key keep their order inside a warp; across warps it
  * follows the order of the atomics, which no result depends on (the deposit is an exact
  * integer sum and everything else is per parcel).  Wider key ranges use CUB's LSD radix
@@ -18,7 +19,6 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
 
 #include "st_internal.h"
 
@@ -171,8 +171,30 @@ __global__ void k_unpermute(const int32_t* __restrict__ id, int64_t n,
     }
 }
 
-/* Owning cell with the step's own locate semantics (A:680-693), 0-based; -1 and a count
- * when the parcel is outside the mesh. */
+/* Owning cell with the step's own locate semantics (A:680-693), 0-based, or -1 when the
+ * position is outside the mesh. */
+template <class P>
+__device__ __forceinline__ int32_t cell_of(const MeshK<P>& m, P x, P y, P z)
+{
+    P fv[3] = {fl((x - m.origin[0]) * m.rD[0]), fl((y - m.origin[1]) * m.rD[1]),
+               fl((z - m.origin[2]) * m.rD[2])};
+    int32_t g[3];
+    for (int a = 0; a < 3; ++a) {
+        if (!(fv[a] >= (P)-2147483648.0 && fv[a] < (P)2147483648.0)) return -1;
+        g[a] = (int32_t)fv[a];
+    }
+    int32_t q[3], r[3];
+    for (int a = 0; a < 3; ++a) {
+        q[a] = g[a] / m.N[a];
+        r[a] = g[a] - q[a] * m.N[a];
+    }
+    const int32_t part = abs(q[2]) + abs(q[1]) + abs(q[0]) + 1;
+    if (part != 1) return -1;
+    return abs(r[2]) * m.NxNy + abs(r[1]) * m.N[0] + abs(r[0]);
+}
+
+/* Owning cell of every parcel (cell_of), written at the parcel's st_set_parcels index; a
+ * count of the parcels outside the mesh. */
 template <class P>
 __global__ void k_cells(const P* __restrict__ x, const P* __restrict__ y,
                         const P* __restrict__ z, const int32_t* __restrict__ id, int64_t n,
@@ -180,31 +202,40 @@ __global__ void k_cells(const P* __restrict__ x, const P* __restrict__ y,
 {
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (int64_t)gridDim.x * blockDim.x) {
-        P fv[3] = {fl((x[p] - m.origin[0]) * m.rD[0]), fl((y[p] - m.origin[1]) * m.rD[1]),
-                   fl((z[p] - m.origin[2]) * m.rD[2])};
-        int32_t g[3];
-        bool bad = false;
-        for (int a = 0; a < 3; ++a) {
-            if (!(fv[a] >= (P)-2147483648.0 && fv[a] < (P)2147483648.0)) {
-                bad = true;
-                g[a] = 0;
-            } else {
-                g[a] = (int32_t)fv[a];
-            }
-        }
-        int32_t part = 1, pos = 0;
-        if (!bad) {
-            int32_t q[3], r[3];
-            for (int a = 0; a < 3; ++a) {
-                q[a] = g[a] / m.N[a];
-                r[a] = g[a] - q[a] * m.N[a];
-            }
-            part = abs(q[2]) + abs(q[1]) + abs(q[0]) + 1;
-            pos = abs(r[2]) * m.NxNy + abs(r[1]) * m.N[0] + abs(r[0]);
-        }
-        const bool out = bad || part != 1;
-        if (out && outside) atomicAdd(outside, 1ULL);
-        cells[id ? id[p] : p] = out ? -1 : pos;
+        const int32_t c = cell_of(m, x[p], y[p], z[p]);
+        if (c < 0 && outside) atomicAdd(outside, 1ULL);
+        cells[id ? id[p] : p] = c;
+    }
+}
+
+/* inv[id[p]] = p: the device position of every parcel by its st_set_parcels index */
+__global__ void k_inverse_ids(const int32_t* __restrict__ id, int64_t n, uint32_t* __restrict__ inv)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x)
+        inv[id[p]] = (uint32_t)p;
+}
+
+/* The parcels ids[0..m) (st_set_parcels indices): state in FP64, out = [6][m] (x, y, z, u,
+ * v, w), and the owning cell (the tracked tet when `cell` is given, else cell_of). */
+template <class P, class V>
+__global__ void k_sample(const uint32_t* __restrict__ inv, const int32_t* __restrict__ ids,
+                         int64_t m, const P* __restrict__ x, const P* __restrict__ y,
+                         const P* __restrict__ z, const V* __restrict__ u,
+                         const V* __restrict__ v, const V* __restrict__ w,
+                         const int32_t* __restrict__ cell, MeshK<P> mesh,
+                         double* __restrict__ out, int32_t* __restrict__ cells_out)
+{
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = inv[ids[j]];
+        out[j] = (double)x[p];
+        out[m + j] = (double)y[p];
+        out[2 * m + j] = (double)z[p];
+        out[3 * m + j] = (double)u[p];
+        out[4 * m + j] = (double)v[p];
+        out[5 * m + j] = (double)w[p];
+        cells_out[j] = cell ? cell[p] : cell_of(mesh, x[p], y[p], z[p]);
     }
 }
 
@@ -252,12 +283,124 @@ __global__ void k_bin_rank(const uint32_t* __restrict__ keys, int64_t n, uint32_
     }
 }
 
+/* Exclusive scan of the per-key counts (up to 2^24 of them): k_scan_reduce sums a contiguous
+ * chunk of the counts per block; k_scan_apply starts each block from the sum of the chunks
+ * before it and scans its chunk in tiles of SCAN_TILE counts (four per thread, a warp
+ * shuffle scan, then one over the warps' totals). */
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_TILE = 4 * SCAN_THREADS;
+constexpr int SCAN_BLOCKS = 2 * 148;
+
+/* sum of v over the block, returned to every thread */
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* wsum)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_WARP, v, o);
+    if (lane == 0) wsum[warp] = v;
+    __syncthreads();
+    uint32_t t = lane < nw ? wsum[lane] : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(FULL_WARP, t, o);
+    __syncthreads();
+    return t;
+}
+
+/* exclusive prefix of v over the block's threads; `total` = the block's sum */
+__device__ __forceinline__ uint32_t block_exclusive(uint32_t v, uint32_t* wsum, uint32_t& total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL_WARP, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? wsum[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL_WARP, w, o);
+            if (lane >= o) w += y;
+        }
+        wsum[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = warp ? wsum[warp - 1] : 0u;
+    total = wsum[nw - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const uint32_t* __restrict__ in,
+                                                              int64_t n, int64_t chunk,
+                                                              uint32_t* __restrict__ partials)
+{
+    __shared__ uint32_t wsum[32];
+    const int64_t begin = blockIdx.x * chunk;
+    const int64_t end = begin + chunk < n ? begin + chunk : n;
+    uint32_t v = 0;
+    for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) v += __ldcs(in + i);
+    v = block_sum(v, wsum);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const uint32_t* __restrict__ in,
+                                                             int64_t n, int64_t chunk,
+                                                             const uint32_t* __restrict__ partials,
+                                                             uint32_t* __restrict__ out)
+{
+    __shared__ uint32_t wsum[32];
+    uint32_t c = 0;
+    for (int j = threadIdx.x; j < (int)blockIdx.x; j += blockDim.x) c += partials[j];
+    uint32_t carry = block_sum(c, wsum);
+    const int64_t begin = blockIdx.x * chunk;
+    const int64_t end = begin + chunk < n ? begin + chunk : n;
+    for (int64_t t0 = begin; t0 < end; t0 += SCAN_TILE) {
+        const int64_t idx = t0 + 4 * (int64_t)threadIdx.x;
+        uint32_t v[4] = {0u, 0u, 0u, 0u};
+        if (idx + 4 <= end) {
+            const uint4 q = *reinterpret_cast<const uint4*>(in + idx);
+            v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+        } else {
+            for (int e = 0; e < 4; ++e)
+                if (idx + e < end) v[e] = in[idx + e];
+        }
+        uint32_t total;
+        uint32_t run = carry + block_exclusive((v[0] + v[1]) + (v[2] + v[3]), wsum, total);
+        uint32_t o[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            o[e] = run;
+            run += v[e];
+        }
+        if (idx + 4 <= end) {
+            *reinterpret_cast<uint4*>(out + idx) = make_uint4(o[0], o[1], o[2], o[3]);
+        } else {
+            for (int e = 0; e < 4; ++e)
+                if (idx + e < end) out[idx + e] = o[e];
+        }
+        carry += total;
+    }
+}
+
+/* out = exclusive scan of in[0..n); partials holds SCAN_BLOCKS counts */
+static cudaError_t scan_counts(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* partials,
+                               cudaStream_t s)
+{
+    int64_t chunk = (n + SCAN_BLOCKS - 1) / SCAN_BLOCKS;
+    chunk = (chunk + 3) / 4 * 4;   /* chunks start on 16-byte boundaries */
+    k_scan_reduce<<<SCAN_BLOCKS, SCAN_THREADS, 0, s>>>(in, n, chunk, partials);
+    k_scan_apply<<<SCAN_BLOCKS, SCAN_THREADS, 0, s>>>(in, n, chunk, partials, out);
+    return cudaGetLastError();
+}
+
 size_t count_sort_scan_bytes(int key_bits)
 {
-    size_t bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
-                                  (int)((int64_t)1 << key_bits));
-    return bytes;
+    (void)key_bits;
+    return SCAN_BLOCKS * sizeof(uint32_t);
 }
 
 static int grid_for(int64_t n)
@@ -299,12 +442,12 @@ cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& me
         const int wg = grid_for(n);
         k_bin_count<<<wg, 256, 0, s>>>(b.keys[0], n, (uint32_t)nbins, b.bins);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        size_t bytes = b.scan_temp_bytes;
-        e = cub::DeviceScan::ExclusiveSum(b.scan_temp, bytes, b.bins, b.offsets, (int)nbins, s);
-        if (e != cudaSuccess) return e;
+        if ((e = scan_counts(b.bins, b.offsets, nbins, static_cast<uint32_t*>(b.scan_temp),
+                             s)) != cudaSuccess)
+            return e;
         k_bin_rank<<<wg, 256, 0, s>>>(b.keys[0], n, (uint32_t)nbins, b.offsets, b.perm[1]);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if (launches) *launches += 2;
+        if (launches) *launches += 4;
     } else {
         size_t bytes = b.temp_bytes;
         e = cub::DeviceRadixSort::SortPairs(b.temp, bytes, b.keys[0], b.keys[1], b.perm[0],
@@ -344,6 +487,20 @@ cudaError_t cells_cloud(const P* x, const P* y, const P* z, const int32_t* id, i
     return cudaGetLastError();
 }
 
+template <class P, class V>
+cudaError_t sample_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& mesh,
+                         const int32_t* ids, int64_t m, double* out, int32_t* cells_out,
+                         cudaStream_t s)
+{
+    if (m == 0) return cudaSuccess;
+    /* the sort's permutation buffer is free between steps: it holds the inverse of the ids */
+    k_inverse_ids<<<grid_for(n), 256, 0, s>>>(b.id[cur], n, b.perm[0]);
+    k_sample<P, V><<<grid_for(m), 256, 0, s>>>(b.perm[0], ids, m, b.x[cur], b.y[cur], b.z[cur],
+                                               b.u[cur], b.v[cur], b.w[cur], b.cell[cur], mesh,
+                                               out, cells_out);
+    return cudaGetLastError();
+}
+
 cudaError_t cells_unpermute(const int32_t* id, const int32_t* cell, int64_t n, int32_t* out,
                             cudaStream_t s)
 {
@@ -356,7 +513,10 @@ cudaError_t cells_unpermute(const int32_t* id, const int32_t* cell, int64_t n, i
     template size_t sort_temp_bytes<P, V>(int64_t);                                           \
     template cudaError_t sort_cloud<P, V>(SortBufs<P, V>&, int, int64_t, const MeshK<P>&, int, \
                                           bool, cudaStream_t, int*);                          \
-    template cudaError_t unpermute_cloud<P, V>(SortBufs<P, V>&, int, int64_t, cudaStream_t);
+    template cudaError_t unpermute_cloud<P, V>(SortBufs<P, V>&, int, int64_t, cudaStream_t); \
+    template cudaError_t sample_cloud<P, V>(SortBufs<P, V>&, int, int64_t, const MeshK<P>&,    \
+                                            const int32_t*, int64_t, double*, int32_t*,        \
+                                            cudaStream_t);
 ST_INST(float, float)
 ST_INST(double, float)
 ST_INST(double, double)

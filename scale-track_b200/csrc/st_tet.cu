@@ -14,8 +14,10 @@
  *   n = (q - p) x (r - p), negated if n . (v_f - p) > 0, c = n . p; s_f(x) = n . x - c;
  *   inside iff all s_f <= 0; ties between faces go to the lowest index.
  * The two tets of a shared face therefore hold the same plane bit for bit up to an exact
- * negation: a point is never outside both, and no walk bounces between two tets.  A walk
- * step reads 128 bytes of planes (one dependent load level) and costs 24 FP64 operations.
+ * negation: a point is never outside both, and no walk bounces between two tets.  Every walk
+ * step first tests the tet with FP32 copies of its planes (64 bytes) and a proven rounding
+ * bound, which settles "inside" for all positions not within about 4e-7 of the plane scale
+ * of a face; only the other steps read the 128 bytes of FP64 planes (24 FP64 operations).
  * The same arithmetic, without fused multiply-adds, is in the CPU oracle, so owning tets agree
  * bit for bit.  A walk that reaches a boundary face or exceeds the hop limit marks the parcel
  * as lost (its state is left unchanged and the host reports it).  Deposits use the same
@@ -47,7 +49,8 @@ __device__ __forceinline__ void tet_signed(const TetMeshK& m, int32_t t, const d
  * increasing order), (p, q, r) the other three in increasing order, n = (q - p) x (r - p)
  * negated if n . (v_f - p) > 0, c = n . p. */
 __global__ void k_tet_planes(const double* __restrict__ verts, const int32_t* __restrict__ tets,
-                             int64_t nt, double4* __restrict__ planes)
+                             int64_t nt, double4* __restrict__ planes,
+                             float4* __restrict__ planes32)
 {
     const int F[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 4 * nt;
@@ -67,18 +70,48 @@ __global__ void k_tet_planes(const double* __restrict__ verts, const int32_t* __
         double n2 = a0 * b1 - a1 * b0;
         const double e = (n0 * (v[f][0] - p[0]) + n1 * (v[f][1] - p[1])) + n2 * (v[f][2] - p[2]);
         if (e > 0.0) { n0 = -n0; n1 = -n1; n2 = -n2; }
-        planes[i] = make_double4(n0, n1, n2, (n0 * p[0] + n1 * p[1]) + n2 * p[2]);
+        const double c = (n0 * p[0] + n1 * p[1]) + n2 * p[2];
+        planes[i] = make_double4(n0, n1, n2, c);
+        planes32[i] = make_float4((float)n0, (float)n1, (float)n2, (float)c);
     }
 }
 
 cudaError_t launch_tet_planes(const double* verts, const int32_t* tets, int64_t nt,
-                              double4* planes, cudaStream_t s)
+                              double4* planes, float4* planes32, cudaStream_t s)
 {
     if (nt == 0) return cudaSuccess;
     int64_t g = (4 * nt + 255) / 256;
     if (g > 148 * 32) g = 148 * 32;
-    k_tet_planes<<<(int)g, 256, 0, s>>>(verts, tets, nt, planes);
+    k_tet_planes<<<(int)g, 256, 0, s>>>(verts, tets, nt, planes, planes32);
     return cudaGetLastError();
+}
+
+/* FP32 pre-check of "x is inside tet t", read from the 64 bytes of FP32 planes instead of the
+ * 128 bytes of FP64 ones.  It returns true only when every FP64 signed distance is certainly
+ * negative, so the walk ends at t exactly where the FP64 test ends it; otherwise the walk
+ * takes the FP64 planes (positions near a face, and every tet the walk leaves).
+ *
+ * Bound: with u = 2^-24, n', c', x' the FP32 roundings of the FP64 plane and position, the FP32
+ * evaluation s' = ((n0'x0' + n1'x1') + n2'x2') - c' (no fused multiply-adds) differs from the
+ * exact s = n.x - c by at most gamma_6 S (Higham, Accuracy and Stability of Numerical
+ * Algorithms, 2nd ed., sec. 3.1: six roundings on the product terms, two on c), with
+ * S = sum |n_i x_i| + |c| and gamma_6 = 6u/(1 - 6u) < 3.6e-7; the FP64 evaluation differs
+ * from s by at most gamma_3 S in double (< 4e-16 S).  |x_i| <= xmax inside the box, so
+ * S <= (sum |n_i|) xmax + |c| <= (1 + 7u) times that sum formed in FP32 from n', c'.
+ * e = 4e-7 times the FP32 sum, plus 1e-37 for rounding near the subnormal range, therefore
+ * bounds |s' - s64|, and s' < -e implies s64 < 0. */
+__device__ __forceinline__ bool tet_inside32(const TetMeshK& m, int32_t t, const float x[3])
+{
+    const float4* pl = m.planes32 + 4 * (int64_t)t;
+    bool in = true;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        const float4 q = __ldg(pl + f);
+        const float s = ((q.x * x[0] + q.y * x[1]) + q.z * x[2]) - q.w;
+        const float S = ((fabsf(q.x) + fabsf(q.y)) + fabsf(q.z)) * m.xmax + fabsf(q.w);
+        in = in && (s < -(4.0e-7f * S + 1.0e-37f));
+    }
+    return in;
 }
 
 /* Greedy walk; at most hop_limit moves (bounded loop). */
@@ -86,7 +119,16 @@ __device__ __forceinline__ int32_t tet_walk(const TetMeshK& m, int32_t t, const 
                                             int hop_limit, int& status, int& hops)
 {
     hops = 0;
+    const float x32[3] = {(float)x[0], (float)x[1], (float)x[2]};
+    /* the pre-check's bound holds for positions with |x_i| <= xmax (every position inside
+     * the box); anything else goes straight to the FP64 test */
+    const bool pre = fabs(x[0]) <= (double)m.xmax && fabs(x[1]) <= (double)m.xmax &&
+                     fabs(x[2]) <= (double)m.xmax;
     for (int it = 0; it <= hop_limit; ++it) {
+        if (pre && tet_inside32(m, t, x32)) {
+            status = TWALK_OK;
+            return t;
+        }
         double s[4];
         tet_signed(m, t, x, s);
         int fb = 0;

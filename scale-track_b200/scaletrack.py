@@ -35,6 +35,7 @@ KERNEL_KINDS = {"step": 0, "finalize": 1, "sort": 2, "probe": 3, "other": 4,
 EXPORTS = [
     "st_version", "st_last_error", "st_params_default", "st_create", "st_destroy",
     "st_set_parcels", "st_get_parcels", "st_get_cells", "st_get_order", "st_num_parcels",
+    "st_get_parcel_sample",
     "st_num_cells",
     "st_set_fluid_velocity", "st_set_fluid_velocity_device", "st_step", "st_get_source",
     "st_source_device", "st_synchronize", "st_get_stream", "st_set_stream",
@@ -117,6 +118,9 @@ def lib():
                             ctypes.c_void_p], ctypes.c_int),
         "st_get_cells": ([c_h, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
         "st_get_order": ([c_h, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+        "st_get_parcel_sample": ([c_h, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                                 ctypes.c_int),
         "st_num_parcels": ([c_h, ctypes.c_int], ctypes.c_int64),
         "st_num_cells": ([c_h], ctypes.c_int64),
         "st_set_fluid_velocity": ([c_h, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
@@ -362,6 +366,17 @@ class ParcelTracker:
         if check:
             _check(rc)
         return cells
+
+    def get_parcel_sample(self, ids, cloud=0):
+        """(xyz [3, m], uvw [3, m], cells [m]) of the parcels with st_set_parcels indices ids"""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        m = ids.shape[0]
+        xyz = np.empty((3, m))
+        uvw = np.empty((3, m))
+        cells = np.empty(m, dtype=np.int32)
+        _check(lib().st_get_parcel_sample(self._h, cloud, m, _dptr(ids), _dptr(xyz), _dptr(uvw),
+                                          _dptr(cells)))
+        return xyz, uvw, cells
 
     def get_order(self, cloud=0):
         """ids[k]: st_set_parcels index of the parcel at device position k."""
