@@ -83,6 +83,8 @@ def parse():
                     help="time the tet mesh workload alone and print its object (profiling runs)")
     ap.add_argument("--no-clouds", dest="clouds", action="store_false",
                     help="skip the configuration-3 multi-cloud timing")
+    ap.add_argument("--clouds-only", action="store_true",
+                    help="time the 64-cloud workload alone and print its object (profiling runs)")
     return ap.parse_args()
 
 
@@ -837,7 +839,12 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.tets_only:
+    if a.clouds_only:
+        import torch
+        import scaletrack as st
+        torch.cuda.set_device(0)
+        print(json.dumps(run_clouds(st, torch, 0, torch.device("cuda", 0))), flush=True)
+    elif a.tets_only:
         import torch
         import scaletrack as st
         torch.cuda.set_device(0)

@@ -32,23 +32,35 @@
 
 namespace st {
 
-constexpr int RING_BT = 1024;                               /* parcels per block tile      */
-constexpr int RING_CONSUMERS = 16;                          /* consumer warps per block    */
+#ifndef ST_RING_BT
+#define ST_RING_BT 1024
+#endif
+#ifndef ST_RING_CONSUMERS
+#define ST_RING_CONSUMERS 16
+#endif
+#ifndef ST_RING_MAX_NS
+#define ST_RING_MAX_NS 4
+#endif
+constexpr int RING_BT = ST_RING_BT;                         /* parcels per block tile      */
+constexpr int RING_CONSUMERS = ST_RING_CONSUMERS;           /* consumer warps per block    */
 constexpr int RING_THREADS = 32 * (RING_CONSUMERS + 1);     /* + one producer warp         */
 constexpr int RING_SPW = RING_BT / (32 * RING_CONSUMERS);   /* slices per warp and tile    */
 constexpr long long RING_WAIT_CYCLES = 2000000000LL;        /* about 1 s at 1.9 GHz        */
-constexpr int RING_MAX_NS = 4;
+constexpr int RING_MAX_NS = ST_RING_MAX_NS;
 
 template <class P, class V>
 struct RingGeom {
     static constexpr uint32_t SP = RING_BT * sizeof(P);     /* bytes of one position array */
     static constexpr uint32_t SV = RING_BT * sizeof(V);     /* bytes of one velocity array */
     static constexpr uint32_t STAGE = 3 * SP + 4 * SV;
-    static constexpr int NS = (RING_MAX_NS * STAGE <= 200u * 1024u) ? RING_MAX_NS : 3;
+    static constexpr int NS = (RING_MAX_NS * STAGE <= 200u * 1024u)
+                                  ? RING_MAX_NS
+                                  : (int)((200u * 1024u) / STAGE);
     static constexpr uint32_t SMEM = NS * STAGE;
 };
 static_assert(RING_SPW * 32 * RING_CONSUMERS == RING_BT, "tile split");
 static_assert(RingGeom<double, double>::SMEM <= 227u * 1024u, "shared memory");
+static_assert(RingGeom<double, double>::NS >= 2, "at least two stages");
 
 /* ------------------------------------------------------------------------------------ */
 /* mbarrier and bulk-copy primitives (PTX)                                              */
