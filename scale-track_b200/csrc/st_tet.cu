@@ -165,6 +165,121 @@ __device__ __forceinline__ int tet_find_cloud(const TetStepArgs<V>& a, int64_t t
     return lo;
 }
 
+/* walk-length histogram of a block (flushed once at the end of the step kernel) */
+__shared__ unsigned s_tet_hist[8];
+
+/* One parcel through the substeps on a tet mesh (evolve_particle!, A:1271-1365, with the
+ * face walk for relocation) after its state has been read: pos, vel and cell (its owning
+ * tet) are updated in place unless the parcel is lost (then they are left as they were);
+ * the final deposit is returned in (key, dep) for the warp reduction, intermediate deposits
+ * (substeps > 1) go straight to memory.  With count_hops, walk lengths go to the block's
+ * histogram s_tet_hist. */
+template <class V, int DEP>
+__device__ __forceinline__ void tet_parcel(const TetStepArgs<V>& a, int nsub, double pos[3],
+                                           V vel[3], V d, int32_t& cell,
+                                           unsigned long long* acc, double* src,
+                                           const Quant& qp, AmaxT<V>& amax, unsigned& ovf,
+                                           bool& lost, int32_t& key, V dep[3], bool count_hops)
+{
+    const PhysK<V>& ph = a.phys;
+    int32_t cur = cell;
+    const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
+    const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
+    constexpr bool MIX = is_mixed<double, V>;
+    const V* Uc = a.U + 3 * (int64_t)cur;
+    V Ur[3] = {__ldg(Uc), __ldg(Uc + 1), __ldg(Uc + 2)};
+    /* deposit forms of the hex step (st_kernels.cu evolve_parcel): FP32/FP64 carry
+     * state0, mixed precision carries D = state0 - v */
+    V state0[3] = {vel[0], vel[1], vel[2]};
+    V D[3] = {(V)0, (V)0, (V)0};
+    double posNew[3] = {pos[0], pos[1], pos[2]};
+    V velNew[3] = {vel[0], vel[1], vel[2]};
+    int32_t tNew = cur;
+    lost = false;
+    for (int t = 1; t <= nsub; ++t) {
+        V inc[3];
+        if (ph.drag == 0) {
+            if constexpr (MIX) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    inc[k] = (f * slip<MIX>(Ur[k], a.fscale, a.fscale_lo, vel[k])) /
+                             ((V)1 + f);
+                    velNew[k] = vel[k] + inc[k];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    velNew[k] = (vel[k] + f * (Ur[k] * a.fscale)) / ((V)1 + f);
+            }
+        } else {
+            V du[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                du[k] = slip<MIX>(Ur[k], a.fscale, a.fscale_lo, vel[k]);
+            V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
+            V Re = (mag * d) * ph.rnu;
+            V pw;
+            if (sizeof(V) == 4) pw = (V)st_pow0687f((float)Re);
+            else pw = (V)st_pow0687((double)Re);
+            V g = f * ((V)1 + (V)0.15 * pw);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                inc[k] = g * du[k];
+                velNew[k] = vel[k] + inc[k];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (double)velNew[k] * a.dtP;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (posNew[k] < a.mesh.origin[k] || posNew[k] > a.mesh.ending[k]) {
+                posNew[k] = pos[k];
+                velNew[k] = -vel[k];
+                if constexpr (!MIX) state0[k] -= (V)2 * vel[k];
+            } else if constexpr (MIX) {
+                D[k] -= inc[k];
+            }
+        }
+        int status = TWALK_OK, hops = 0;
+        tNew = tet_walk(a.mesh, tNew, posNew, a.mesh.hop_limit, status, hops);
+        if (status != TWALK_OK) { lost = true; break; }
+        if (count_hops) atomicAdd(&s_tet_hist[hops < 7 ? hops : 7], 1u);
+        if (t != nsub && tNew != cur) {
+            V di[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                di[k] = MIX ? mB * D[k] : mB * (state0[k] - velNew[k]);
+            if (DEP == DEP_PROBE) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) track_max(di[k], amax);
+            } else {
+                deposit_direct<DEP, V>(di, (int64_t)cur, acc, src, qp, amax, ovf);
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                state0[k] = velNew[k];
+                D[k] = (V)0;
+            }
+            const V* Un = a.U + 3 * (int64_t)tNew;
+            Ur[0] = __ldg(Un);
+            Ur[1] = __ldg(Un + 1);
+            Ur[2] = __ldg(Un + 2);
+            cur = tNew;
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { vel[k] = velNew[k]; pos[k] = posNew[k]; }
+    }
+    if (lost) return;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        dep[k] = MIX ? mB * D[k] : mB * (state0[k] - velNew[k]);
+        pos[k] = posNew[k];
+        vel[k] = velNew[k];
+    }
+    key = cur;
+    cell = tNew;
+}
+
 /* Resident blocks of 256 threads per SM the compiler must allow: 4 (64 registers). */
 #ifndef ST_TET_MIN_BLOCKS
 #define ST_TET_MIN_BLOCKS 4
@@ -187,10 +302,8 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
     AmaxT<V> amax = (V)0;
     unsigned ovf = 0, nlost = 0;
     const int nsub = ONE ? 1 : ph.nsub;
-    /* walk-length histogram of the block, flushed once at the end */
-    __shared__ unsigned s_hist[8];
     const bool count_hops = a.hop_hist != nullptr && DEP != DEP_PROBE;
-    if (threadIdx.x < 8) s_hist[threadIdx.x] = 0;
+    if (threadIdx.x < 8) s_tet_hist[threadIdx.x] = 0;
     __syncthreads();
 
     for (int64_t tile = warp0; tile < a.total_tiles; tile += nwarps) {
@@ -212,112 +325,24 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
             double pos[3] = {ld_stream(cl->x + i), ld_stream(cl->y + i), ld_stream(cl->z + i)};
             V vel[3] = {ld_stream(cl->u + i), ld_stream(cl->v + i), ld_stream(cl->w + i)};
             const V d = ld_stream(cl->d + i) * ph.dscale;
-            int32_t cur = ld_stream(cl->cell + i);
-            /* the first walk step reads this tet's planes: start that line towards L1 now,
-             * alongside the cell-velocity gather */
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(a.mesh.planes + 4 * (int64_t)cur));
-            const V mB = ((ph.rr * (V)3.14159265358979323846) * ((d * d) * d)) / (V)6;
-            const V f = ((((V)18 * ph.mu) * a.dtV) / (ph.rho_d * (d * d))) * ph.alpha;
-            constexpr bool MIX = is_mixed<double, V>;
-            const V* Uc = a.U + 3 * (int64_t)cur;
-            V Ur[3] = {__ldg(Uc), __ldg(Uc + 1), __ldg(Uc + 2)};
-            /* deposit forms of the hex step (st_kernels.cu evolve_parcel): FP32/FP64 carry
-             * state0, mixed precision carries D = state0 - v */
-            V state0[3] = {vel[0], vel[1], vel[2]};
-            V D[3] = {(V)0, (V)0, (V)0};
-            double posNew[3] = {pos[0], pos[1], pos[2]};
-            V velNew[3] = {vel[0], vel[1], vel[2]};
-            int32_t tNew = cur;
+            int32_t cell = ld_stream(cl->cell + i);
+            /* the first walk step reads this tet's FP32 planes: start that line towards L1
+             * now, alongside the cell-velocity gather */
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(a.mesh.planes32 + 4 * (int64_t)cell));
             bool lost = false;
-            for (int t = 1; t <= nsub; ++t) {
-                V inc[3];
-                if (ph.drag == 0) {
-                    if constexpr (MIX) {
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            inc[k] = (f * slip<MIX>(Ur[k], a.fscale, a.fscale_lo, vel[k])) /
-                                     ((V)1 + f);
-                            velNew[k] = vel[k] + inc[k];
-                        }
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < 3; ++k)
-                            velNew[k] = (vel[k] + f * (Ur[k] * a.fscale)) / ((V)1 + f);
-                    }
-                } else {
-                    V du[3];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k)
-                        du[k] = slip<MIX>(Ur[k], a.fscale, a.fscale_lo, vel[k]);
-                    V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
-                    V Re = (mag * d) * ph.rnu;
-                    V pw;
-                    if (sizeof(V) == 4) pw = (V)st_pow0687f((float)Re);
-                    else pw = (V)st_pow0687((double)Re);
-                    V g = f * ((V)1 + (V)0.15 * pw);
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        inc[k] = g * du[k];
-                        velNew[k] = vel[k] + inc[k];
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < 3; ++k) posNew[k] = pos[k] + (double)velNew[k] * a.dtP;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    if (posNew[k] < a.mesh.origin[k] || posNew[k] > a.mesh.ending[k]) {
-                        posNew[k] = pos[k];
-                        velNew[k] = -vel[k];
-                        if constexpr (!MIX) state0[k] -= (V)2 * vel[k];
-                    } else if constexpr (MIX) {
-                        D[k] -= inc[k];
-                    }
-                }
-                int status = TWALK_OK, hops = 0;
-                tNew = tet_walk(a.mesh, tNew, posNew, a.mesh.hop_limit, status, hops);
-                if (status != TWALK_OK) { lost = true; break; }
-                if (count_hops) atomicAdd(&s_hist[hops < 7 ? hops : 7], 1u);
-                if (t != nsub && tNew != cur) {
-                    V di[3];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k)
-                        di[k] = MIX ? mB * D[k] : mB * (state0[k] - velNew[k]);
-                    if (DEP == DEP_PROBE) {
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) track_max(di[k], amax);
-                    } else {
-                        deposit_direct<DEP, V>(di, (int64_t)cur, acc, src, qp, amax, ovf);
-                    }
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        state0[k] = velNew[k];
-                        D[k] = (V)0;
-                    }
-                    const V* Un = a.U + 3 * (int64_t)tNew;
-                    Ur[0] = __ldg(Un);
-                    Ur[1] = __ldg(Un + 1);
-                    Ur[2] = __ldg(Un + 2);
-                    cur = tNew;
-                }
-#pragma unroll
-                for (int k = 0; k < 3; ++k) { vel[k] = velNew[k]; pos[k] = posNew[k]; }
-            }
+            tet_parcel<V, DEP>(a, nsub, pos, vel, d, cell, acc, src, qp, amax, ovf, lost, key,
+                               dep, count_hops);
             if (lost) {
                 ++nlost;
-            } else {
-                if (DEP != DEP_PROBE) {
-                    st_stream(cl->x + i, posNew[0]);
-                    st_stream(cl->y + i, posNew[1]);
-                    st_stream(cl->z + i, posNew[2]);
-                    st_stream(cl->u + i, velNew[0]);
-                    st_stream(cl->v + i, velNew[1]);
-                    st_stream(cl->w + i, velNew[2]);
-                    st_stream(cl->cell + i, tNew);
-                }
-                key = cur;
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    dep[k] = MIX ? mB * D[k] : mB * (state0[k] - velNew[k]);
+                key = -1;
+            } else if (DEP != DEP_PROBE) {
+                st_stream(cl->x + i, pos[0]);
+                st_stream(cl->y + i, pos[1]);
+                st_stream(cl->z + i, pos[2]);
+                st_stream(cl->u + i, vel[0]);
+                st_stream(cl->v + i, vel[1]);
+                st_stream(cl->w + i, vel[2]);
+                st_stream(cl->cell + i, cell);
             }
         }
         deposit_warp<DEP, V>(key, dep, acc, src, qp, lane, amax, ovf);
@@ -325,8 +350,8 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
     }
     if (cur_cloud >= 0) flush_ctl<DEP>(a.ctl + cur_cloud, lane, amax, ovf, nlost);
     __syncthreads();
-    if (count_hops && threadIdx.x < 8 && s_hist[threadIdx.x])
-        atomicAdd(a.hop_hist + threadIdx.x, (unsigned long long)s_hist[threadIdx.x]);
+    if (count_hops && threadIdx.x < 8 && s_tet_hist[threadIdx.x])
+        atomicAdd(a.hop_hist + threadIdx.x, (unsigned long long)s_tet_hist[threadIdx.x]);
 }
 
 template <class V, bool ONE>
