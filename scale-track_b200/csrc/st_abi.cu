@@ -38,6 +38,10 @@
 
 using namespace st;
 
+#ifndef ST_FINALIZE_CLEARS
+#define ST_FINALIZE_CLEARS 0
+#endif
+
 /* ------------------------------------------------------------------------------------ */
 /* errors                                                                               */
 /* ------------------------------------------------------------------------------------ */
@@ -504,7 +508,9 @@ int step_phases(st_handle* h, double dt, int phase, bool empty, L&& launch, S&& 
                                h->stride, finalize_grid(h), h->stream));
             h->launches += 1;
         }
+#if !ST_FINALIZE_CLEARS
         CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * nc * h->limbs * 8, h->stream));
+#endif
     }
     h->steps += 1;
     h->steps_since_sort += 1;

@@ -15,9 +15,9 @@
  *   inside iff all s_f <= 0; ties between faces go to the lowest index.
  * The two tets of a shared face therefore hold the same plane bit for bit up to an exact
  * negation: a point is never outside both, and no walk bounces between two tets.  Every walk
- * step first tests the tet with FP32 copies of its planes (64 bytes) and a proven rounding
- * bound, which settles "inside" for all positions not within about 4e-7 of the plane scale
- * of a face; only the other steps read the 128 bytes of FP64 planes (24 FP64 operations).
+ * step is first decided from FP32 copies of the tet's planes (64 bytes) with a proven rounding
+ * bound, which settles "inside" and "leave through face f" except within about 4e-7 of the
+ * plane scale of a face or of a tie; only those steps read the 128 bytes of FP64 planes.
  * The same arithmetic, without fused multiply-adds, is in the CPU oracle, so owning tets agree
  * bit for bit.  A walk that reaches a boundary face or exceeds the hop limit marks the parcel
  * as lost (its state is left unchanged and the host reports it).  Deposits use the same
@@ -86,10 +86,12 @@ cudaError_t launch_tet_planes(const double* verts, const int32_t* tets, int64_t 
     return cudaGetLastError();
 }
 
-/* FP32 pre-check of "x is inside tet t", read from the 64 bytes of FP32 planes instead of the
- * 128 bytes of FP64 ones.  It returns true only when every FP64 signed distance is certainly
- * negative, so the walk ends at t exactly where the FP64 test ends it; otherwise the walk
- * takes the FP64 planes (positions near a face, and every tet the walk leaves).
+/* One walk step at tet t decided from the FP32 copies of its planes (64 bytes instead of
+ * the 128 bytes of FP64 ones).  Returns 1 when x is certainly inside t (every FP64 signed
+ * distance negative), 2 when the FP64 test certainly leaves through face fb (its signed
+ * distance positive and strictly the largest, so no tie rule applies), 0 when FP32 cannot
+ * decide and the walk must evaluate the FP64 planes.  Where it decides, it decides exactly
+ * as the FP64 step does.
  *
  * Bound: with u = 2^-24, n', c', x' the FP32 roundings of the FP64 plane and position, the FP32
  * evaluation s' = ((n0'x0' + n1'x1') + n2'x2') - c' (no fused multiply-adds) differs from the
@@ -99,46 +101,64 @@ cudaError_t launch_tet_planes(const double* verts, const int32_t* tets, int64_t 
  * from s by at most gamma_3 S in double (< 4e-16 S).  |x_i| <= xmax inside the box, so
  * S <= (sum |n_i|) xmax + |c| <= (1 + 7u) times that sum formed in FP32 from n', c'.
  * e = 4e-7 times the FP32 sum, plus 1e-37 for rounding near the subnormal range, therefore
- * bounds |s' - s64|, and s' < -e implies s64 < 0. */
-__device__ __forceinline__ bool tet_inside32(const TetMeshK& m, int32_t t, const float x[3])
+ * bounds |s' - s64| with a 10 % margin, which also covers the roundings of the comparisons
+ * below: s' < -e gives s64 < 0, s' > e gives s64 > 0, and s'_b - s'_f > e_b + e_f gives
+ * s64_f < s64_b. */
+__device__ __forceinline__ int tet_step32(const TetMeshK& m, int32_t t, const float x[3], int& fb)
 {
     const float4* pl = m.planes32 + 4 * (int64_t)t;
+    float s[4], e[4];
     bool in = true;
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
         const float4 q = __ldg(pl + f);
-        const float s = ((q.x * x[0] + q.y * x[1]) + q.z * x[2]) - q.w;
-        const float S = ((fabsf(q.x) + fabsf(q.y)) + fabsf(q.z)) * m.xmax + fabsf(q.w);
-        in = in && (s < -(4.0e-7f * S + 1.0e-37f));
+        s[f] = ((q.x * x[0] + q.y * x[1]) + q.z * x[2]) - q.w;
+        e[f] = 4.0e-7f * (((fabsf(q.x) + fabsf(q.y)) + fabsf(q.z)) * m.xmax + fabsf(q.w)) +
+               1.0e-37f;
+        in = in && (s[f] < -e[f]);
     }
-    return in;
+    if (in) return 1;
+    int b = 0;
+#pragma unroll
+    for (int f = 1; f < 4; ++f)
+        if (s[f] > s[b]) b = f;
+    if (!(s[b] > e[b])) return 0;
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+        if (f != b && !(s[b] - s[f] > e[b] + e[f])) return 0;
+    fb = b;
+    return 2;
 }
 
-/* Greedy walk; at most hop_limit moves (bounded loop). */
+/* Greedy walk; at most hop_limit moves (bounded loop).  Each step is decided in FP32 where
+ * tet_step32 can, else from the FP64 planes; both give the FP64 walk's tets and hops. */
 __device__ __forceinline__ int32_t tet_walk(const TetMeshK& m, int32_t t, const double x[3],
                                             int hop_limit, int& status, int& hops)
 {
     hops = 0;
     const float x32[3] = {(float)x[0], (float)x[1], (float)x[2]};
-    /* the pre-check's bound holds for positions with |x_i| <= xmax (every position inside
-     * the box); anything else goes straight to the FP64 test */
+    /* the FP32 bound holds for positions with |x_i| <= xmax (every position inside the box);
+     * anything else goes straight to the FP64 test */
     const bool pre = fabs(x[0]) <= (double)m.xmax && fabs(x[1]) <= (double)m.xmax &&
                      fabs(x[2]) <= (double)m.xmax;
     for (int it = 0; it <= hop_limit; ++it) {
-        if (pre && tet_inside32(m, t, x32)) {
+        int fb = 0;
+        const int r = pre ? tet_step32(m, t, x32, fb) : 0;
+        if (r == 1) {
             status = TWALK_OK;
             return t;
         }
-        double s[4];
-        tet_signed(m, t, x, s);
-        int fb = 0;
-        double smax = s[0];
+        if (r == 0) {
+            double s[4];
+            tet_signed(m, t, x, s);
+            double smax = s[0];
 #pragma unroll
-        for (int f = 1; f < 4; ++f)
-            if (s[f] > smax) { smax = s[f]; fb = f; }
-        if (!(smax > 0.0)) {
-            status = TWALK_OK;
-            return t;
+            for (int f = 1; f < 4; ++f)
+                if (s[f] > smax) { smax = s[f]; fb = f; }
+            if (!(smax > 0.0)) {
+                status = TWALK_OK;
+                return t;
+            }
         }
         const int32_t nb = __ldg(m.nbr + 4 * (int64_t)t + fb);
         if (nb < 0) {
