@@ -38,10 +38,6 @@
 
 using namespace st;
 
-#ifndef ST_FINALIZE_CLEARS
-#define ST_FINALIZE_CLEARS 0
-#endif
-
 /* ------------------------------------------------------------------------------------ */
 /* errors                                                                               */
 /* ------------------------------------------------------------------------------------ */
@@ -508,9 +504,7 @@ int step_phases(st_handle* h, double dt, int phase, bool empty, L&& launch, S&& 
                                h->stride, finalize_grid(h), h->stream));
             h->launches += 1;
         }
-#if !ST_FINALIZE_CLEARS
         CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * nc * h->limbs * 8, h->stream));
-#endif
     }
     h->steps += 1;
     h->steps_since_sort += 1;

@@ -252,9 +252,6 @@ template int step_max_active_blocks<double, double>(int, int);
 /* source finalize: fixed point -> FP64, clear accumulators, next scale                 */
 /* ------------------------------------------------------------------------------------ */
 
-#ifndef ST_FINALIZE_CLEARS
-#define ST_FINALIZE_CLEARS 0
-#endif
 template <int LIMBS>
 __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict__ acc,
                                                   double* __restrict__ src,
@@ -278,10 +275,6 @@ __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict
         if (LIMBS == 1) {
             ulonglong2 q0 = __ldcs(a + 2 * g);
             ulonglong2 q1 = __ldcs(a + 2 * g + 1);
-#if ST_FINALIZE_CLEARS
-            const_cast<ulonglong2*>(a)[2 * g] = make_ulonglong2(0ULL, 0ULL);
-            const_cast<ulonglong2*>(a)[2 * g + 1] = make_ulonglong2(0ULL, 0ULL);
-#endif
             v[0] = (double)(long long)q0.x;
             v[1] = (double)(long long)q0.y;
             v[2] = (double)(long long)q1.x;
@@ -290,11 +283,6 @@ __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict
             ulonglong2 q[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) q[k] = __ldcs(a + 4 * g + k);
-#if ST_FINALIZE_CLEARS
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                const_cast<ulonglong2*>(a)[4 * g + k] = make_ulonglong2(0ULL, 0ULL);
-#endif
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 long long hi = (long long)q[k].x;
