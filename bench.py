@@ -85,6 +85,8 @@ def parse():
                     help="skip the configuration-3 multi-cloud timing")
     ap.add_argument("--clouds-only", action="store_true",
                     help="time the 64-cloud workload alone and print its object (profiling runs)")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="with --clouds-only: skip the autotuner (profiling runs)")
     return ap.parse_args()
 
 
@@ -560,7 +562,7 @@ def accuracy(st, xyz, uvw, d, U, mesh, local, steps, dt, fs):
     return out
 
 
-def run_clouds(st, torch, local, dev):
+def run_clouds(st, torch, local, dev, tune=True):
     """64 clouds with log-uniform sizes on a 64^3 mesh, each with its own
     source, one persistent launch per step; block size and re-sort interval from the
     autotuner; the step sequence replayed from a captured CUDA graph."""
@@ -577,7 +579,11 @@ def run_clouds(st, torch, local, dev):
             xyz, uvw, d = workload.parcels(int(sizes[k]), 1000 + k, d_median=float(dmed[k]))
             h.set_parcels(xyz, uvw, d, cloud=k)
         h.set_fluid_velocity(U)
-        tune = h.autotune(workload.DT, trial_steps=40)
+        if tune:
+            tune = h.autotune(workload.DT, trial_steps=40)
+        else:   # profiling runs: the handle's defaults, no trial launches
+            tune = {"block_size": prm.block_size or 256, "sort_interval": prm.sort_interval,
+                    "note": "autotuner skipped"}
         si = tune["sort_interval"]
         chunk = 2 * si if si else 20
         timer = DeviceTimer(torch, h.stream(), dev)
@@ -843,7 +849,7 @@ if __name__ == "__main__":
         import torch
         import scaletrack as st
         torch.cuda.set_device(0)
-        print(json.dumps(run_clouds(st, torch, 0, torch.device("cuda", 0))), flush=True)
+        print(json.dumps(run_clouds(st, torch, 0, torch.device("cuda", 0), a.tune)), flush=True)
     elif a.tets_only:
         import torch
         import scaletrack as st

@@ -61,13 +61,18 @@ __device__ __forceinline__ int find_cloud(const StepArgs<P, V>& a, int64_t tile)
 #ifndef ST_MIN_BLOCKS_FP64
 #define ST_MIN_BLOCKS_FP64 3
 #endif
-template <class V>
+/* Several substeps per call (the multi-cloud workload) keep more state live per parcel. */
+#ifndef ST_MIN_BLOCKS_SUB
+#define ST_MIN_BLOCKS_SUB 3
+#endif
+template <class V, bool ONE>
 struct MinBlocks {
-    static constexpr int value = sizeof(V) == 8 ? ST_MIN_BLOCKS_FP64 : ST_MIN_BLOCKS;
+    static constexpr int value =
+        sizeof(V) == 8 ? ST_MIN_BLOCKS_FP64 : (ONE ? ST_MIN_BLOCKS : ST_MIN_BLOCKS_SUB);
 };
 
 template <class P, class V, int DEP, bool ONE, bool SINGLE>
-__global__ void __launch_bounds__(256, MinBlocks<V>::value) k_step(const StepArgs<P, V> a)
+__global__ void __launch_bounds__(256, MinBlocks<V, ONE>::value) k_step(const StepArgs<P, V> a)
 {
     const int lane = threadIdx.x & 31;
     const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
