@@ -192,6 +192,16 @@ def ncu_traffic_per_parcel(precision):
         return None
 
 
+def ncu_tet_traffic():
+    """DRAM bytes per launch of the tet step kernel from a committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "k_step_traffic.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["tets"]["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
 def ncu_instructions_per_parcel_substep(workload_name):
     """Warp instructions per parcel and substep of a step kernel, from a committed ncu
     summary (profiles/instructions.json), or None."""
@@ -345,7 +355,7 @@ def run_ours(args):
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
                 "traffic": None if tpp is None else round(tpp * npcl),
-                "kernel": "k_step<double,float,DET1>", "peak_source": peak_src,
+                "kernel": "k_step_ring<double,float,DET1,1 substep>", "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": algo_step,
                 "avg_launch_ms": round(step_avg_ms, 5)}
     whole_step_frac = workload.algorithmic_bytes("mixed", npcl, ncells) / (ms_per_step / 1e3) \
@@ -710,6 +720,7 @@ def run_tets(st, torch, local, dev, steps, npcl=None):
                           "sort_per_call": round(sort_ms / max(nsort, 1), 5),
                           "finalize": round(fin_ms / max(nfin, 1), 5)},
             "roofline_step": {"bound": "hbm", "algorithmic_bytes_per_launch": algo,
+                              "traffic": ncu_tet_traffic(),
                               "achieved": round(algo / (step_avg / 1e3) / 1e9, 1),
                               "peak": peak, "unit": "GB/s", "peak_source": peak_src,
                               "frac": round(algo / (step_avg / 1e3) / 1e9 / peak, 4)},

@@ -150,7 +150,9 @@ ST_API int st_step(st_handle* h, double dt, double fluid_scale);
  * components: the sum over deposits of (rho_d/rho_c)(pi d^3/6)(state0 - v) (A:703-725),
  * not divided by the cell volume or dt, exactly as the reference's UTrans.  Synchronous. */
 ST_API int st_get_source(st_handle* h, int cloud, void* S, int elem_bytes);
-/* Device pointer to the FP64 source [nCells][3] of `cloud`, valid until st_destroy. */
+/* Device pointer to the FP64 source [nCells][3] of `cloud`, valid until st_destroy.  The
+ * call orders the handle's stream after the computation of the last step's source (see
+ * st_set_finalize_overlap): work enqueued on that stream afterwards reads it complete. */
 ST_API const double* st_source_device(st_handle* h, int cloud);
 
 /* Waits for the handle's stream and reports device-side errors. */
@@ -238,6 +240,15 @@ ST_API int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result*
  * reference (one kernel, A:1258-1269). */
 enum { ST_STEP_KERNEL_RING = 0, ST_STEP_KERNEL_WARP = 1 };
 ST_API int st_set_step_kernel(st_handle* h, int kind);
+/* With one cloud and the deterministic deposit, a step's conversion of the fixed-point sums
+ * to the FP64 source (and the clearing of its accumulator) runs on a second stream of the
+ * library, concurrent with the next step on the handle's stream; the two steps use two
+ * accumulators in turn.  st_get_source, st_synchronize and st_source_device order the
+ * handle's stream after it, so work the caller enqueues on that stream afterwards sees the
+ * source.  on = 0 runs the conversion in the handle's stream after each step instead (as
+ * graph capture, several clouds, tet meshes, the sharded phases and the coupling shims always
+ * do).  Results do not depend on the choice.  Default: on. */
+ST_API int st_set_finalize_overlap(st_handle* h, int on);
 
 /* ---- instrumentation --------------------------------------------------------------- */
 enum { ST_KERNEL_STEP = 0, ST_KERNEL_FINALIZE = 1, ST_KERNEL_SORT = 2, ST_KERNEL_PROBE = 3,

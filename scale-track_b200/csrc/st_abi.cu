@@ -150,6 +150,18 @@ struct st_handle {
     int32_t* dexp = nullptr;   /* [nclouds] largest-deposit exponents of a sharded step */
     float* dsrc32 = nullptr;   /* when set, the finalize also writes the FP32 source here
                                   ([nclouds][stride]; the coupling's 4-byte exchange) */
+    /* Overlapped finalize (one cloud, deterministic deposit, outside graph capture and the
+     * sharded phases): step n deposits into accumulator par, k_next_scale keeps its scale in
+     * dLfin[par] and sets the next one, and the finalize and clearing of accumulator par run
+     * on fin_stream while step n + 1 runs on the handle's stream with the other accumulator. */
+    bool fin_overlap = true;
+    cudaStream_t fin_stream = nullptr;
+    cudaEvent_t ev_step[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fin[2] = {nullptr, nullptr};
+    bool fin_pending[2] = {false, false};
+    int par = 0;
+    unsigned long long* dacc2 = nullptr;
+    int32_t* dLfin = nullptr;  /* [2][nclouds] */
     bool shard_probed = false; /* st_shard_probe ran; its exponents are in dexp */
     int key_bits = 32;
     bool morton = true;
@@ -262,12 +274,14 @@ cudaEvent_t take_event(st_handle* h)
 struct ProfScope {
     st_handle* h;
     int kind;
+    cudaStream_t s;
     cudaEvent_t a = nullptr;
-    ProfScope(st_handle* hh, int k) : h(hh), kind(k)
+    ProfScope(st_handle* hh, int k, cudaStream_t st = nullptr)
+        : h(hh), kind(k), s(st ? st : hh->stream)
     {
         if (h->prof) {
             a = take_event(h);
-            if (a && cudaEventRecord(a, h->stream) != cudaSuccess) {
+            if (a && cudaEventRecord(a, s) != cudaSuccess) {
                 cudaGetLastError();
                 h->pool.push_back(a);
                 a = nullptr;
@@ -279,7 +293,7 @@ struct ProfScope {
         /* a launch whose events could not be recorded is left out of the profile */
         if (h->prof && a) {
             cudaEvent_t b = take_event(h);
-            if (b && cudaEventRecord(b, h->stream) == cudaSuccess) {
+            if (b && cudaEventRecord(b, s) == cudaSuccess) {
                 h->recs.push_back({kind, a, b});
                 return;
             }
@@ -300,6 +314,46 @@ int finalize_grid(const st_handle* h)
     if (gx > cap) gx = cap;
     if (gx < 1) gx = 1;
     return (int)gx;
+}
+
+/* Orders the handle's stream after every finalize still pending on fin_stream: the source
+ * and both accumulators are then final on the handle's stream. */
+int join_fin(st_handle* h)
+{
+    for (int p = 0; p < 2; ++p)
+        if (h->fin_pending[p]) {
+            CK(cudaStreamWaitEvent(h->stream, h->ev_fin[p], 0));
+            h->fin_pending[p] = false;
+        }
+    return ST_OK;
+}
+
+/* Waits on the host for the finalize stream (before the handle's stream changes, a graph is
+ * captured or the handle goes away). */
+int drain_fin(st_handle* h)
+{
+    if (h->fin_stream) CK(cudaStreamSynchronize(h->fin_stream));
+    h->fin_pending[0] = h->fin_pending[1] = false;
+    return ST_OK;
+}
+
+/* The second accumulator, scale slots, stream and events of the overlapped finalize, made on
+ * the first overlapped step. */
+int ensure_overlap(st_handle* h)
+{
+    if (h->fin_stream) return ST_OK;
+    const size_t bytes = (size_t)h->stride * h->p.n_clouds * h->limbs * 8;
+    if (!h->dacc2) {
+        CK(cudaMalloc((void**)&h->dacc2, bytes));
+        CK(cudaMemsetAsync(h->dacc2, 0, bytes, h->stream));
+    }
+    if (!h->dLfin) CK(cudaMalloc((void**)&h->dLfin, 2 * sizeof(int32_t) * h->p.n_clouds));
+    for (int p = 0; p < 2; ++p) {
+        if (!h->ev_step[p]) CK(cudaEventCreateWithFlags(&h->ev_step[p], cudaEventDisableTiming));
+        if (!h->ev_fin[p]) CK(cudaEventCreateWithFlags(&h->ev_fin[p], cudaEventDisableTiming));
+    }
+    CK(cudaStreamCreateWithFlags(&h->fin_stream, cudaStreamNonBlocking));
+    return ST_OK;
 }
 
 int ensure_stage(st_handle* h, size_t bytes)
@@ -438,7 +492,8 @@ enum StepPhase { PH_ALL = 0, PH_PROBE = 1, PH_DEPOSIT = 2, PH_FINISH = 3 };
  * of the mesh with deposit mode dep (DEP_PROBE for the read-only pass), `sort()` re-sorts
  * every cloud. */
 template <class L, class S>
-int step_phases(st_handle* h, double dt, int phase, bool empty, L&& launch, S&& sort)
+int step_phases(st_handle* h, double dt, int phase, bool empty, L&& launch, S&& sort,
+                unsigned long long* acc_ovl = nullptr)
 {
     const bool det = (h->dep == DEP_DET1 || h->dep == DEP_DET2);
     const int nc = h->p.n_clouds;
@@ -496,12 +551,30 @@ int step_phases(st_handle* h, double dt, int phase, bool empty, L&& launch, S&& 
             return ST_OK;
         }
     }
-    if (det) {
+    if (det && acc_ovl) {
+        /* overlapped finalize: the next scale now, in stream order; the conversion and the
+         * clearing of this step's accumulator on fin_stream, concurrent with the next step */
+        const int p = h->par;
+        int32_t* Lf = h->dLfin + (size_t)p * nc;
+        CK(launch_next_scale(h->dctl, Lf, nc, h->stream));
+        CK(cudaEventRecord(h->ev_step[p], h->stream));
+        CK(cudaStreamWaitEvent(h->fin_stream, h->ev_step[p], 0));
+        {
+            ProfScope ps(h, ST_KERNEL_FINALIZE, h->fin_stream);
+            CK(launch_finalize(h->limbs, acc_ovl, h->dsrc, h->dsrc32, h->dctl, Lf, h->dcounter,
+                               nc, h->stride, finalize_grid(h), h->fin_stream));
+        }
+        CK(cudaMemsetAsync(acc_ovl, 0, (size_t)h->stride * nc * h->limbs * 8, h->fin_stream));
+        CK(cudaEventRecord(h->ev_fin[p], h->fin_stream));
+        h->fin_pending[p] = true;
+        h->par ^= 1;
+        h->launches += 2;
+    } else if (det) {
         if (phase == PH_FINISH) CK(launch_ctl_exponents(h->dctl, h->dexp, nc, true, h->stream));
         {
             ProfScope ps(h, ST_KERNEL_FINALIZE);
-            CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dsrc32, h->dctl, h->dcounter, nc,
-                               h->stride, finalize_grid(h), h->stream));
+            CK(launch_finalize(h->limbs, h->dacc, h->dsrc, h->dsrc32, h->dctl, nullptr,
+                               h->dcounter, nc, h->stride, finalize_grid(h), h->stream));
             h->launches += 1;
         }
         CK(cudaMemsetAsync(h->dacc, 0, (size_t)h->stride * nc * h->limbs * 8, h->stream));
@@ -523,6 +596,9 @@ int do_step(st_handle* h, double dt, double fscale, int phase = PH_ALL)
         if (h->tet) return do_step_tet<V>(h, dt, fscale, phase);
     }
     if (!h->capturing && h->clouds_dirty && (rc = upload_clouds<P, V>(h)) != ST_OK) return rc;
+    const bool ovl = h->fin_overlap && phase == PH_ALL && !h->capturing &&
+                     (h->dep == DEP_DET1 || h->dep == DEP_DET2) && h->p.n_clouds == 1;
+    if ((rc = ovl ? ensure_overlap(h) : join_fin(h))) return rc;
     StepArgs<P, V> a;
     a.mesh = mesh_k<P>(h);
     a.phys = phys_k<V>(h);
@@ -543,6 +619,16 @@ int do_step(st_handle* h, double dt, double fscale, int phase = PH_ALL)
     } else {
         memset(&a.one, 0, sizeof a.one);
     }
+    unsigned long long* acc_ovl = nullptr;
+    if (ovl) {
+        /* this step deposits into accumulator par, cleared by the finalize two steps back */
+        acc_ovl = h->par ? h->dacc2 : h->dacc;
+        a.one.acc = acc_ovl;
+        if (h->fin_pending[h->par]) {
+            CK(cudaStreamWaitEvent(h->stream, h->ev_fin[h->par], 0));
+            h->fin_pending[h->par] = false;
+        }
+    }
     int grid = h->grid;
     const int64_t warps_per_block = h->block / 32;
     const int64_t need = (a.total_tiles + warps_per_block - 1) / warps_per_block;
@@ -554,7 +640,7 @@ int do_step(st_handle* h, double dt, double fscale, int phase = PH_ALL)
         return launch_step<P, V>(a, dep, grid, h->block, h->stream);
     };
     return step_phases(h, dt, phase, a.total_tiles == 0, launch,
-                       [&] { return do_sort_all<P, V>(h); });
+                       [&] { return do_sort_all<P, V>(h); }, acc_ovl);
 }
 
 /* The step on a tetrahedral mesh: the launch sequence of do_step with the face-walk kernel
@@ -563,6 +649,7 @@ template <class V>
 int do_step_tet(st_handle* h, double dt, double fscale, int phase)
 {
     int rc;
+    if ((rc = join_fin(h))) return rc;
     if (!h->capturing && h->clouds_dirty && (rc = upload_clouds<double, V>(h)) != ST_OK) return rc;
     TetStepArgs<V> a;
     a.mesh = h->tmesh;
@@ -989,6 +1076,8 @@ int graph_capture(st_handle* h, int n, double dt, const double* fs)
 {
     int rc;
     release_graph(h);
+    /* the capture runs the finalize in stream order: nothing may still run on fin_stream */
+    if ((rc = drain_fin(h))) return rc;
     CK(cudaStreamSynchronize(h->stream));
     const bool det = (h->dep == DEP_DET1 || h->dep == DEP_DET2);
     if (det && (h->need_probe || dt != h->last_dt)) {
@@ -1557,12 +1646,20 @@ int st_destroy(st_handle* h)
     if (!h) return ST_OK;
     DeviceGuard g(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->fin_stream) {
+        cudaStreamSynchronize(h->fin_stream);
+        cudaStreamDestroy(h->fin_stream);
+    }
+    for (int p = 0; p < 2; ++p) {
+        if (h->ev_step[p]) cudaEventDestroy(h->ev_step[p]);
+        if (h->ev_fin[p]) cudaEventDestroy(h->ev_fin[p]);
+    }
     for (auto& c : h->clouds) free_cloud(c);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
     void* arrs[] = {h->dU, h->dsrc, h->dacc, h->dctl, h->dcounter, h->dcount, h->dclouds,
                     h->dstage, h->adj.mem, h->dclouds2, h->d_verts, h->d_tets, h->d_planes, h->d_planes32, h->d_nbr,
-                    h->d_hops, h->dbins, h->doffs, h->dscan, h->dexp};
+                    h->d_hops, h->dbins, h->doffs, h->dscan, h->dexp, h->dacc2, h->dLfin};
     for (void* p : arrs)
         if (p) cudaFree(p);
     for (auto& r : h->recs) {
@@ -1813,6 +1910,7 @@ static int copy_source(st_handle* h, int cloud, void* S, int elem_bytes, bool sy
     const int64_t ncomp = h->ncells * 3;
     const double* src = h->dsrc + (int64_t)cloud * h->stride;
     int rc;
+    if ((rc = join_fin(h))) return rc;
     if (elem_bytes == 8) {
         CK(cudaMemcpyAsync(S, src, ncomp * 8, cudaMemcpyDeviceToHost, h->stream));
     } else {
@@ -1843,6 +1941,8 @@ int st_get_source(st_handle* h, int cloud, void* S, int elem_bytes)
 const double* st_source_device(st_handle* h, int cloud)
 {
     if (!h || cloud < 0 || cloud >= h->p.n_clouds) return nullptr;
+    DeviceGuard g(h->device);
+    if (join_fin(h)) return nullptr;   /* the handle's stream now follows the last source */
     return h->dsrc + (int64_t)cloud * h->stride;
 }
 
@@ -1851,6 +1951,7 @@ int st_synchronize(st_handle* h)
     int rc;
     if ((rc = check_handle(h))) return rc;
     DeviceGuard g(h->device);
+    if ((rc = join_fin(h))) return rc;
     CK(cudaStreamSynchronize(h->stream));
     return check_device_errors(h);
 }
@@ -1862,6 +1963,7 @@ int st_set_stream(st_handle* h, void* stream)
     int rc;
     if ((rc = check_handle(h))) return rc;
     DeviceGuard g(h->device);
+    if ((rc = drain_fin(h))) return rc;
     CK(cudaStreamSynchronize(h->stream));
     if (h->own_stream) cudaStreamDestroy(h->stream);
     h->stream = (cudaStream_t)stream;
@@ -1884,6 +1986,7 @@ int st_profile_read(st_handle* h, int kind, int64_t* launches, double* ms, int r
     if (kind < 0 || kind >= ST_KERNEL_KINDS)
         return fail(ST_ERR_INVALID_ARGUMENT, "unknown kernel kind %d", kind);
     DeviceGuard g(h->device);
+    if ((rc = drain_fin(h))) return rc;   /* finalize events are recorded on fin_stream */
     CK(cudaStreamSynchronize(h->stream));
     cudaError_t err = cudaSuccess;
     for (auto& r : h->recs) {
@@ -1989,6 +2092,16 @@ int st_shard_deposit(st_handle* h, double dt, double fluid_scale)
 int st_shard_finish(st_handle* h)
 {
     return shard_phase(h, h ? h->last_dt : 0.0, 1.0, PH_FINISH);
+}
+
+int st_set_finalize_overlap(st_handle* h, int on)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    DeviceGuard g(h->device);
+    if ((rc = drain_fin(h))) return rc;
+    h->fin_overlap = on != 0;
+    return ST_OK;
 }
 
 int st_set_step_kernel(st_handle* h, int kind)
@@ -2229,6 +2342,7 @@ int st_save_state(st_handle* h, const char* path)
 static int load_state_impl(st_handle* h, const char* path)
 {
     int rc;
+    if (h && (rc = drain_fin(h))) return rc;
     struct Closer {
         FILE* f;
         ~Closer() { if (f) fclose(f); }
@@ -2400,6 +2514,8 @@ int st_setup(const st_params* p, const st_mesh_desc* m)
     if (rc) return rc;
     async_release();
     if (g_default) st_destroy(g_default);
+    /* the coupling calls synchronise every step: nothing to overlap the finalize with */
+    h->fin_overlap = false;
     g_default = h;
     return ST_OK;
 }

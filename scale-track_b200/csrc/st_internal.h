@@ -215,8 +215,11 @@ bool ring_eligible(const StepArgs<P, V>& a, int dep);
 /* Fixed point -> FP64 source [nclouds][stride] (and, when src32 is not null, its FP32
  * rounding in the same layout), next scale per cloud. */
 cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, float* src32,
-                            CloudCtl* ctl, unsigned int* counter, int nclouds, int64_t stride,
-                            int grid_x, cudaStream_t s);
+                            CloudCtl* ctl, const int32_t* Lsrc, unsigned int* counter,
+                            int nclouds, int64_t stride, int grid_x, cudaStream_t s);
+/* Scale of the step just run -> Lfin, next scale from its largest deposit (overlapped
+ * finalize: the finalize then reads Lfin). */
+cudaError_t launch_next_scale(CloudCtl* ctl, int32_t* Lfin, int nclouds, cudaStream_t s);
 cudaError_t launch_set_scale(CloudCtl* ctl, int nclouds, cudaStream_t s);
 cudaError_t launch_ctl_exponents(CloudCtl* ctl, int32_t* e, int nclouds, bool to_ctl,
                                  cudaStream_t s);

@@ -261,13 +261,15 @@ template <int LIMBS>
 __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict__ acc,
                                                   double* __restrict__ src,
                                                   float* __restrict__ src32, CloudCtl* ctl,
+                                                  const int32_t* __restrict__ Lsrc,
                                                   unsigned int* counter, int nclouds,
                                                   int64_t stride)
 {
     /* stride: per-cloud component count, a multiple of 4 (padding stays zero).  The caller
-     * clears the accumulators after this kernel. */
+     * clears the accumulators after this kernel.  Lsrc: the scale of each cloud when the next
+     * scale was already set by k_next_scale (overlapped finalize), else null. */
     const int c = blockIdx.y;
-    const int L = ctl[c].L;
+    const int L = Lsrc ? Lsrc[c] : ctl[c].L;
     const ulonglong2* a = reinterpret_cast<const ulonglong2*>(acc + (int64_t)c * stride * LIMBS);
     double2* s = reinterpret_cast<double2*>(src + (int64_t)c * stride);
     float4* s32 = src32 ? reinterpret_cast<float4*>(src32 + (int64_t)c * stride) : nullptr;
@@ -305,6 +307,7 @@ __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict
         if (s32) __stcs(s32 + g, make_float4((float)o[0], (float)o[1], (float)o[2], (float)o[3]));
     }
     /* the last block to finish moves every cloud to the scale of its largest deposit */
+    if (Lsrc) return;
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -324,15 +327,35 @@ __global__ void __launch_bounds__(256) k_finalize(unsigned long long* __restrict
 }
 
 cudaError_t launch_finalize(int limbs, unsigned long long* acc, double* src, float* src32,
-                            CloudCtl* ctl, unsigned int* counter, int nclouds, int64_t stride,
-                            int grid_x, cudaStream_t s)
+                            CloudCtl* ctl, const int32_t* Lsrc, unsigned int* counter,
+                            int nclouds, int64_t stride, int grid_x, cudaStream_t s)
 {
     if (stride % 4) return cudaErrorInvalidValue;
     dim3 grid(grid_x, nclouds);
     if (limbs == 1)
-        k_finalize<1><<<grid, 256, 0, s>>>(acc, src, src32, ctl, counter, nclouds, stride);
+        k_finalize<1><<<grid, 256, 0, s>>>(acc, src, src32, ctl, Lsrc, counter, nclouds, stride);
     else
-        k_finalize<2><<<grid, 256, 0, s>>>(acc, src, src32, ctl, counter, nclouds, stride);
+        k_finalize<2><<<grid, 256, 0, s>>>(acc, src, src32, ctl, Lsrc, counter, nclouds, stride);
+    return cudaGetLastError();
+}
+
+/* The scale bookkeeping of k_finalize on its own, for an overlapped finalize: keeps each
+ * cloud's scale of the step just run in Lfin (for the finalize on the other stream) and moves
+ * the cloud to the scale of that step's largest deposit for the next step. */
+__global__ void k_next_scale(CloudCtl* ctl, int32_t* Lfin, int nclouds)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nclouds) {
+        Lfin[k] = ctl[k].L;
+        const int em = ctl[k].emax;
+        if (em != EXP_NONE) ctl[k].L = em - ctl[k].H;
+        ctl[k].emax = EXP_NONE;
+    }
+}
+
+cudaError_t launch_next_scale(CloudCtl* ctl, int32_t* Lfin, int nclouds, cudaStream_t s)
+{
+    k_next_scale<<<(nclouds + 127) / 128, 128, 0, s>>>(ctl, Lfin, nclouds);
     return cudaGetLastError();
 }
 
