@@ -328,6 +328,9 @@ def run_ours(args):
     for _ in range(args.steps):
         step(dt, fs(k))
         k += 1
+    # the last step's source conversion runs beside the stream: order the stream after it so
+    # that the stop event covers it
+    h.source_device_ptr(0)
     ms = timer.stop()
     w1 = time.time()
     time.sleep(0.3)

@@ -2168,6 +2168,9 @@ int st_graph_launch(st_handle* h)
     if ((rc = check_handle(h))) return rc;
     if (!h->gexec) return fail(ST_ERR_INVALID_ARGUMENT, "no captured graph");
     DeviceGuard g(h->device);
+    /* the graph deposits into the first accumulator in stream order: pending overlapped
+     * finalizes (which clear it) come first */
+    if ((rc = join_fin(h))) return rc;
     CK(cudaGraphLaunch(h->gexec, h->stream));
     h->steps += h->graph_steps;
     h->launches += h->graph_launches;
