@@ -232,11 +232,12 @@ typedef struct st_tune_result {
  * changes positions, velocities or the fixed-point source. */
 ST_API int st_autotune(st_handle* h, double dt, int trial_steps, st_tune_result* out);
 
-/* Step kernel of a handle with one cloud.  ST_STEP_KERNEL_RING (the default): a persistent
- * block per SM streams block tiles of 1024 parcels through a shared-memory ring with bulk
- * copies.  ST_STEP_KERNEL_WARP: every warp loads and steps its own 32 parcels.  Both give
- * bit-identical positions, velocities, cells and sources; handles with several clouds, and
- * the first (probe) pass of a run, always use the warp kernel.  No counterpart in the
+/* Step kernel of a handle with one cloud (cuboid or tet mesh).  ST_STEP_KERNEL_RING (the
+ * default): a persistent block per SM streams block tiles of 1024 parcels through a
+ * shared-memory ring with bulk copies.  ST_STEP_KERNEL_WARP: every warp loads and steps its
+ * own 32 parcels.  Both give bit-identical positions, velocities, cells, sources and walk
+ * lengths; handles with several clouds, and the first (probe) pass of a run, always use the
+ * warp kernel.  No counterpart in the
  * reference (one kernel, A:1258-1269). */
 enum { ST_STEP_KERNEL_RING = 0, ST_STEP_KERNEL_WARP = 1 };
 ST_API int st_set_step_kernel(st_handle* h, int kind);

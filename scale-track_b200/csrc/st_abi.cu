@@ -665,11 +665,20 @@ int do_step_tet(st_handle* h, double dt, double fscale, int phase)
     a.ctl = h->dctl;
     a.total_tiles = h->total_tiles;
     a.hop_hist = h->d_hops;
+    if (h->p.n_clouds == 1) {
+        const std::vector<unsigned char>& hc = h->capturing ? h->hclouds2 : h->hclouds;
+        const size_t off = h->capturing ? (size_t)h->cap_parity * sizeof(CloudK<double, V>) : 0;
+        memcpy(&a.one, hc.data() + off, sizeof(CloudK<double, V>));
+    } else {
+        memset(&a.one, 0, sizeof a.one);
+    }
     int grid = h->grid;
     const int64_t need = (a.total_tiles + h->block / 32 - 1) / (h->block / 32);
     if (grid > need) grid = (int)need;
     if (grid < 1) grid = 1;
     auto launch = [&](int dep) -> cudaError_t {
+        if (dep != DEP_PROBE && h->ring && tet_ring_eligible<V>(a, dep))
+            return launch_step_tet_ring<V>(a, dep, h->nsm, h->stream);
         return launch_step_tet<V>(a, dep, grid, h->block, h->stream);
     };
     return step_phases(h, dt, phase, a.total_tiles == 0, launch,
@@ -1557,6 +1566,9 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
     if (occ < 1) occ = 1;
     h->grid = p->grid_blocks > 0 ? p->grid_blocks : nsm * occ;
     if (!h->tet && (e = DISPATCH(h, ring_prepare)) != cudaSuccess)
+        return bail(fail(ST_ERR_CUDA, "ring kernel set-up: %s", cudaGetErrorString(e)));
+    if (h->tet && (e = (p->precision == ST_PREC_FP64 ? tet_ring_prepare<double>()
+                                                       : tet_ring_prepare<float>())) != cudaSuccess)
         return bail(fail(ST_ERR_CUDA, "ring kernel set-up: %s", cudaGetErrorString(e)));
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
         return bail(fail(ST_ERR_CUDA, "set-up: %s", cudaGetErrorString(e)));

@@ -135,6 +135,7 @@ struct TetStepArgs {
     CloudCtl* ctl;
     int64_t total_tiles;                 /* warp tiles of WARP_TILE parcels */
     unsigned long long* hop_hist;        /* [8] walk lengths per substep, or nullptr */
+    CloudK<double, V> one;               /* with one cloud: its descriptor (kernel parameters) */
 };
 
 template <class V>
@@ -142,6 +143,14 @@ cudaError_t launch_step_tet(const TetStepArgs<V>& a, int dep, int grid, int bloc
                             cudaStream_t s);
 template <class V>
 int step_tet_max_active_blocks(int dep, int block);
+/* The tet step of a single cloud as a shared-memory ring (st_ring.cuh): true when it can run
+ * this step (one cloud, a real deposit mode, 16-byte aligned arrays). */
+template <class V>
+bool tet_ring_eligible(const TetStepArgs<V>& a, int dep);
+template <class V>
+cudaError_t launch_step_tet_ring(const TetStepArgs<V>& a, int dep, int nsm, cudaStream_t s);
+template <class V>
+cudaError_t tet_ring_prepare();
 /* Walks every parcel from hint[i] to the tet that contains it (hop limit of the mesh);
  * cells[i] = tet or -1, and `outside` counts failures. */
 /* Face planes of every tet (canonical vertex order) from vertices and vertex ids. */

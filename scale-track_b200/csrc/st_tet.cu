@@ -26,7 +26,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "st_device.cuh"
+#include "st_ring.cuh"
 
 namespace st {
 
@@ -373,6 +376,156 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
     if (count_hops && threadIdx.x < 8 && s_tet_hist[threadIdx.x])
         atomicAdd(a.hop_hist + threadIdx.x, (unsigned long long)s_tet_hist[threadIdx.x]);
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* the tet step of one cloud on the shared-memory ring                                  */
+/* ------------------------------------------------------------------------------------ */
+
+/* The consumer work of the tet ring: each warp's RING_SPW slices of 32 parcels through
+ * tet_parcel, the new state written back into the tile, deposits reduced per slice. */
+template <class V, int DEP, bool ONE>
+struct TetRing {
+    const TetStepArgs<V>& a;
+    unsigned long long* acc;
+    double* src;
+    const Quant& qp;
+    int lane;
+    bool count_hops;
+    AmaxT<V>& amax;
+    unsigned& ovf;
+    unsigned& nlost;
+    template <bool GLOBAL>
+    __device__ __forceinline__ void run(const RingArrays<double, V>& r, int j0, int64_t nvalid)
+    {
+        const int nsub = ONE ? 1 : a.phys.nsub;
+#pragma unroll
+        for (int sl = 0; sl < RING_SPW; ++sl) {
+            const int j = j0 + 32 * sl;
+            int32_t key = -1;
+            V dep[3] = {(V)0, (V)0, (V)0};
+            if (!GLOBAL || j < nvalid) {
+                double pos[3] = {ring_ld<GLOBAL>(r.x + j), ring_ld<GLOBAL>(r.y + j),
+                                 ring_ld<GLOBAL>(r.z + j)};
+                V vel[3] = {ring_ld<GLOBAL>(r.u + j), ring_ld<GLOBAL>(r.v + j),
+                            ring_ld<GLOBAL>(r.w + j)};
+                const V d = ring_ld<GLOBAL>(r.d + j) * a.phys.dscale;
+                int32_t cell = ring_ld<GLOBAL>(r.cell + j);
+                bool lost = false;
+                tet_parcel<V, DEP>(a, nsub, pos, vel, d, cell, acc, src, qp, amax, ovf, lost,
+                                   key, dep, count_hops);
+                if (lost) {
+                    ++nlost;
+                    key = -1;
+                } else {
+                    ring_st<GLOBAL>(r.x + j, pos[0]);
+                    ring_st<GLOBAL>(r.y + j, pos[1]);
+                    ring_st<GLOBAL>(r.z + j, pos[2]);
+                    ring_st<GLOBAL>(r.u + j, vel[0]);
+                    ring_st<GLOBAL>(r.v + j, vel[1]);
+                    ring_st<GLOBAL>(r.w + j, vel[2]);
+                    ring_st<GLOBAL>(r.cell + j, cell);
+                }
+            }
+            deposit_warp<DEP, V>(key, dep, acc, src, qp, lane, amax, ovf);
+        }
+    }
+};
+
+template <class V, int DEP, bool ONE>
+__global__ void __launch_bounds__(RING_THREADS, 1) k_step_tet_ring(const TetStepArgs<V> a)
+{
+    constexpr bool DET = (DEP == DEP_DET1 || DEP == DEP_DET2);
+    Quant qp = {0.0, 0.0, 0.0f, 0.0f, 0, false};
+    if (DET) qp = make_quant(a.ctl[0].L, a.ctl[0].H + QUANT_GROWTH_BITS);
+    AmaxT<V> amax = (V)0;
+    unsigned ovf = 0, nlost = 0;
+    const int lane = threadIdx.x & 31;
+    const bool count_hops = a.hop_hist != nullptr;
+    if (threadIdx.x < 8) s_tet_hist[threadIdx.x] = 0;   /* ring_block synchronises */
+    TetRing<V, DEP, ONE> step{a, DET ? a.one.acc : nullptr,
+                              DEP == DEP_ATOMIC ? a.one.src : nullptr, qp, lane, count_hops,
+                              amax, ovf, nlost};
+    if (!ring_block<double, V, true>(a.one, a.ctl, step)) return;
+    flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost);
+    ring_consumers_sync();
+    if (count_hops && threadIdx.x < 8 && s_tet_hist[threadIdx.x])
+        atomicAdd(a.hop_hist + threadIdx.x, (unsigned long long)s_tet_hist[threadIdx.x]);
+}
+
+template <class V, int DEP, bool ONE>
+static cudaError_t tet_ring_attr()
+{
+    static std::atomic<unsigned long long> ready{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ULL << (dev & 63);
+    if (ready.load() & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_step_tet_ring<V, DEP, ONE>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)RingGeom<double, V, true>::SMEM);
+    if (e == cudaSuccess) ready.fetch_or(bit);
+    return e;
+}
+
+template <class V, int DEP, bool ONE>
+static cudaError_t launch_tet_ring_t(const TetStepArgs<V>& a, int nsm, cudaStream_t s)
+{
+    cudaError_t e = tet_ring_attr<V, DEP, ONE>();
+    if (e != cudaSuccess) return e;
+    const int64_t nfull = a.one.n / RING_BT;
+    int64_t grid = nfull < nsm ? nfull : nsm;
+    if (grid < 1) grid = 1;
+    k_step_tet_ring<V, DEP, ONE><<<(int)grid, RING_THREADS, RingGeom<double, V, true>::SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class V>
+bool tet_ring_eligible(const TetStepArgs<V>& a, int dep)
+{
+    if (a.nclouds != 1 || a.one.n <= 0 || !a.one.cell) return false;
+    if (dep != DEP_DET1 && dep != DEP_DET2 && dep != DEP_ATOMIC) return false;
+    const void* p[8] = {a.one.x, a.one.y, a.one.z, a.one.u, a.one.v, a.one.w, a.one.d, a.one.cell};
+    for (const void* q : p)
+        if (reinterpret_cast<uintptr_t>(q) % 16) return false;
+    return true;
+}
+
+template <class V>
+cudaError_t launch_step_tet_ring(const TetStepArgs<V>& a, int dep, int nsm, cudaStream_t s)
+{
+    const bool one = a.phys.nsub == 1;
+    switch (dep) {
+    case DEP_DET1: return one ? launch_tet_ring_t<V, DEP_DET1, true>(a, nsm, s)
+                              : launch_tet_ring_t<V, DEP_DET1, false>(a, nsm, s);
+    case DEP_DET2: return one ? launch_tet_ring_t<V, DEP_DET2, true>(a, nsm, s)
+                              : launch_tet_ring_t<V, DEP_DET2, false>(a, nsm, s);
+    case DEP_ATOMIC: return one ? launch_tet_ring_t<V, DEP_ATOMIC, true>(a, nsm, s)
+                                : launch_tet_ring_t<V, DEP_ATOMIC, false>(a, nsm, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+/* Makes every tet ring kernel instance of a precision launchable on the current device
+ * (called when a tet handle is created, outside any stream capture). */
+template <class V>
+cudaError_t tet_ring_prepare()
+{
+    const cudaError_t r[6] = {tet_ring_attr<V, DEP_DET1, true>(), tet_ring_attr<V, DEP_DET1, false>(),
+                              tet_ring_attr<V, DEP_DET2, true>(), tet_ring_attr<V, DEP_DET2, false>(),
+                              tet_ring_attr<V, DEP_ATOMIC, true>(),
+                              tet_ring_attr<V, DEP_ATOMIC, false>()};
+    for (cudaError_t e : r)
+        if (e != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+template bool tet_ring_eligible<float>(const TetStepArgs<float>&, int);
+template bool tet_ring_eligible<double>(const TetStepArgs<double>&, int);
+template cudaError_t launch_step_tet_ring<float>(const TetStepArgs<float>&, int, int, cudaStream_t);
+template cudaError_t launch_step_tet_ring<double>(const TetStepArgs<double>&, int, int, cudaStream_t);
+template cudaError_t tet_ring_prepare<float>();
+template cudaError_t tet_ring_prepare<double>();
 
 template <class V, bool ONE>
 static cudaError_t launch_step_tet_t(const TetStepArgs<V>& a, int dep, int grid, int block,

@@ -124,3 +124,32 @@ def test_overlapped_finalize_same_results(prec):
         assert np.array_equal(s1, s2)
     for p, q in zip(a[1:], b[1:]):
         assert np.array_equal(p, q)
+
+
+@pytest.mark.parametrize("prec,nsub", [("mixed", 1), ("fp64", 1), ("mixed", 3)])
+def test_tet_ring_equals_warp_kernel(prec, nsub):
+    """The tet step on the shared-memory ring (default for one cloud) and on per-warp tiles:
+    parcels, owning tets, sources and walk-length histograms identical."""
+    n, npcl, steps = 12, 148 * 1024 + 333, 3
+    verts, tets, nbr, hex_ijk = workload.kuhn_tet_mesh(n, workload.L_BOX, 0.15, 1)
+    xyz, _, d = workload.parcels(npcl, 17)
+    uvw = np.random.default_rng(18).normal(0.0, 5.0, (3, npcl)).astype(np.float32).astype(np.float64)
+    hint = workload.tet_hints(xyz, hex_ijk, n)
+    U = workload.tgv_at(workload.tet_centroids(verts, tets), U0=3.0)
+    prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                    drag_model="schiller_naumann", precision=prec, n_substeps=nsub,
+                    sort_interval=2)
+    out = {}
+    for kind in ("ring", "warp"):
+        with st.ParcelTracker(prm, st.tet_mesh_desc(verts, tets, nbr, 0.0, workload.L_BOX)) as h:
+            h.set_step_kernel(kind)
+            h.set_parcels(xyz, uvw, d, hint=hint)
+            h.set_fluid_velocity(U.astype(np.float64 if prec == "fp64" else np.float32))
+            for k in range(steps):
+                h.step(1e-3, workload.fluid_scale(k))
+            h.synchronize()
+            x, u, _ = h.get_parcels()
+            out[kind] = (x, u, h.get_cells(), h.get_source(), h.hop_histogram())
+    for p, q in zip(out["ring"], out["warp"]):
+        assert np.array_equal(p, q)
+    assert out["ring"][4][1:].sum() > 0    # the walks did hop
