@@ -18,6 +18,10 @@
 #include "st_step.cuh"
 #include "st_ring.cuh"
 
+#ifndef ST_RING_DEPOSIT_AFTER
+#define ST_RING_DEPOSIT_AFTER 0
+#endif
+
 namespace st {
 
 /* Steps parcels j0, j0 + 32, ... (RING_SPW of them, those below nvalid) of the arrays: the
@@ -59,11 +63,22 @@ __device__ __forceinline__ void ring_slices(const StepArgs<P, V>& a, P* xs, P* y
             }
         }
     }
+#if ST_RING_DEPOSIT_AFTER
+    int32_t keys[RING_SPW];
+    V deps[RING_SPW][3];
+#endif
 #pragma unroll
     for (int s = 0; s < RING_SPW; ++s) {
         const int j = j0 + 32 * s;
+#if ST_RING_DEPOSIT_AFTER
+        int32_t& key = keys[s];
+        V* dep = deps[s];
+        key = -1;
+        dep[0] = dep[1] = dep[2] = (V)0;
+#else
         int32_t key = -1;
         V dep[3] = {(V)0, (V)0, (V)0};
+#endif
         if (pI[s] > 0) {
             P pos[3] = {X[s], Y[s], Z[s]};
             V vel[3] = {Uv[s], Vv[s], Wv[s]};
@@ -87,8 +102,15 @@ __device__ __forceinline__ void ring_slices(const StepArgs<P, V>& a, P* xs, P* y
                 ring_st<GLOBAL>(ws + j, vel[2]);
             }
         }
+#if !ST_RING_DEPOSIT_AFTER
         deposit_warp<DEP, V>(key, dep, acc, src, qp, lane, amax, ovf);
+#endif
     }
+#if ST_RING_DEPOSIT_AFTER
+#pragma unroll
+    for (int s = 0; s < RING_SPW; ++s)
+        deposit_warp<DEP, V>(keys[s], deps[s], acc, src, qp, lane, amax, ovf);
+#endif
 }
 
 /* The consumer work of the hex ring: ring_slices on the tile's arrays. */
