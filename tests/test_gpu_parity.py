@@ -313,7 +313,15 @@ def test_profile_counters_and_launch_count():
         nstep, ms = h.profile_read("step")
         nfin, _ = h.profile_read("finalize")
         assert nstep == 4 and nfin == 4 and ms > 0
-        assert h.launch_count() - c0 == 4 * 2 + 2   # probe + set_scale on the first step
+        # step, next-scale and finalize per step (the finalize overlapping the next step),
+        # probe + set_scale on the first step
+        assert h.launch_count() - c0 == 4 * 3 + 2
+        h.set_finalize_overlap(False)
+        c1 = h.launch_count()
+        for s in range(4):
+            h.step(workload.DT)
+        h.synchronize()
+        assert h.launch_count() - c1 == 4 * 2   # step and finalize (with its scale update)
 
 
 @pytest.mark.slow

@@ -145,11 +145,16 @@ def test_tet_ring_equals_warp_kernel(prec, nsub):
             h.set_step_kernel(kind)
             h.set_parcels(xyz, uvw, d, hint=hint)
             h.set_fluid_velocity(U.astype(np.float64 if prec == "fp64" else np.float32))
+            lost = 0
             for k in range(steps):
                 h.step(1e-3, workload.fluid_scale(k))
-            h.synchronize()
+                try:   # fast parcels can outrun the walk's hop limit; both kernels count them
+                    h.synchronize()
+                except st.ScaleTrackError as e:
+                    assert e.code == st.ST_ERR_PARCEL_OUTSIDE, str(e)
+                    lost += int(str(e).split(":", 1)[1].split()[0])
             x, u, _ = h.get_parcels()
-            out[kind] = (x, u, h.get_cells(), h.get_source(), h.hop_histogram())
+            out[kind] = (x, u, h.get_cells(), h.get_source(), h.hop_histogram(), lost)
     for p, q in zip(out["ring"], out["warp"]):
         assert np.array_equal(p, q)
     assert out["ring"][4][1:].sum() > 0    # the walks did hop
