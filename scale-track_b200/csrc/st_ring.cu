@@ -18,11 +18,18 @@
 #include "st_step.cuh"
 #include "st_ring.cuh"
 
-#ifndef ST_RING_DEPOSIT_AFTER
-#define ST_RING_DEPOSIT_AFTER 0
-#endif
 
 namespace st {
+
+/* 1024-parcel tiles, 16 consumer warps with two slices each (17 warps: 96 registers) */
+#ifndef ST_RING_BT
+#define ST_RING_BT 1024
+#endif
+#ifndef ST_RING_CONSUMERS
+#define ST_RING_CONSUMERS 16
+#endif
+using HexShape = RingShape<ST_RING_BT, ST_RING_CONSUMERS>;
+constexpr int RING_SPW = HexShape::SPW;
 
 /* Steps parcels j0, j0 + 32, ... (RING_SPW of them, those below nvalid) of the arrays: the
  * state of every slice is read and its cell velocity gathered first, then each slice is
@@ -63,22 +70,11 @@ __device__ __forceinline__ void ring_slices(const StepArgs<P, V>& a, P* xs, P* y
             }
         }
     }
-#if ST_RING_DEPOSIT_AFTER
-    int32_t keys[RING_SPW];
-    V deps[RING_SPW][3];
-#endif
 #pragma unroll
     for (int s = 0; s < RING_SPW; ++s) {
         const int j = j0 + 32 * s;
-#if ST_RING_DEPOSIT_AFTER
-        int32_t& key = keys[s];
-        V* dep = deps[s];
-        key = -1;
-        dep[0] = dep[1] = dep[2] = (V)0;
-#else
         int32_t key = -1;
         V dep[3] = {(V)0, (V)0, (V)0};
-#endif
         if (pI[s] > 0) {
             P pos[3] = {X[s], Y[s], Z[s]};
             V vel[3] = {Uv[s], Vv[s], Wv[s]};
@@ -102,15 +98,8 @@ __device__ __forceinline__ void ring_slices(const StepArgs<P, V>& a, P* xs, P* y
                 ring_st<GLOBAL>(ws + j, vel[2]);
             }
         }
-#if !ST_RING_DEPOSIT_AFTER
         deposit_warp<DEP, V>(key, dep, acc, src, qp, lane, amax, ovf);
-#endif
     }
-#if ST_RING_DEPOSIT_AFTER
-#pragma unroll
-    for (int s = 0; s < RING_SPW; ++s)
-        deposit_warp<DEP, V>(keys[s], deps[s], acc, src, qp, lane, amax, ovf);
-#endif
 }
 
 /* The consumer work of the hex ring: ring_slices on the tile's arrays. */
@@ -133,7 +122,7 @@ struct HexRing {
 };
 
 template <class P, class V, int DEP, bool ONE>
-__global__ void __launch_bounds__(RING_THREADS, 1) k_step_ring(const StepArgs<P, V> a)
+__global__ void __launch_bounds__(HexShape::THREADS, 1) k_step_ring(const StepArgs<P, V> a)
 {
     constexpr bool DET = (DEP == DEP_DET1 || DEP == DEP_DET2);
     Quant qp = {0.0, 0.0, 0.0f, 0.0f, 0, false};
@@ -144,7 +133,7 @@ __global__ void __launch_bounds__(RING_THREADS, 1) k_step_ring(const StepArgs<P,
     HexRing<P, V, DEP, ONE> step{a, DET ? a.one.acc : nullptr,
                                  DEP == DEP_ATOMIC ? a.one.src : nullptr, qp, lane, amax, ovf,
                                  nlost};
-    if (!ring_block<P, V, false>(a.one, a.ctl, step)) return;
+    if (!ring_block<HexShape, P, V, false>(a.one, a.ctl, step)) return;
     flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost);
 }
 
@@ -165,7 +154,7 @@ static cudaError_t ring_attr()
     if (ready.load() & bit) return cudaSuccess;
     e = cudaFuncSetAttribute(k_step_ring<P, V, DEP, ONE>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)RingGeom<P, V, false>::SMEM);
+                             (int)RingGeom<HexShape, P, V, false>::SMEM);
     if (e == cudaSuccess) ready.fetch_or(bit);
     return e;
 }
@@ -175,10 +164,11 @@ static cudaError_t launch_ring_t(const StepArgs<P, V>& a, int nsm, cudaStream_t 
 {
     cudaError_t e = ring_attr<P, V, DEP, ONE>();
     if (e != cudaSuccess) return e;
-    const int64_t nfull = a.one.n / RING_BT;
+    const int64_t nfull = a.one.n / HexShape::BT;
     int64_t grid = nfull < nsm ? nfull : nsm;
     if (grid < 1) grid = 1;
-    k_step_ring<P, V, DEP, ONE><<<(int)grid, RING_THREADS, RingGeom<P, V, false>::SMEM, s>>>(a);
+    k_step_ring<P, V, DEP, ONE>
+        <<<(int)grid, HexShape::THREADS, RingGeom<HexShape, P, V, false>::SMEM, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -2,7 +2,7 @@
  * st_ring.cuh -- the shared-memory ring that streams a cloud's parcel state through the SMs
  * (used by the hex step kernel, st_ring.cu, and the tet step kernel, st_tet.cu).
  *
- * One block per SM.  The cloud's parcels are cut into block tiles of RING_BT consecutive
+ * One block per SM.  The cloud's parcels are cut into block tiles of BT consecutive
  * parcels; tile t belongs to block t mod grid.  A producer warp streams each tile's state
  * arrays (x, y, z, u, v, w, d and, on tet meshes, the owning tet: 4-8 KB each) from HBM into
  * a stage of a RING_NS-deep ring in shared memory with 1-D bulk copies (cp.async.bulk, no
@@ -13,7 +13,8 @@
  * ahead.  The loads of up to RING_NS - 1 tiles are in flight while a tile is stepped,
  * independent of how many warps are resident, and the consumers spend no instructions on
  * global addressing.  The last block also steps the ragged end of the cloud (fewer than
- * RING_BT parcels) with direct loads and stores.
+ * BT parcels) with direct loads and stores.  The tile size and the number of consumer warps
+ * are a RingShape per kernel.
  *
  * Every wait on an mbarrier gives up after about a second of clock cycles, sets the cloud's
  * fault word and lets the block drain (the producer waits, again bounded, for its own copies
@@ -29,36 +30,35 @@
 
 namespace st {
 
-#ifndef ST_RING_BT
-#define ST_RING_BT 1024
-#endif
-#ifndef ST_RING_CONSUMERS
-#define ST_RING_CONSUMERS 16
-#endif
-#ifndef ST_RING_MAX_NS
-#define ST_RING_MAX_NS 4
-#endif
-constexpr int RING_BT = ST_RING_BT;                         /* parcels per block tile      */
-constexpr int RING_CONSUMERS = ST_RING_CONSUMERS;           /* consumer warps per block    */
-constexpr int RING_THREADS = 32 * (RING_CONSUMERS + 1);     /* + one producer warp         */
-constexpr int RING_SPW = RING_BT / (32 * RING_CONSUMERS);   /* slices per warp and tile    */
 constexpr long long RING_WAIT_CYCLES = 2000000000LL;        /* about 1 s at 1.9 GHz        */
-constexpr int RING_MAX_NS = ST_RING_MAX_NS;
+constexpr int RING_MAX_NS = 4;
 
-template <class P, class V, bool CELL>
+/* The shape of a ring block: BT parcels per block tile, CONS consumer warps (one producer
+ * warp more), SPW 32-parcel slices per consumer warp and tile.  BT * 4 bytes must be a
+ * multiple of 16 (bulk copies start on 16-byte boundaries). */
+template <int BT_, int CONS_>
+struct RingShape {
+    static constexpr int BT = BT_;
+    static constexpr int CONS = CONS_;
+    static constexpr int THREADS = 32 * (CONS_ + 1);
+    static constexpr int SPW = BT_ / (32 * CONS_);
+    static_assert(SPW * 32 * CONS_ == BT_, "tile split");
+    static_assert((BT_ * 4) % 16 == 0, "16-byte tiles");
+};
+
+template <class S, class P, class V, bool CELL>
 struct RingGeom {
-    static constexpr uint32_t SP = RING_BT * sizeof(P);     /* bytes of one position array */
-    static constexpr uint32_t SV = RING_BT * sizeof(V);     /* bytes of one velocity array */
-    static constexpr uint32_t SC = CELL ? RING_BT * 4 : 0;  /* the owning-tet array        */
+    static constexpr uint32_t SP = S::BT * sizeof(P);       /* bytes of one position array */
+    static constexpr uint32_t SV = S::BT * sizeof(V);       /* bytes of one velocity array */
+    static constexpr uint32_t SC = CELL ? S::BT * 4 : 0;    /* the owning-tet array        */
     static constexpr uint32_t STAGE = 3 * SP + 4 * SV + SC;
     static constexpr int NS = (RING_MAX_NS * STAGE <= 200u * 1024u)
                                   ? RING_MAX_NS
                                   : (int)((200u * 1024u) / STAGE);
     static constexpr uint32_t SMEM = NS * STAGE;
+    static_assert(NS >= 2, "at least two stages");
+    static_assert(SMEM <= 227u * 1024u, "shared memory");
 };
-static_assert(RING_SPW * 32 * RING_CONSUMERS == RING_BT, "tile split");
-static_assert(RingGeom<double, double, true>::SMEM <= 227u * 1024u, "shared memory");
-static_assert(RingGeom<double, double, true>::NS >= 2, "at least two stages");
 
 /* ------------------------------------------------------------------------------------ */
 /* mbarrier and bulk-copy primitives (PTX)                                              */
@@ -188,23 +188,23 @@ __device__ __forceinline__ RingArrays<P, V> ring_global(const CloudK<P, V>& c, i
             c.cell ? c.cell + off : nullptr};
 }
 
-template <class P, class V, bool CELL>
+template <class S, class P, class V, bool CELL>
 __device__ __forceinline__ RingArrays<P, V> ring_stage(unsigned char* stage)
 {
     P* x = reinterpret_cast<P*>(stage);
-    V* u = reinterpret_cast<V*>(x + 3 * RING_BT);
-    V* d = u + 3 * RING_BT;
-    return {x, x + RING_BT, x + 2 * RING_BT, u, u + RING_BT, u + 2 * RING_BT, d,
-            CELL ? reinterpret_cast<int32_t*>(d + RING_BT) : nullptr};
+    V* u = reinterpret_cast<V*>(x + 3 * S::BT);
+    V* d = u + 3 * S::BT;
+    return {x, x + S::BT, x + 2 * S::BT, u, u + S::BT, u + 2 * S::BT, d,
+            CELL ? reinterpret_cast<int32_t*>(d + S::BT) : nullptr};
 }
 
 /* The producer (one thread): loads tiles into the ring, writes stepped tiles back. */
-template <class P, class V, bool CELL>
+template <class S, class P, class V, bool CELL>
 __device__ __forceinline__ void ring_producer(const CloudK<P, V>& cl, CloudCtl* ctl, int64_t cnt,
                                               int64_t blk, int64_t nblk, uint32_t sbase,
                                               uint32_t full0, uint32_t empty0)
 {
-    using R = RingGeom<P, V, CELL>;
+    using R = RingGeom<S, P, V, CELL>;
     const uint64_t pol = policy_evict_first();
     int64_t issued = 0;
     bool ok = true;
@@ -217,7 +217,7 @@ __device__ __forceinline__ void ring_producer(const CloudK<P, V>& cl, CloudCtl* 
                 ok = false;
                 break;
             }
-            const int64_t p0 = (blk + j * nblk) * RING_BT;
+            const int64_t p0 = (blk + j * nblk) * S::BT;
             const uint32_t st = sbase + s * R::STAGE;
             bulk_store(cl.x + p0, st, R::SP, pol);
             bulk_store(cl.y + p0, st + R::SP, R::SP, pol);
@@ -232,7 +232,7 @@ __device__ __forceinline__ void ring_producer(const CloudK<P, V>& cl, CloudCtl* 
             const int s = (int)(k % R::NS);
             /* the stage is free once the stores of its previous tile have read it */
             if (k >= R::NS) bulk_wait_read_all();
-            const int64_t p0 = (blk + k * nblk) * RING_BT;
+            const int64_t p0 = (blk + k * nblk) * S::BT;
             const uint32_t st = sbase + s * R::STAGE;
             const uint32_t fb = full0 + 8 * s;
             mbar_expect_tx(fb, R::STAGE);
@@ -260,20 +260,20 @@ __device__ __forceinline__ void ring_producer(const CloudK<P, V>& cl, CloudCtl* 
 }
 
 /* The block's part of the ring: barrier set-up, then the producer warp streams the block's
- * tiles and the consumer warps call step.run<false>(stage arrays, j0, RING_BT) per tile and,
- * in the last block, step.run<true>(global arrays, j0, n mod RING_BT) for the ragged end
+ * tiles and the consumer warps call step.run<false>(stage arrays, j0, S::BT) per tile and,
+ * in the last block, step.run<true>(global arrays, j0, n mod S::BT) for the ragged end
  * (j0 = the lane's first parcel of the warp's slices).  Returns false in the producer warp,
  * which must then return without touching barrier 1 (the consumers' named barrier). */
-template <class P, class V, bool CELL, class Step>
+template <class S, class P, class V, bool CELL, class Step>
 __device__ __forceinline__ bool ring_block(const CloudK<P, V>& cl, CloudCtl* ctl, Step& step)
 {
-    using R = RingGeom<P, V, CELL>;
+    using R = RingGeom<S, P, V, CELL>;
     extern __shared__ __align__(128) unsigned char ring_smem[];
     __shared__ __align__(8) unsigned long long ring_bars[2 * RING_MAX_NS];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t n = cl.n;
-    const int64_t nfull = n / RING_BT;
+    const int64_t nfull = n / S::BT;
     const int64_t nblk = gridDim.x;
     const int64_t blk = blockIdx.x;
     const int64_t cnt = blk < nfull ? (nfull - 1 - blk) / nblk + 1 : 0;
@@ -283,40 +283,41 @@ __device__ __forceinline__ bool ring_block(const CloudK<P, V>& cl, CloudCtl* ctl
     if (threadIdx.x == 0) {
         for (int s = 0; s < R::NS; ++s) {
             mbar_init(full0 + 8 * s, 1);
-            mbar_init(empty0 + 8 * s, RING_CONSUMERS);
+            mbar_init(empty0 + 8 * s, S::CONS);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
-    if (warp == RING_CONSUMERS) {
-        if (lane == 0) ring_producer<P, V, CELL>(cl, ctl, cnt, blk, nblk, sbase, full0, empty0);
+    if (warp == S::CONS) {
+        if (lane == 0) ring_producer<S, P, V, CELL>(cl, ctl, cnt, blk, nblk, sbase, full0, empty0);
         return false;
     }
-    const int j0 = warp * (RING_SPW * 32) + lane;
+    const int j0 = warp * (S::SPW * 32) + lane;
     bool ok = true;
     for (int64_t k = 0; k < cnt; ++k) {
         const int s = (int)(k % R::NS);
         /* every lane waits; the warp goes on only if all of them saw the stage arrive */
         ok = __all_sync(FULL_MASK, mbar_wait(full0 + 8 * s, (uint32_t)((k / R::NS) & 1)));
         if (!ok) break;
-        step.template run<false>(ring_stage<P, V, CELL>(ring_smem + (size_t)s * R::STAGE), j0,
-                                 (int64_t)RING_BT);
+        step.template run<false>(ring_stage<S, P, V, CELL>(ring_smem + (size_t)s * R::STAGE), j0,
+                                 (int64_t)S::BT);
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) mbar_arrive(empty0 + 8 * s);
     }
     if (!ok) ring_fault(ctl, 2);
     /* the ragged end of the cloud: the last block, straight from global memory */
-    if (ok && blk == nblk - 1 && n > nfull * RING_BT)
-        step.template run<true>(ring_global(cl, nfull * RING_BT), j0, n - nfull * RING_BT);
+    if (ok && blk == nblk - 1 && n > nfull * S::BT)
+        step.template run<true>(ring_global(cl, nfull * S::BT), j0, n - nfull * S::BT);
     return true;
 }
 
 /* barrier among the consumer warps of a ring block (the producer warp has returned) */
+template <class S>
 __device__ __forceinline__ void ring_consumers_sync()
 {
-    asm volatile("bar.sync 1, %0;" ::"n"(RING_CONSUMERS * 32) : "memory");
+    asm volatile("bar.sync 1, %0;" ::"n"(S::CONS * 32) : "memory");
 }
 
 }  // namespace st

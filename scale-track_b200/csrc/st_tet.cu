@@ -303,6 +303,10 @@ __device__ __forceinline__ void tet_parcel(const TetStepArgs<V>& a, int nsub, do
     cell = tNew;
 }
 
+#ifndef ST_TET_PREFETCH_NEXT
+#define ST_TET_PREFETCH_NEXT 0
+#endif
+
 /* Resident blocks of 256 threads per SM the compiler must allow: 4 (64 registers). */
 #ifndef ST_TET_MIN_BLOCKS
 #define ST_TET_MIN_BLOCKS 4
@@ -340,6 +344,18 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
         const int64_t n = __ldg(&cl->n);
         unsigned long long* const acc = DET ? cl->acc : nullptr;
         double* const src = (DEP == DEP_ATOMIC) ? cl->src : nullptr;
+#if ST_TET_PREFETCH_NEXT
+        /* the owning tets of this warp's next tile (same cloud): their FP32 planes and cell
+         * velocities towards L2 now, so that the next tile's first gathers hit L2 */
+        if (WARP_TILE == 32 && tile + nwarps < a.total_tiles) {
+            const int64_t inext = (tile + nwarps - __ldg(&cl->tile0)) * WARP_TILE + lane;
+            if (inext < n) {
+                const int32_t cn = ld_stream(cl->cell + inext);
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(a.mesh.planes32 + 4 * (int64_t)cn));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(a.U + 3 * (int64_t)cn));
+            }
+        }
+#endif
         for (int sl = 0; sl < WARP_TILE / 32; ++sl) {
         const int64_t i = (tile - __ldg(&cl->tile0)) * WARP_TILE + 32 * sl + lane;
         int32_t key = -1;
@@ -381,7 +397,11 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
 /* the tet step of one cloud on the shared-memory ring                                  */
 /* ------------------------------------------------------------------------------------ */
 
-/* The consumer work of the tet ring: each warp's RING_SPW slices of 32 parcels through
+/* 992-parcel tiles, 31 consumer warps with one slice each (32 warps at 64 registers: the
+ * walk's chains of dependent gathers need many warps in flight) */
+using TetShape = RingShape<992, 31>;
+
+/* The consumer work of the tet ring: each warp's slices of 32 parcels through
  * tet_parcel, the new state written back into the tile, deposits reduced per slice. */
 template <class V, int DEP, bool ONE>
 struct TetRing {
@@ -399,7 +419,7 @@ struct TetRing {
     {
         const int nsub = ONE ? 1 : a.phys.nsub;
 #pragma unroll
-        for (int sl = 0; sl < RING_SPW; ++sl) {
+        for (int sl = 0; sl < TetShape::SPW; ++sl) {
             const int j = j0 + 32 * sl;
             int32_t key = -1;
             V dep[3] = {(V)0, (V)0, (V)0};
@@ -432,7 +452,7 @@ struct TetRing {
 };
 
 template <class V, int DEP, bool ONE>
-__global__ void __launch_bounds__(RING_THREADS, 1) k_step_tet_ring(const TetStepArgs<V> a)
+__global__ void __launch_bounds__(TetShape::THREADS, 1) k_step_tet_ring(const TetStepArgs<V> a)
 {
     constexpr bool DET = (DEP == DEP_DET1 || DEP == DEP_DET2);
     Quant qp = {0.0, 0.0, 0.0f, 0.0f, 0, false};
@@ -445,9 +465,9 @@ __global__ void __launch_bounds__(RING_THREADS, 1) k_step_tet_ring(const TetStep
     TetRing<V, DEP, ONE> step{a, DET ? a.one.acc : nullptr,
                               DEP == DEP_ATOMIC ? a.one.src : nullptr, qp, lane, count_hops,
                               amax, ovf, nlost};
-    if (!ring_block<double, V, true>(a.one, a.ctl, step)) return;
+    if (!ring_block<TetShape, double, V, true>(a.one, a.ctl, step)) return;
     flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost);
-    ring_consumers_sync();
+    ring_consumers_sync<TetShape>();
     if (count_hops && threadIdx.x < 8 && s_tet_hist[threadIdx.x])
         atomicAdd(a.hop_hist + threadIdx.x, (unsigned long long)s_tet_hist[threadIdx.x]);
 }
@@ -463,7 +483,7 @@ static cudaError_t tet_ring_attr()
     if (ready.load() & bit) return cudaSuccess;
     e = cudaFuncSetAttribute(k_step_tet_ring<V, DEP, ONE>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)RingGeom<double, V, true>::SMEM);
+                             (int)RingGeom<TetShape, double, V, true>::SMEM);
     if (e == cudaSuccess) ready.fetch_or(bit);
     return e;
 }
@@ -473,10 +493,11 @@ static cudaError_t launch_tet_ring_t(const TetStepArgs<V>& a, int nsm, cudaStrea
 {
     cudaError_t e = tet_ring_attr<V, DEP, ONE>();
     if (e != cudaSuccess) return e;
-    const int64_t nfull = a.one.n / RING_BT;
+    const int64_t nfull = a.one.n / TetShape::BT;
     int64_t grid = nfull < nsm ? nfull : nsm;
     if (grid < 1) grid = 1;
-    k_step_tet_ring<V, DEP, ONE><<<(int)grid, RING_THREADS, RingGeom<double, V, true>::SMEM, s>>>(a);
+    k_step_tet_ring<V, DEP, ONE>
+        <<<(int)grid, TetShape::THREADS, RingGeom<TetShape, double, V, true>::SMEM, s>>>(a);
     return cudaGetLastError();
 }
 
