@@ -250,6 +250,17 @@ ST_API int st_set_step_kernel(st_handle* h, int kind);
  * graph capture, several clouds, tet meshes, the sharded phases and the coupling shims always
  * do).  Results do not depend on the choice.  Default: on. */
 ST_API int st_set_finalize_overlap(st_handle* h, int on);
+/* Failure detection of the ring step kernels: every wait of their shared-memory pipeline
+ * (on a copy into a stage, or on the consumers releasing it) gives up after `cycles` SM clock
+ * cycles, records the fault in the cloud's control block and lets the kernel drain and exit;
+ * the next st_synchronize (or other synchronous call) then returns ST_ERR_CUDA, and that
+ * step's parcels and source are incomplete (set the parcels again).  cycles = 0: the default
+ * of about one second, far above any wait of a correct run.  stall != 0 (with cycles > 0)
+ * tests this path: the consumer warps of every ring block first wait on a barrier that
+ * nothing completes, give up after `cycles`, and the block drains (its own copies in flight
+ * are always waited for, with the default limit, before it exits).  stall = 0 ends the test.
+ * No counterpart in the reference (its kernels have no such waits). */
+ST_API int st_set_wait_limit(st_handle* h, int64_t cycles, int stall);
 
 /* ---- instrumentation --------------------------------------------------------------- */
 enum { ST_KERNEL_STEP = 0, ST_KERNEL_FINALIZE = 1, ST_KERNEL_SORT = 2, ST_KERNEL_PROBE = 3,

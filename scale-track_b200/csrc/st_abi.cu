@@ -155,6 +155,8 @@ struct st_handle {
      * dLfin[par] and sets the next one, and the finalize and clearing of accumulator par run
      * on fin_stream while step n + 1 runs on the handle's stream with the other accumulator. */
     bool fin_overlap = true;
+    int64_t wait_cycles = 0;     /* ring kernels' pipeline-wait limit (st_set_wait_limit),
+                                    negated for the stall test */
     cudaStream_t fin_stream = nullptr;
     cudaEvent_t ev_step[2] = {nullptr, nullptr};
     cudaEvent_t ev_fin[2] = {nullptr, nullptr};
@@ -612,6 +614,7 @@ int do_step(st_handle* h, double dt, double fscale, int phase = PH_ALL)
                    : (const CloudK<P, V>*)h->dclouds;
     a.ctl = h->dctl;
     a.total_tiles = h->total_tiles;
+    a.wait_cycles = h->wait_cycles;
     if (h->p.n_clouds == 1) {
         const std::vector<unsigned char>& hc = h->capturing ? h->hclouds2 : h->hclouds;
         const size_t off = h->capturing ? (size_t)h->cap_parity * sizeof(CloudK<P, V>) : 0;
@@ -664,6 +667,7 @@ int do_step_tet(st_handle* h, double dt, double fscale, int phase)
                    : (const CloudK<double, V>*)h->dclouds;
     a.ctl = h->dctl;
     a.total_tiles = h->total_tiles;
+    a.wait_cycles = h->wait_cycles;
     a.hop_hist = h->d_hops;
     if (h->p.n_clouds == 1) {
         const std::vector<unsigned char>& hc = h->capturing ? h->hclouds2 : h->hclouds;
@@ -2113,6 +2117,17 @@ int st_set_finalize_overlap(st_handle* h, int on)
     DeviceGuard g(h->device);
     if ((rc = drain_fin(h))) return rc;
     h->fin_overlap = on != 0;
+    return ST_OK;
+}
+
+int st_set_wait_limit(st_handle* h, int64_t cycles, int stall)
+{
+    int rc;
+    if ((rc = check_handle(h))) return rc;
+    if (cycles < 0) return fail(ST_ERR_INVALID_ARGUMENT, "st_set_wait_limit: cycles < 0");
+    if (stall && cycles == 0)
+        return fail(ST_ERR_INVALID_ARGUMENT, "st_set_wait_limit: a stall test needs cycles > 0");
+    h->wait_cycles = stall ? -cycles : cycles;
     return ST_OK;
 }
 

@@ -270,6 +270,30 @@ __device__ __forceinline__ void deposit_warp(int32_t key, const V dep[3],
     const int prev = __shfl_up_sync(FULL_MASK, key, 1);
     const bool head = (lane == 0) || (prev != key);
     const unsigned heads = __ballot_sync(FULL_MASK, head);
+    if (DEP == DEP_DET1 && heads == 1u) {
+        /* One cell for the whole warp (dense cells after a re-sort): exact full-warp
+         * reductions replace the scan and lane 0 adds the sum.  With q = hi*2^32 + lo, the
+         * sums of lo's two 16-bit halves stay below 2^21, and |sum of hi| <= 2^30 + 32 because
+         * the headroom bounds the magnitudes of all of a step's deposits together by 2^62. */
+        if (key >= 0) {
+            long long t[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const unsigned lo = (unsigned)(unsigned long long)q[k];
+                const long long shi = __reduce_add_sync(FULL_MASK, (int)(q[k] >> 32));
+                const unsigned s0 = __reduce_add_sync(FULL_MASK, lo & 0xffffu);
+                const unsigned s1 = __reduce_add_sync(FULL_MASK, lo >> 16);
+                t[k] = shi * 4294967296LL + (long long)s0 + (long long)s1 * 65536LL;
+            }
+            if (lane == 0) {
+                unsigned long long* p = acc + 3 * (int64_t)key;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    if (t[k]) atomicAdd(p + k, (unsigned long long)t[k]);
+            }
+        }
+        return;
+    }
     const int segstart = 31 - __clz(heads & (FULL_MASK >> (31 - lane)));
     const bool tail = (lane == 31) || ((heads >> (lane + 1)) & 1u);
     /* A scan of SCAN_STEPS steps sums runs in chunks of SPAN lanes: lane j holds the sum of

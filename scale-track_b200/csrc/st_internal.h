@@ -105,6 +105,8 @@ struct StepArgs {
     CloudCtl* ctl;              /* [nclouds] */
     int64_t total_tiles;        /* warp tiles (32 parcels) over all clouds */
     CloudK<P, V> one;           /* with one cloud: its descriptor, read from parameter space */
+    int64_t wait_cycles = 0;    /* ring kernels: pipeline-wait limit in SM cycles, 0 = ~1 s;
+                                   negative: the failure-detection test (ring_wait_limit) */
 };
 
 /* Unstructured tetrahedral mesh (st_tet.cu). */
@@ -136,6 +138,7 @@ struct TetStepArgs {
     int64_t total_tiles;                 /* warp tiles of WARP_TILE parcels */
     unsigned long long* hop_hist;        /* [8] walk lengths per substep, or nullptr */
     CloudK<double, V> one;               /* with one cloud: its descriptor (kernel parameters) */
+    int64_t wait_cycles = 0;             /* ring kernel: pipeline-wait limit (as StepArgs) */
 };
 
 template <class V>

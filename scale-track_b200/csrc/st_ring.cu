@@ -2,10 +2,10 @@
  * st_ring.cu -- the parcel step of one cloud on the uniform hex mesh as a persistent
  * shared-memory ring (st_ring.cuh), for sm_100a.
  *
- * Sixteen consumer warps step each 1024-parcel tile out of shared memory -- two 32-parcel
- * slices per warp, their cell velocity gathers issued together -- and write the new positions
- * and velocities back into the stage, which the producer warp writes back to HBM with bulk
- * stores.  Arithmetic, deposit and bookkeeping are those of the per-warp kernel (st_step.cuh,
+ * Twenty consumer warps step each 1280-parcel tile out of shared memory (FP64 velocities:
+ * sixteen, 1024) -- two 32-parcel slices per warp, their cell velocity gathers issued
+ * together -- and write the new positions and velocities back into the stage, which the
+ * producer warp writes back to HBM with bulk stores.  Arithmetic, deposit and bookkeeping are those of the per-warp kernel (st_step.cuh,
  * st_device.cuh): positions, velocities, cells and the fixed-point source are bit-identical.
  *
  * Reference: A: run/icoJuliaParcelFoam/cavity3D/asyncParallelTracking.jl
@@ -21,15 +21,28 @@
 
 namespace st {
 
-/* 1024-parcel tiles, 16 consumer warps with two slices each (17 warps: 96 registers) */
+/* Ring shapes, two 32-parcel slices per consumer warp.  FP32 velocities (FP32 and mixed
+ * precision, 40-byte parcels): 1280-parcel tiles and 20 consumer warps (21 warps: 96
+ * registers, four 50 KB stages); measured on the 1e7-parcel step, 1024 x 16, 1152 x 18,
+ * 1216 x 19 and 1280 x 20 took 0.1985, 0.1958, 0.1949 and 0.1943 ms.  FP64 velocities
+ * (56-byte parcels): 1024-parcel tiles and 16 consumer warps, which keep three stages. */
 #ifndef ST_RING_BT
-#define ST_RING_BT 1024
+#define ST_RING_BT 1280
 #endif
 #ifndef ST_RING_CONSUMERS
-#define ST_RING_CONSUMERS 16
+#define ST_RING_CONSUMERS 20
 #endif
-using HexShape = RingShape<ST_RING_BT, ST_RING_CONSUMERS>;
-constexpr int RING_SPW = HexShape::SPW;
+template <class V>
+struct HexShapeOf {
+    using type = RingShape<ST_RING_BT, ST_RING_CONSUMERS>;
+};
+template <>
+struct HexShapeOf<double> {
+    using type = RingShape<1024, 16>;
+};
+constexpr int RING_SPW = 2;
+static_assert(HexShapeOf<float>::type::SPW == RING_SPW && HexShapeOf<double>::type::SPW == RING_SPW,
+              "two slices per consumer warp");
 
 /* Steps parcels j0, j0 + 32, ... (RING_SPW of them, those below nvalid) of the arrays: the
  * state of every slice is read and its cell velocity gathered first, then each slice is
@@ -122,8 +135,10 @@ struct HexRing {
 };
 
 template <class P, class V, int DEP, bool ONE>
-__global__ void __launch_bounds__(HexShape::THREADS, 1) k_step_ring(const StepArgs<P, V> a)
+__global__ void __launch_bounds__(HexShapeOf<V>::type::THREADS, 1)
+    k_step_ring(const StepArgs<P, V> a)
 {
+    using HexShape = typename HexShapeOf<V>::type;
     constexpr bool DET = (DEP == DEP_DET1 || DEP == DEP_DET2);
     Quant qp = {0.0, 0.0, 0.0f, 0.0f, 0, false};
     if (DET) qp = make_quant(a.ctl[0].L, a.ctl[0].H + QUANT_GROWTH_BITS);
@@ -133,7 +148,7 @@ __global__ void __launch_bounds__(HexShape::THREADS, 1) k_step_ring(const StepAr
     HexRing<P, V, DEP, ONE> step{a, DET ? a.one.acc : nullptr,
                                  DEP == DEP_ATOMIC ? a.one.src : nullptr, qp, lane, amax, ovf,
                                  nlost};
-    if (!ring_block<HexShape, P, V, false>(a.one, a.ctl, step)) return;
+    if (!ring_block<HexShape, P, V, false>(a.one, a.ctl, step, a.wait_cycles)) return;
     flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost);
 }
 
@@ -154,7 +169,7 @@ static cudaError_t ring_attr()
     if (ready.load() & bit) return cudaSuccess;
     e = cudaFuncSetAttribute(k_step_ring<P, V, DEP, ONE>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)RingGeom<HexShape, P, V, false>::SMEM);
+                             (int)RingGeom<typename HexShapeOf<V>::type, P, V, false>::SMEM);
     if (e == cudaSuccess) ready.fetch_or(bit);
     return e;
 }
@@ -162,6 +177,7 @@ static cudaError_t ring_attr()
 template <class P, class V, int DEP, bool ONE>
 static cudaError_t launch_ring_t(const StepArgs<P, V>& a, int nsm, cudaStream_t s)
 {
+    using HexShape = typename HexShapeOf<V>::type;
     cudaError_t e = ring_attr<P, V, DEP, ONE>();
     if (e != cudaSuccess) return e;
     const int64_t nfull = a.one.n / HexShape::BT;

@@ -98,14 +98,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
     return ok != 0;
 }
 
+/* The pipeline-wait limit of a launch from its wait_cycles argument: |wait_cycles| when
+ * non-zero, else RING_WAIT_CYCLES.  A negative value also asks for the failure-detection
+ * test: the consumers first wait on a barrier that nothing completes. */
+__device__ __forceinline__ long long ring_wait_limit(long long cycles)
+{
+    return cycles > 0 ? cycles : cycles < 0 ? -cycles : RING_WAIT_CYCLES;
+}
+
 /* Waits until the phase of parity `parity` of the barrier has completed; false when that
- * has not happened within RING_WAIT_CYCLES. */
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+ * has not happened within ring_wait_limit(wait_cycles) SM clock cycles (the limit is worked
+ * out only once the first try has failed). */
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long wait_cycles = 0)
 {
     if (mbar_try_wait(bar, parity)) return true;
+    const long long limit = ring_wait_limit(wait_cycles);
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > RING_WAIT_CYCLES) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 
@@ -202,7 +212,8 @@ __device__ __forceinline__ RingArrays<P, V> ring_stage(unsigned char* stage)
 template <class S, class P, class V, bool CELL>
 __device__ __forceinline__ void ring_producer(const CloudK<P, V>& cl, CloudCtl* ctl, int64_t cnt,
                                               int64_t blk, int64_t nblk, uint32_t sbase,
-                                              uint32_t full0, uint32_t empty0)
+                                              uint32_t full0, uint32_t empty0,
+                                              long long wait_cycles)
 {
     using R = RingGeom<S, P, V, CELL>;
     const uint64_t pol = policy_evict_first();
@@ -213,7 +224,7 @@ __device__ __forceinline__ void ring_producer(const CloudK<P, V>& cl, CloudCtl* 
             /* tile j = k - NS has been stepped in stage j mod NS: write it back */
             const int64_t j = k - R::NS;
             const int s = (int)(j % R::NS);
-            if (!mbar_wait(empty0 + 8 * s, (uint32_t)((j / R::NS) & 1))) {
+            if (!mbar_wait(empty0 + 8 * s, (uint32_t)((j / R::NS) & 1), wait_cycles)) {
                 ok = false;
                 break;
             }
@@ -250,8 +261,9 @@ __device__ __forceinline__ void ring_producer(const CloudK<P, V>& cl, CloudCtl* 
     bulk_wait_all();
     if (!ok) {
         ring_fault(ctl, 1);
-        /* the loads still in flight write into this block's shared memory: wait (bounded)
-         * for the last one issued into every stage before the block may exit */
+        /* the loads still in flight write into this block's shared memory: wait (bounded
+         * by RING_WAIT_CYCLES, whatever the launch's limit) for the last one issued into
+         * every stage before the block may exit */
         for (int s = 0; s < R::NS && s < issued; ++s) {
             const int64_t last = s + ((issued - 1 - s) / R::NS) * R::NS;
             mbar_wait(full0 + 8 * s, (uint32_t)((last / R::NS) & 1));
@@ -263,13 +275,15 @@ __device__ __forceinline__ void ring_producer(const CloudK<P, V>& cl, CloudCtl* 
  * tiles and the consumer warps call step.run<false>(stage arrays, j0, S::BT) per tile and,
  * in the last block, step.run<true>(global arrays, j0, n mod S::BT) for the ragged end
  * (j0 = the lane's first parcel of the warp's slices).  Returns false in the producer warp,
- * which must then return without touching barrier 1 (the consumers' named barrier). */
+ * which must then return without touching barrier 1 (the consumers' named barrier).
+ * wait_cycles: the limit of the pipeline waits (ring_wait_limit). */
 template <class S, class P, class V, bool CELL, class Step>
-__device__ __forceinline__ bool ring_block(const CloudK<P, V>& cl, CloudCtl* ctl, Step& step)
+__device__ __forceinline__ bool ring_block(const CloudK<P, V>& cl, CloudCtl* ctl, Step& step,
+                                           long long wait_cycles)
 {
     using R = RingGeom<S, P, V, CELL>;
     extern __shared__ __align__(128) unsigned char ring_smem[];
-    __shared__ __align__(8) unsigned long long ring_bars[2 * RING_MAX_NS];
+    __shared__ __align__(8) unsigned long long ring_bars[2 * RING_MAX_NS + 1];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t n = cl.n;
@@ -280,25 +294,31 @@ __device__ __forceinline__ bool ring_block(const CloudK<P, V>& cl, CloudCtl* ctl
     const uint32_t sbase = smem_u32(ring_smem);
     const uint32_t full0 = smem_u32(ring_bars);
     const uint32_t empty0 = full0 + 8 * R::NS;
+    const uint32_t never = full0 + 8 * (2 * RING_MAX_NS);   /* the test's barrier: no arrivals */
     if (threadIdx.x == 0) {
         for (int s = 0; s < R::NS; ++s) {
             mbar_init(full0 + 8 * s, 1);
             mbar_init(empty0 + 8 * s, S::CONS);
         }
+        mbar_init(never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
     if (warp == S::CONS) {
-        if (lane == 0) ring_producer<S, P, V, CELL>(cl, ctl, cnt, blk, nblk, sbase, full0, empty0);
+        if (lane == 0)
+            ring_producer<S, P, V, CELL>(cl, ctl, cnt, blk, nblk, sbase, full0, empty0,
+                                         wait_cycles);
         return false;
     }
     const int j0 = warp * (S::SPW * 32) + lane;
     bool ok = true;
-    for (int64_t k = 0; k < cnt; ++k) {
+    if (wait_cycles < 0) ok = __all_sync(FULL_MASK, mbar_wait(never, 0, wait_cycles));
+    for (int64_t k = 0; ok && k < cnt; ++k) {
         const int s = (int)(k % R::NS);
         /* every lane waits; the warp goes on only if all of them saw the stage arrive */
-        ok = __all_sync(FULL_MASK, mbar_wait(full0 + 8 * s, (uint32_t)((k / R::NS) & 1)));
+        ok = __all_sync(FULL_MASK,
+                        mbar_wait(full0 + 8 * s, (uint32_t)((k / R::NS) & 1), wait_cycles));
         if (!ok) break;
         step.template run<false>(ring_stage<S, P, V, CELL>(ring_smem + (size_t)s * R::STAGE), j0,
                                  (int64_t)S::BT);

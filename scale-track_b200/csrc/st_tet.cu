@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(TetShape::THREADS, 1) k_step_tet_ring(const Te
     TetRing<V, DEP, ONE> step{a, DET ? a.one.acc : nullptr,
                               DEP == DEP_ATOMIC ? a.one.src : nullptr, qp, lane, count_hops,
                               amax, ovf, nlost};
-    if (!ring_block<TetShape, double, V, true>(a.one, a.ctl, step)) return;
+    if (!ring_block<TetShape, double, V, true>(a.one, a.ctl, step, a.wait_cycles)) return;
     flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost);
     ring_consumers_sync<TetShape>();
     if (count_hops && threadIdx.x < 8 && s_tet_hist[threadIdx.x])

@@ -39,7 +39,8 @@ EXPORTS = [
     "st_num_cells",
     "st_set_fluid_velocity", "st_set_fluid_velocity_device", "st_step", "st_get_source",
     "st_source_device", "st_synchronize", "st_get_stream", "st_set_stream",
-    "st_profile_enable", "st_profile_read", "st_launch_count", "st_set_step_kernel", "st_set_finalize_overlap", "st_setup",
+    "st_profile_enable", "st_profile_read", "st_launch_count", "st_set_step_kernel", "st_set_finalize_overlap", "st_set_wait_limit",
+    "st_setup",
     "st_set_drag_parameters", "st_shard_set_total", "st_shard_buffers", "st_shard_needs_probe",
     "st_shard_probe", "st_shard_deposit", "st_shard_finish",
     "st_default_handle",
@@ -137,6 +138,7 @@ def lib():
         "st_launch_count": ([c_h], ctypes.c_int64),
         "st_set_step_kernel": ([c_h, ctypes.c_int], ctypes.c_int),
         "st_set_finalize_overlap": ([c_h, ctypes.c_int], ctypes.c_int),
+        "st_set_wait_limit": ([c_h, ctypes.c_int64, ctypes.c_int], ctypes.c_int),
         "st_set_drag_parameters": ([c_h, ctypes.c_double, ctypes.c_double], ctypes.c_int),
         "st_shard_set_total": ([c_h, ctypes.c_int, ctypes.c_int64], ctypes.c_int),
         "st_shard_buffers": ([c_h, P(ctypes.c_void_p), P(ctypes.c_int64), P(ctypes.c_void_p),
@@ -461,6 +463,11 @@ class ParcelTracker:
     def set_finalize_overlap(self, on):
         """Overlap each step's source conversion with the next step (default on)."""
         _check(lib().st_set_finalize_overlap(self._h, 1 if on else 0))
+
+    def set_wait_limit(self, cycles, stall=False):
+        """Limit of the ring kernels' pipeline waits in SM clock cycles (0 = about 1 s);
+        stall=True makes the waits run out (failure-detection test)."""
+        _check(lib().st_set_wait_limit(self._h, int(cycles), 1 if stall else 0))
 
     def set_step_kernel(self, kind):
         """'ring' (default: shared-memory ring of block tiles) or 'warp' (per-warp tiles);

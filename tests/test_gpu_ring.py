@@ -2,7 +2,8 @@
 kernel (ST_STEP_KERNEL_WARP): both run the same parcel arithmetic, so positions, velocities,
 owning cells and the deterministic source must agree bit for bit; the FP64 atomic source adds
 in a different order and agrees to 1e-12.  Sizes cover clouds smaller than one block tile
-(1024 parcels), exact multiples, several tiles per block with a ragged end, and the default
+(1280 parcels in FP32 and mixed precision, 1024 in FP64), exact multiples, several tiles per
+block with a ragged end, and the default
 kernel is also checked against the oracle (the parity tests use it throughout)."""
 import numpy as np
 import pytest
@@ -34,7 +35,7 @@ def run(kind, prec, npcl, steps=3, nsub=1, deposit="deterministic", drag="schill
         return x, u, h.get_cells(), h.get_source()
 
 
-@pytest.mark.parametrize("npcl", [1, 1000, 1024, 3 * 1024, 148 * 1024 * 2 + 517])
+@pytest.mark.parametrize("npcl", [1, 1000, 1024, 1280, 3 * 1280, 148 * 1280 * 2 + 517])
 @pytest.mark.parametrize("prec", ["mixed", "fp64", "fp32"])
 def test_ring_equals_warp_kernel(prec, npcl):
     a = run("ring", prec, npcl)
@@ -62,7 +63,7 @@ def test_ring_atomic_source_fp64():
 
 def test_ring_matches_oracle_many_tiles():
     """Several tiles per block, a ragged end and a re-sort, against the CPU oracle."""
-    npcl, steps = 148 * 1024 * 3 + 333, 3
+    npcl, steps = 148 * 1280 * 3 + 333, 3
     xyz, uvw, d = workload.parcels(npcl, 9)
     U = workload.tgv_field(N, dtype=np.float32)
     fs = [workload.fluid_scale(k) for k in range(steps)]
@@ -158,3 +159,76 @@ def test_tet_ring_equals_warp_kernel(prec, nsub):
     for p, q in zip(out["ring"], out["warp"]):
         assert np.array_equal(p, q)
     assert out["ring"][4][1:].sum() > 0    # the walks did hop
+
+
+@pytest.mark.parametrize("kind", ["ring", "warp"])
+def test_dense_cells_against_oracle(kind):
+    """4^3 cells and 2e5 parcels (about 3000 per cell): after each re-sort nearly every warp
+    holds a single cell, so the deposit takes its full-warp reduction; parcels, cells and the
+    fixed-point source stay bit-exact with the CPU oracle."""
+    n, npcl, steps = 4, 200_000, 3
+    xyz, uvw, d = workload.parcels(npcl, 21)
+    U = workload.tgv_field(n, dtype=np.float32)
+    fs = [workload.fluid_scale(k) for k in range(steps)]
+    prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                    drag_model="schiller_naumann", precision="mixed", n_substeps=1,
+                    sort_interval=1)
+    with st.ParcelTracker(prm, st.mesh_desc(n, 0.0, workload.L_BOX)) as h:
+        h.set_step_kernel(kind)
+        h.set_parcels(xyz, uvw, d)
+        h.set_fluid_velocity(U)
+        for k in range(steps):
+            h.step(workload.DT, fs[k])
+        h.synchronize()
+        gx, gu, _ = h.get_parcels()
+        gc, gs = h.get_cells(), h.get_source()
+    cfg = oracle.make_cfg(n, 0.0, workload.L_BOX, workload.MU_F, workload.RHO_F,
+                          workload.RHO_P, drag="sn_explicit", precision="mixed", n_substeps=1)
+    r = oracle.run(cfg, xyz, uvw, d, U.astype(np.float64), steps, workload.DT, fscale=fs,
+                   nthreads=8)
+    assert r["status"] == 0
+    assert np.array_equal(gx, r["xyz"])
+    assert np.array_equal(gu, r["uvw"])
+    assert np.array_equal(gc, r["cells"])
+    assert np.array_equal(gs, r["src_quant"])
+
+
+def test_bounded_wait_reports_fault_and_recovers():
+    """Failure detection without a fault: in the stall test every ring block's consumers wait
+    on a barrier that nothing completes; after the limit (2e6 cycles, about 1 ms) they record
+    it, the producer's wait for them runs out too, the block drains its copies in flight, and
+    the host gets an error status instead of a hang.  The device stays usable: with the
+    default limit the same handle, given the parcels again, steps to the same results as a
+    fresh handle."""
+    npcl = 148 * 1280 * 2 + 100
+    xyz, uvw, d = workload.parcels(npcl, 23)
+    U = workload.tgv_field(N, dtype=np.float32)
+    prm = st.params(mu_c=workload.MU_F, rho_c=workload.RHO_F, rho_d=workload.RHO_P,
+                    drag_model="schiller_naumann", precision="mixed", n_substeps=1,
+                    sort_interval=0)
+    with st.ParcelTracker(prm, st.mesh_desc(N, 0.0, workload.L_BOX)) as h:
+        h.set_parcels(xyz, uvw, d)
+        h.set_fluid_velocity(U)
+        h.step(workload.DT, 1.0)            # scale set-up and one normal step
+        h.synchronize()
+        h.set_wait_limit(2_000_000, stall=True)
+        h.step(workload.DT, 1.0)
+        with pytest.raises(st.ScaleTrackError) as e:
+            h.synchronize()
+        assert e.value.code == st.ST_ERR_CUDA and "gave up waiting" in str(e.value)
+        assert "fault bits 3" in str(e.value)      # consumers (2) and producer (1)
+        h.set_wait_limit(0)
+        h.set_parcels(xyz, uvw, d)
+        for k in range(2):
+            h.step(workload.DT, 1.0)
+        h.synchronize()
+        a = (*h.get_parcels()[:2], h.get_cells(), h.get_source())
+    with st.ParcelTracker(prm, st.mesh_desc(N, 0.0, workload.L_BOX)) as h:
+        h.set_parcels(xyz, uvw, d)
+        h.set_fluid_velocity(U)
+        for k in range(2):
+            h.step(workload.DT, 1.0)
+        h.synchronize()
+        b = (*h.get_parcels()[:2], h.get_cells(), h.get_source())
+    for p, q in zip(a, b):
+        assert np.array_equal(p, q)
