@@ -84,9 +84,13 @@ __global__ void __launch_bounds__(256, MinBlocks<V, ONE>::value) k_step(const St
     AmaxT<V> amax = (V)0;
     unsigned ovf = 0, nlost = 0;
 
-    /* Software pipeline over the warp's tiles: the streaming loads of the next tile are
-     * issued before the current tile is stepped, so each warp keeps two tiles of parcel data
-     * in flight and the HBM latency overlaps the arithmetic. */
+    /* Software pipeline over the warp's tiles (one substep): the streaming loads of the next
+     * tile are issued before the current tile is stepped, so each warp keeps two tiles of
+     * parcel data in flight and the HBM latency overlaps the arithmetic.  With several
+     * substeps the kernel is bound by their arithmetic, the loads are a small share of it,
+     * and the second tile's registers would spill in the substep loop: each tile is loaded
+     * when it is stepped. */
+    constexpr bool AHEAD = ONE;
     struct Raw {
         P X[SLICES], Y[SLICES], Z[SLICES];
         V Uv[SLICES], Vv[SLICES], Wv[SLICES], D[SLICES];
@@ -111,9 +115,12 @@ __global__ void __launch_bounds__(256, MinBlocks<V, ONE>::value) k_step(const St
         }
     };
     Raw R, RN;
-    if (warp0 < a.total_tiles) load(warp0, R);
+    if (AHEAD && warp0 < a.total_tiles) load(warp0, R);
     for (int64_t tile = warp0; tile < a.total_tiles; tile += nwarps) {
-        if (tile + nwarps < a.total_tiles) load(tile + nwarps, RN);
+        if (!AHEAD)
+            load(tile, R);
+        else if (tile + nwarps < a.total_tiles)
+            load(tile + nwarps, RN);
         const int c = SINGLE ? 0 : find_cloud(a, tile);
         if (c != cur) {
             if (cur >= 0) flush_ctl<DEP>(a.ctl + cur, lane, amax, ovf, nlost);
@@ -123,12 +130,6 @@ __global__ void __launch_bounds__(256, MinBlocks<V, ONE>::value) k_step(const St
         const CloudK<P, V>& cl = SINGLE ? a.one : a.clouds[c];
         const int64_t n = cl.n;
         const int64_t base = (tile - cl.tile0) * TILE + lane;
-        P* const xp = cl.x;
-        P* const yp = cl.y;
-        P* const zp = cl.z;
-        V* const up = cl.u;
-        V* const vp = cl.v;
-        V* const wp = cl.w;
         unsigned long long* const acc = DET ? cl.acc : nullptr;
         double* const src = (DEP == DEP_ATOMIC) ? cl.src : nullptr;
         P X[SLICES], Y[SLICES], Z[SLICES];
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(256, MinBlocks<V, ONE>::value) k_step(const St
             X[s] = R.X[s]; Y[s] = R.Y[s]; Z[s] = R.Z[s];
             Uv[s] = R.Uv[s]; Vv[s] = R.Vv[s]; Wv[s] = R.Wv[s]; D[s] = R.D[s];
         }
-        R = RN;
+        if (AHEAD) R = RN;
         /* phase 2: start cells (A:1286) and raw cell velocities (A:1288; the fluid factor is
          * applied in the slip) */
         int32_t pI[SLICES];
@@ -181,12 +182,14 @@ __global__ void __launch_bounds__(256, MinBlocks<V, ONE>::value) k_step(const St
                     ++nlost;
                     key = -1;
                 } else if (DEP != DEP_PROBE) {                                   /* A:1355-1360 */
-                    st_stream(xp + i, pos[0]);
-                    st_stream(yp + i, pos[1]);
-                    st_stream(zp + i, pos[2]);
-                    st_stream(up + i, vel[0]);
-                    st_stream(vp + i, vel[1]);
-                    st_stream(wp + i, vel[2]);
+                    /* the array pointers are read here, after the substeps, not held in
+                     * registers through them */
+                    st_stream(cl.x + i, pos[0]);
+                    st_stream(cl.y + i, pos[1]);
+                    st_stream(cl.z + i, pos[2]);
+                    st_stream(cl.u + i, vel[0]);
+                    st_stream(cl.v + i, vel[1]);
+                    st_stream(cl.w + i, vel[2]);
                 }
             }
             deposit_warp<DEP, V>(key, dep, acc, src, qp, lane, amax, ovf);

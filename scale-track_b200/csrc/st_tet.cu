@@ -303,10 +303,6 @@ __device__ __forceinline__ void tet_parcel(const TetStepArgs<V>& a, int nsub, do
     cell = tNew;
 }
 
-#ifndef ST_TET_PREFETCH_NEXT
-#define ST_TET_PREFETCH_NEXT 0
-#endif
-
 /* Resident blocks of 256 threads per SM the compiler must allow: 4 (64 registers). */
 #ifndef ST_TET_MIN_BLOCKS
 #define ST_TET_MIN_BLOCKS 4
@@ -344,18 +340,6 @@ __global__ void __launch_bounds__(256, TetMinBlocks<V>::value) k_step_tet(const 
         const int64_t n = __ldg(&cl->n);
         unsigned long long* const acc = DET ? cl->acc : nullptr;
         double* const src = (DEP == DEP_ATOMIC) ? cl->src : nullptr;
-#if ST_TET_PREFETCH_NEXT
-        /* the owning tets of this warp's next tile (same cloud): their FP32 planes and cell
-         * velocities towards L2 now, so that the next tile's first gathers hit L2 */
-        if (WARP_TILE == 32 && tile + nwarps < a.total_tiles) {
-            const int64_t inext = (tile + nwarps - __ldg(&cl->tile0)) * WARP_TILE + lane;
-            if (inext < n) {
-                const int32_t cn = ld_stream(cl->cell + inext);
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(a.mesh.planes32 + 4 * (int64_t)cn));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(a.U + 3 * (int64_t)cn));
-            }
-        }
-#endif
         for (int sl = 0; sl < WARP_TILE / 32; ++sl) {
         const int64_t i = (tile - __ldg(&cl->tile0)) * WARP_TILE + 32 * sl + lane;
         int32_t key = -1;
