@@ -101,7 +101,12 @@ struct Quant {
     float thr_f;    /* 2^(cap+L) as float, when `fast` */
     int L;
     bool fast;
+    float thr_small; /* 2^(SMALL_Q_BITS+L) as float when that is a normal float, else 0 */
 };
+
+/* Quantised deposits below 2^SMALL_Q_BITS in magnitude: a sum of up to four of them fits in
+ * a 32-bit integer (the warp run reduction's 32-bit path). */
+constexpr int SMALL_Q_BITS = 29;
 
 __device__ __forceinline__ Quant make_quant(int L, int cap)
 {
@@ -112,6 +117,9 @@ __device__ __forceinline__ Quant make_quant(int L, int cap)
     q.fast = (-L >= -126 && -L <= 127) && (cap + L >= -126 && cap + L <= 127);
     q.scale_f = q.fast ? st_pow2if(-L) : 0.0f;
     q.thr_f = q.fast ? st_pow2if(cap + L) : 0.0f;
+    q.thr_small = (q.fast && SMALL_Q_BITS + L >= -126 && SMALL_Q_BITS + L <= 127)
+                      ? st_pow2if(SMALL_Q_BITS + L)
+                      : 0.0f;
     return q;
 }
 
@@ -265,11 +273,65 @@ __device__ __forceinline__ void deposit_warp(int32_t key, const V dep[3],
         if (key >= 0) deposit_direct<DEP_ATOMIC, V>(dep, key, acc, src, qp, amax, ovf);
         return;
     }
-    long long q[3] = {0, 0, 0};
-    if (key >= 0) quantize3(dep, qp, amax, ovf, q);
     const int prev = __shfl_up_sync(FULL_MASK, key, 1);
     const bool head = (lane == 0) || (prev != key);
     const unsigned heads = __ballot_sync(FULL_MASK, head);
+    if constexpr (DEP == DEP_DET1 && sizeof(V) == 4) {
+        /* 32-bit path: when every lane's deposit components quantise below 2^SMALL_Q_BITS
+         * (|d0| + |d1| + |d2| below 2^(SMALL_Q_BITS+L), the bound argument of quantize3), the
+         * integers are those of quantize3, a chunk of SPAN <= 4 lanes sums below 2^31, and the
+         * run sums are formed in 32-bit registers: the same integers reach the accumulators. */
+        int q32[3] = {0, 0, 0};
+        bool small = key < 0;
+        if (key >= 0) {
+            const float a0 = fabsf((float)dep[0]), a1 = fabsf((float)dep[1]),
+                        a2 = fabsf((float)dep[2]);
+            if ((a0 + a1) + a2 < qp.thr_small) {
+                amax = fmaxf(amax, fmaxf(fmaxf(a0, a1), a2));
+#pragma unroll
+                for (int k = 0; k < 3; ++k) q32[k] = __float2int_rn((float)dep[k] * qp.scale_f);
+                small = true;
+            }
+        }
+        static_assert(SPAN <= 4, "32-bit chunk sums");
+        if (__all_sync(FULL_MASK, small)) {
+            if (heads == 1u) {
+                /* one cell for the whole warp: 16-bit halves, each sum exact in 32 bits */
+                if (key >= 0) {
+                    long long t[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int shi = __reduce_add_sync(FULL_MASK, q32[k] >> 16);
+                        const unsigned slo = __reduce_add_sync(FULL_MASK, (unsigned)q32[k] & 0xffffu);
+                        t[k] = (long long)shi * 65536LL + (long long)slo;
+                    }
+                    if (lane == 0) {
+                        unsigned long long* p = acc + 3 * (int64_t)key;
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            if (t[k]) atomicAdd(p + k, (unsigned long long)t[k]);
+                    }
+                }
+                return;
+            }
+            const int segstart = 31 - __clz(heads & (FULL_MASK >> (31 - lane)));
+            const bool tail = (lane == 31) || ((heads >> (lane + 1)) & 1u);
+            const unsigned tails = __ballot_sync(FULL_MASK, tail);
+            const int tailpos = lane + __ffs(tails >> lane) - 1;
+            const bool emit = ((tailpos - lane) & (SPAN - 1)) == 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) q32[k] = seg_scan(q32[k], lane, segstart);
+            if (emit && key >= 0) {
+                unsigned long long* p = acc + 3 * (int64_t)key;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    if (q32[k]) atomicAdd(p + k, (unsigned long long)(long long)q32[k]);
+            }
+            return;
+        }
+    }
+    long long q[3] = {0, 0, 0};
+    if (key >= 0) quantize3(dep, qp, amax, ovf, q);
     if (DEP == DEP_DET1 && heads == 1u) {
         /* One cell for the whole warp (dense cells after a re-sort): exact full-warp
          * reductions replace the scan and lane 0 adds the sum.  With q = hi*2^32 + lo, the
