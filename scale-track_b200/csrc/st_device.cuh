@@ -37,6 +37,34 @@ __device__ __forceinline__ V slip(V Ur, V fs_hi, V fs_lo, V vel)
     else return Ur * fs_hi - vel;
 }
 
+/* x^0.687 in single precision (st_pow0687f) with its exponent factor, which depends only on
+ * the binary exponent e of x, read from a table in shared memory.  The table is filled on
+ * the device by st_pow0687f_efac itself, so the result is st_pow0687f's bit for bit.  A
+ * kernel that calls pow0687f_tab fills the table (pow_tab_fill) and synchronises its block
+ * first. */
+constexpr int POW_TAB_EMIN = -150;   /* st_pow0687f_mant gives -149 <= e <= 128 */
+constexpr int POW_TAB_N = 280;
+__shared__ float2 s_pow_tab[POW_TAB_N];
+
+__device__ __forceinline__ void pow_tab_fill()
+{
+    for (int i = threadIdx.x; i < POW_TAB_N; i += blockDim.x) {
+        float q, s2k;
+        st_pow0687f_efac(i + POW_TAB_EMIN, &q, &s2k);
+        s_pow_tab[i] = make_float2(q, s2k);
+    }
+}
+
+__device__ __forceinline__ float pow0687f_tab(float x)
+{
+    if (!(x > 0.0f)) return x != x ? x : 0.0f;
+    if ((__float_as_uint(x) >> 23) == 0xffu) return x;   /* +inf */
+    int e;
+    const float p = st_pow0687f_mant(x, &e);
+    const float2 qs = s_pow_tab[e - POW_TAB_EMIN];
+    return (p * qs.x) * qs.y;
+}
+
 /* floor(label, v) (A:668-670); values outside int32 mark the parcel as lost.  floor(v) lies
  * in [-2^31, 2^31) exactly when v does (both bounds are integers), so the range test is made
  * on v and one round-down conversion gives the label. */

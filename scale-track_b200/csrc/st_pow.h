@@ -186,12 +186,12 @@ ST_HD float st_fmaf(float a, float b, float c)
  * evaluated by Horner's rule with fma, the last by the exponent field.  All arithmetic is
  * single precision or integer; nothing is converted to double.
  * Within 2 ulp of the correctly rounded value for every normal and subnormal x (the CPU
- * tests check this against a double-precision reference). */
-ST_HD float st_pow0687f(float x)
+ * tests check this against a double-precision reference).
+ *
+ * st_pow0687f_mant: for finite x > 0, the first factor p and the exponent e. */
+ST_HD float st_pow0687f_mant(float x, int* ep)
 {
-    if (!(x > 0.0f)) return x != x ? x : 0.0f;
     uint32_t b = st_bits_of_f(x);
-    if ((b >> 23) == 0xff) return x;               /* +inf */
     int e = 0;
     if ((b >> 23) == 0) {                          /* subnormal */
         x = x * 16777216.0f;                       /* 2^24, exact */
@@ -214,7 +214,15 @@ ST_HD float st_pow0687f(float x)
     p = st_fmaf(p, t, -0x1.b862bep-4f);
     p = st_fmaf(p, t, 0x1.5fbe76p-1f);
     p = st_fmaf(p, t, 1.0f);
-    const int y = 687 * e;                         /* |y| <= 102363 */
+    *ep = e;                                       /* -149 <= e <= 128 */
+    return p;
+}
+
+/* The exponent factor of x^0.687 = p * q * 2^k for x = 2^e m: q = 2^(r/1000) and s2k = 2^k,
+ * which depend on e alone (callers may tabulate them). */
+ST_HD void st_pow0687f_efac(int e, float* q_out, float* s2k_out)
+{
+    const int y = 687 * e;                         /* |y| <= 103050 */
     const int k = y >= 0 ? y / 1000 : -((999 - y) / 1000);   /* floor(y / 1000) */
     const float r = (float)(y - 1000 * k);         /* exact integer in [0, 1000) */
     float q = 0x1.08638ep-72f;
@@ -224,7 +232,19 @@ ST_HD float st_pow0687f(float x)
     q = st_fmaf(q, r, 0x1.01f20ep-22f);
     q = st_fmaf(q, r, 0x1.6b689cp-11f);
     q = st_fmaf(q, r, 1.0f);
-    return (p * q) * st_pow2if(k);                 /* -103 <= k <= 87 */
+    *q_out = q;
+    *s2k_out = st_pow2if(k);                       /* -104 <= k <= 88 */
+}
+
+ST_HD float st_pow0687f(float x)
+{
+    if (!(x > 0.0f)) return x != x ? x : 0.0f;
+    if ((st_bits_of_f(x) >> 23) == 0xff) return x;   /* +inf */
+    int e;
+    const float p = st_pow0687f_mant(x, &e);
+    float q, s2k;
+    st_pow0687f_efac(e, &q, &s2k);
+    return (p * q) * s2k;
 }
 
 #endif /* ST_POW_H */

@@ -110,7 +110,7 @@ __device__ __forceinline__ void evolve_parcel(const StepArgs<P, V>& a, P pos[3],
             V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
             V Re = (mag * d) * ph.rnu;
             V pw;
-            if (sizeof(V) == 4) pw = (V)st_pow0687f((float)Re);
+            if (sizeof(V) == 4) pw = (V)pow0687f_tab((float)Re);
             else pw = (V)st_pow0687((double)Re);
             V g = f * ((V)1 + (V)0.15 * pw);
 #pragma unroll
