@@ -82,8 +82,6 @@ struct CloudBufs {
     int32_t* cell[2] = {nullptr, nullptr};  /* owning tet (tet meshes) */
     uint32_t* keys[2] = {nullptr, nullptr};
     uint32_t* perm[2] = {nullptr, nullptr};
-    void* temp = nullptr;
-    size_t temp_bytes = 0;
     int cur = 0;
 };
 
@@ -165,7 +163,8 @@ struct st_handle {
     unsigned long long* dacc2 = nullptr;
     int32_t* dLfin = nullptr;  /* [2][nclouds] */
     bool shard_probed = false; /* st_shard_probe ran; its exponents are in dexp */
-    int key_bits = 32;
+    int key_bits = 24;     /* bits of the sort key, at most COUNT_SORT_MAX_BITS */
+    int key_shift = 0;     /* low bits dropped to fit them (sort keys are for locality only) */
     bool morton = true;
     int64_t total_tiles = 0;
     int64_t launches = 0;
@@ -426,8 +425,6 @@ SortBufs<P, V> sort_bufs(const st_handle* h, CloudBufs& c)
         b.keys[k] = c.keys[k];
         b.perm[k] = c.perm[k];
     }
-    b.temp = c.temp;
-    b.temp_bytes = c.temp_bytes;
     return b;
 }
 
@@ -473,7 +470,8 @@ int do_sort_all(st_handle* h)
         int nl = 0;
         {
             ProfScope ps(h, ST_KERNEL_SORT);
-            CK(sort_cloud<P, V>(b, c.cur, c.n, mk, h->key_bits, h->morton, h->stream, &nl));
+            CK(sort_cloud<P, V>(b, c.cur, c.n, mk, h->key_bits, h->key_shift, h->morton, h->stream,
+                                &nl));
         }
         h->launches += nl;
         c.cur = 1 - c.cur;
@@ -724,10 +722,6 @@ int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
             CK(cudaMalloc(&c.keys[k], (size_t)n * sizeof(uint32_t)));
             CK(cudaMalloc(&c.perm[k], (size_t)n * sizeof(uint32_t)));
         }
-        if (c.temp) cudaFree(c.temp);
-        c.temp = nullptr;
-        c.temp_bytes = sort_temp_bytes<P, V>(n);
-        CK(cudaMalloc(&c.temp, c.temp_bytes > 0 ? c.temp_bytes : 16));
         c.cap = n;
     }
     c.n = n;
@@ -803,8 +797,8 @@ int do_set_parcels(st_handle* h, int cloud, int64_t n, const double* xyz, const 
         SortBufs<P, V> b = sort_bufs<P, V>(h, cc);
         int nl = 0;
         ProfScope ps(h, ST_KERNEL_SORT);
-        CK(sort_cloud<P, V>(b, cc.cur, cc.n, mesh_k<P>(h), h->key_bits, h->morton, h->stream,
-                            &nl));
+        CK(sort_cloud<P, V>(b, cc.cur, cc.n, mesh_k<P>(h), h->key_bits, h->key_shift, h->morton,
+                            h->stream, &nl));
         h->launches += nl;
         cc.cur = 1 - cc.cur;
     }
@@ -848,9 +842,7 @@ int do_append_parcels(st_handle* h, int cloud, int64_t m, const double* xyz, con
             ok = ok && (nkeys[k] = grab((size_t)cap * sizeof(uint32_t))) != nullptr;
             ok = ok && (nperm[k] = grab((size_t)cap * sizeof(uint32_t))) != nullptr;
         }
-        const size_t tb = sort_temp_bytes<P, V>(cap);
-        void* ntemp = ok ? grab(tb > 0 ? tb : 16) : nullptr;
-        if (!ok || !ntemp) {
+        if (!ok) {
             for (void* p : fresh) cudaFree(p);
             cudaGetLastError();
             return fail(ST_ERR_OUT_OF_MEMORY, "no device memory for %lld parcels", (long long)cap);
@@ -869,9 +861,6 @@ int do_append_parcels(st_handle* h, int cloud, int64_t m, const double* xyz, con
             c.keys[k] = (uint32_t*)nkeys[k];
             c.perm[k] = (uint32_t*)nperm[k];
         }
-        if (c.temp) cudaFree(c.temp);
-        c.temp = ntemp;
-        c.temp_bytes = tb;
         c.cap = cap;
         c.cur = 0;
         h->clouds_dirty = true;
@@ -1033,7 +1022,6 @@ void free_cloud(CloudBufs& c)
         for (void* p : arrs)
             if (p) cudaFree(p);
     }
-    if (c.temp) cudaFree(c.temp);
     c = CloudBufs();
 }
 
@@ -1456,9 +1444,12 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
         int b = 1;
         int nmax = std::max(m->n[0], std::max(m->n[1], m->n[2]));
         while ((1 << b) < nmax) ++b;
-        h->key_bits = 3 * b;
+        h->key_shift = std::max(0, b - COUNT_SORT_MAX_BITS / 3);
+        h->key_bits = 3 * (b - h->key_shift);
     } else {
-        h->key_bits = quant_nbits(ncells);
+        const int b = quant_nbits(ncells);
+        h->key_shift = std::max(0, b - COUNT_SORT_MAX_BITS);
+        h->key_bits = b - h->key_shift;
     }
     h->block = p->block_size ? p->block_size : 256;
     h->clouds.resize(p->n_clouds);
@@ -1488,7 +1479,7 @@ static int create_impl(const st_params* p, const st_mesh_desc* m, int64_t ncells
         (e = cudaMemsetAsync(h->dacc, 0, cells_total * h->limbs * 8, h->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->dcounter, 0, sizeof(unsigned int), h->stream)) != cudaSuccess)
         return bail(fail(ST_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e)));
-    if (h->key_bits <= COUNT_SORT_MAX_BITS) {
+    {
         const size_t nb = (size_t)1 << h->key_bits;
         h->scan_bytes = count_sort_scan_bytes(h->key_bits);
         if ((e = cudaMalloc((void**)&h->dbins, nb * sizeof(uint32_t))) != cudaSuccess ||

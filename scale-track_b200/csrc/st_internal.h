@@ -262,22 +262,20 @@ struct SortBufs {
     int32_t* cell[2];       /* tet meshes: owning tet, sorted along; nullptr on hex meshes */
     uint32_t* keys[2];
     uint32_t* perm[2];
-    void* temp;
-    size_t temp_bytes;
     /* counting sort (key range of at most 2^COUNT_SORT_MAX_BITS): per-key counts and
-     * offsets, shared by the clouds of a handle; nullptr selects the radix sort */
+     * offsets, shared by the clouds of a handle */
     uint32_t* bins;
     uint32_t* offsets;
     void* scan_temp;
     size_t scan_temp_bytes;
 };
 constexpr int COUNT_SORT_MAX_BITS = 24;
-template <class P, class V>
-size_t sort_temp_bytes(int64_t n);
 size_t count_sort_scan_bytes(int key_bits);
+/* key_bits: bits of the (coarsened) key, at most COUNT_SORT_MAX_BITS; key_shift: low bits
+ * dropped from each Morton coordinate, the linear cell index or the owning tet */
 template <class P, class V>
 cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& mesh, int key_bits,
-                       bool morton, cudaStream_t s, int* launches);
+                       int key_shift, bool morton, cudaStream_t s, int* launches);
 template <class P, class V>
 cudaError_t unpermute_cloud(SortBufs<P, V>& b, int cur, int64_t n, cudaStream_t s);
 cudaError_t cells_unpermute(const int32_t* id, const int32_t* cell, int64_t n, int32_t* out,

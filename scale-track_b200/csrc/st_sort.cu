@@ -6,19 +6,19 @@
  * reduction of the deposit collapses most of a tile into a few atomics, and neighbouring
  * warps gather neighbouring cells of U (L2 locality).  Keys are the Morton code of the cell
  * (i, j, k) (the linear cell index for meshes wider than 1024 cells, the owning tet on tet
- * meshes).  Key ranges of at most 2^24 values are ranked by a counting sort: per-key counts
- * with warp-aggregated atomics, an exclusive scan of the counts (two kernels of this file),
- * then each warp claims its slots of each
- * key with one atomic.  Parcels of one key keep their order inside a warp; across warps it
- * follows the order of the atomics, which no result depends on (the deposit is an exact
- * integer sum and everything else is per parcel).  Wider key ranges use CUB's LSD radix
- * sort.  Then every SoA array and the parcel id are gathered out of place into the other
- * buffer.  The reference has no re-sort: its parcels keep their Hilbert ordered initial
- * positions inside each chunk (A:559-638).
+ * meshes).  A key range wider than 2^24 values is coarsened to 2^24 by dropping low bits
+ * (of each of i, j, k for Morton keys, of the index otherwise): neighbouring cells then share
+ * a key, which keeps the locality the sort is for.  Keys are ranked by a counting sort: per-key
+ * counts with warp-aggregated atomics, an exclusive scan of the counts (two kernels of this
+ * file), then each warp claims its slots of each key with one atomic.  Parcels of one key keep
+ * their order inside a warp; across warps it follows the order of the atomics, which no
+ * result depends on (the deposit is an exact integer sum and everything else is per parcel).
+ * Then every SoA array and the parcel id are gathered out of place into the other buffer.
+ * The reference has no re-sort: its parcels keep their Hilbert ordered initial positions
+ * inside each chunk (A:559-638).
  */
 #include <cstdint>
 #include <cuda_runtime.h>
-#include <cub/device/device_radix_sort.cuh>
 
 #include "st_internal.h"
 
@@ -50,20 +50,21 @@ __device__ __forceinline__ void cell_ijk(const MeshK<P>& m, P x, P y, P z, int32
     k = fz < (P)0 ? 0 : (fz >= (P)m.N[2] ? m.N[2] - 1 : (int32_t)fz);
 }
 
+/* shift: low bits dropped (of each of i, j, k for Morton keys, of the index otherwise) */
 template <class P>
 __global__ void k_sort_keys(const P* __restrict__ x, const P* __restrict__ y,
                             const P* __restrict__ z, int64_t n, MeshK<P> m, int morton,
-                            uint32_t* __restrict__ keys, uint32_t* __restrict__ perm)
+                            int shift, uint32_t* __restrict__ keys)
 {
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (int64_t)gridDim.x * blockDim.x) {
         int32_t i, j, k;
         cell_ijk(m, x[p], y[p], z[p], i, j, k);
-        uint32_t key = morton ? (spread3((uint32_t)i) | (spread3((uint32_t)j) << 1) |
-                                 (spread3((uint32_t)k) << 2))
-                              : (uint32_t)(k * m.NxNy + j * m.N[0] + i);
+        const uint32_t key =
+            morton ? (spread3((uint32_t)i >> shift) | (spread3((uint32_t)j >> shift) << 1) |
+                      (spread3((uint32_t)k >> shift) << 2))
+                   : ((uint32_t)(k * m.NxNy + j * m.N[0] + i) >> shift);
         keys[p] = key;
-        if (perm) perm[p] = (uint32_t)p;
     }
 }
 
@@ -71,15 +72,14 @@ __global__ void k_sort_keys(const P* __restrict__ x, const P* __restrict__ y,
  * issues all their (scattered) loads before any store, so that many reads are in flight. */
 constexpr int GATHER_ILP = 2;
 
-/* tet meshes: the key is the owning tet (tets are numbered with spatial locality) */
-__global__ void k_sort_keys_cell(const int32_t* __restrict__ cell, int64_t n,
-                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ perm)
+/* tet meshes: the key is the owning tet (tets are numbered with spatial locality), less
+ * `shift` low bits */
+__global__ void k_sort_keys_cell(const int32_t* __restrict__ cell, int64_t n, int shift,
+                                 uint32_t* __restrict__ keys)
 {
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
-         p += (int64_t)gridDim.x * blockDim.x) {
-        keys[p] = (uint32_t)cell[p];
-        if (perm) perm[p] = (uint32_t)p;
-    }
+         p += (int64_t)gridDim.x * blockDim.x)
+        keys[p] = (uint32_t)cell[p] >> shift;
 }
 
 /* out[id[p]] = cell[p] */
@@ -412,48 +412,29 @@ static int grid_for(int64_t n)
 }
 
 template <class P, class V>
-size_t sort_temp_bytes(int64_t n)
-{
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t*)nullptr,
-                                    (uint32_t*)nullptr, (const uint32_t*)nullptr,
-                                    (uint32_t*)nullptr, (int)n, 0, 32);
-    return bytes;
-}
-
-template <class P, class V>
 cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& mesh, int key_bits,
-                       bool morton, cudaStream_t s, int* launches)
+                       int key_shift, bool morton, cudaStream_t s, int* launches)
 {
     if (n <= 1) return cudaSuccess;
+    if (!b.bins || key_bits > COUNT_SORT_MAX_BITS) return cudaErrorInvalidValue;
     const int o = 1 - cur;
-    const bool counting = b.bins && key_bits <= COUNT_SORT_MAX_BITS;
-    uint32_t* const iota = counting ? nullptr : b.perm[0];   /* the radix sort's values */
     if (b.cell[cur])
-        k_sort_keys_cell<<<grid_for(n), 256, 0, s>>>(b.cell[cur], n, b.keys[0], iota);
+        k_sort_keys_cell<<<grid_for(n), 256, 0, s>>>(b.cell[cur], n, key_shift, b.keys[0]);
     else
         k_sort_keys<P><<<grid_for(n), 256, 0, s>>>(b.x[cur], b.y[cur], b.z[cur], n, mesh,
-                                                   morton ? 1 : 0, b.keys[0], iota);
+                                                   morton ? 1 : 0, key_shift, b.keys[0]);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (counting) {
-        const int64_t nbins = (int64_t)1 << key_bits;
-        if ((e = cudaMemsetAsync(b.bins, 0, nbins * sizeof(uint32_t), s)) != cudaSuccess) return e;
-        const int wg = grid_for(n);
-        k_bin_count<<<wg, 256, 0, s>>>(b.keys[0], n, (uint32_t)nbins, b.bins);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if ((e = scan_counts(b.bins, b.offsets, nbins, static_cast<uint32_t*>(b.scan_temp),
-                             s)) != cudaSuccess)
-            return e;
-        k_bin_rank<<<wg, 256, 0, s>>>(b.keys[0], n, (uint32_t)nbins, b.offsets, b.perm[1]);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if (launches) *launches += 4;
-    } else {
-        size_t bytes = b.temp_bytes;
-        e = cub::DeviceRadixSort::SortPairs(b.temp, bytes, b.keys[0], b.keys[1], b.perm[0],
-                                            b.perm[1], (int)n, 0, key_bits, s);
-        if (e != cudaSuccess) return e;
-    }
+    const int64_t nbins = (int64_t)1 << key_bits;
+    if ((e = cudaMemsetAsync(b.bins, 0, nbins * sizeof(uint32_t), s)) != cudaSuccess) return e;
+    const int wg = grid_for(n);
+    k_bin_count<<<wg, 256, 0, s>>>(b.keys[0], n, (uint32_t)nbins, b.bins);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = scan_counts(b.bins, b.offsets, nbins, static_cast<uint32_t*>(b.scan_temp), s)) !=
+        cudaSuccess)
+        return e;
+    k_bin_rank<<<wg, 256, 0, s>>>(b.keys[0], n, (uint32_t)nbins, b.offsets, b.perm[1]);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int64_t gblocks = (n + 256 * GATHER_ILP - 1) / (256 * GATHER_ILP);
     if (gblocks > 148 * 64) gblocks = 148 * 64;
     k_gather<P, V><<<(int)gblocks, 256, 0, s>>>(b.perm[1], n, b.x[cur], b.y[cur], b.z[cur],
@@ -461,7 +442,8 @@ cudaError_t sort_cloud(SortBufs<P, V>& b, int cur, int64_t n, const MeshK<P>& me
                                                b.id[cur], b.x[o], b.y[o], b.z[o], b.u[o],
                                                b.v[o], b.w[o], b.d[o], b.id[o], b.cell[cur],
                                                b.cell[o]);
-    if (launches) *launches += 2;  /* our keys and gather kernels; CUB's own are not counted */
+    /* keys, counts, the two scan kernels, slots, gather */
+    if (launches) *launches += 6;
     return cudaGetLastError();
 }
 
@@ -510,9 +492,8 @@ cudaError_t cells_unpermute(const int32_t* id, const int32_t* cell, int64_t n, i
 }
 
 #define ST_INST(P, V)                                                                         \
-    template size_t sort_temp_bytes<P, V>(int64_t);                                           \
     template cudaError_t sort_cloud<P, V>(SortBufs<P, V>&, int, int64_t, const MeshK<P>&, int, \
-                                          bool, cudaStream_t, int*);                          \
+                                          int, bool, cudaStream_t, int*);                     \
     template cudaError_t unpermute_cloud<P, V>(SortBufs<P, V>&, int, int64_t, cudaStream_t); \
     template cudaError_t sample_cloud<P, V>(SortBufs<P, V>&, int, int64_t, const MeshK<P>&,    \
                                             const int32_t*, int64_t, double*, int32_t*,        \

@@ -2,8 +2,10 @@
 re-sort during stepping, the device-side order (st_get_order) is a permutation that groups
 parcels by owning cell in key order (the Morton code of the cell on cuboid meshes up to 1024
 cells per axis, the linear cell index on wider ones, the owning tet on tet meshes).  Key ranges
-up to 2^24 values use the counting sort, wider ones the radix sort; both are covered.  Results
-do not depend on the order (the parity tests compare runs with and without re-sorting)."""
+wider than 2^24 values are coarsened by dropping low bits (of each Morton coordinate, or of the
+index), so the library's counting sort serves every mesh; both kinds of coarsening are
+covered.  Results do not depend on the order (the parity tests compare runs with and without
+re-sorting)."""
 import numpy as np
 import pytest
 
@@ -63,9 +65,9 @@ def test_cuboid_resort_groups_parcels_by_morton_key(n, prec):
         assert np.array_equal(np.sort(order), np.arange(m, dtype=np.int32))
 
 
-def test_wide_mesh_uses_the_radix_sort_by_linear_cell():
-    """1100 x 1100 x 14 cells (more than 2^24, wider than 1024): linear cell keys through the
-    radix sort."""
+def test_wide_mesh_sorts_by_coarsened_linear_cell():
+    """1100 x 1100 x 14 cells (more than 2^24, wider than 1024): linear cell keys less their
+    lowest bit (25-bit indices, 24-bit keys)."""
     dims = (1100, 1100, 14)
     m = 100000
     rng = np.random.default_rng(3)
@@ -75,12 +77,39 @@ def test_wide_mesh_uses_the_radix_sort_by_linear_cell():
     mesh = st.mesh_desc(dims, 0.0, L)
     with st.ParcelTracker(_params(sort_interval=3), mesh) as h:
         h.set_parcels(xyz, uvw, d)
-        _check_grouped(h.get_order(), h.get_cells().astype(np.int64))
+        _check_grouped(h.get_order(), h.get_cells().astype(np.int64) >> 1)
         h.set_fluid_velocity(np.zeros((int(np.prod(dims)), 3), np.float32))
         for s in range(3):
             h.step(workload.DT, 1.0)
         h.synchronize()
-        _check_grouped(h.get_order(), h.get_cells().astype(np.int64))
+        _check_grouped(h.get_order(), h.get_cells().astype(np.int64) >> 1)
+
+
+def test_morton_keys_coarsened_above_256_cells_per_axis():
+    """300 x 20 x 12 cells: 9-bit coordinates would make 27-bit Morton keys; the keys are the
+    Morton codes of (i >> 1, j >> 1, k >> 1)."""
+    dims = (300, 20, 12)
+    m = 80000
+    rng = np.random.default_rng(5)
+    xyz = rng.uniform(0.0, L, (3, m))
+    uvw = rng.normal(0.0, 0.5, (3, m)).astype(np.float32).astype(np.float64)
+    d = np.full(m, 2e-5)
+    mesh = st.mesh_desc(dims, 0.0, L)
+
+    def keys(cells):
+        i = cells % dims[0]
+        j = (cells // dims[0]) % dims[1]
+        k = cells // (dims[0] * dims[1])
+        return workload._morton3(i >> 1, j >> 1, k >> 1)
+
+    with st.ParcelTracker(_params(sort_interval=3), mesh) as h:
+        h.set_parcels(xyz, uvw, d)
+        _check_grouped(h.get_order(), keys(h.get_cells().astype(np.int64)))
+        h.set_fluid_velocity(np.zeros((int(np.prod(dims)), 3), np.float32))
+        for s in range(3):
+            h.step(workload.DT, 1.0)
+        h.synchronize()
+        _check_grouped(h.get_order(), keys(h.get_cells().astype(np.int64)))
 
 
 def test_tet_resort_groups_parcels_by_owning_tet():
