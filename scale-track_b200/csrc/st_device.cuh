@@ -65,6 +65,15 @@ __device__ __forceinline__ float pow0687f_tab(float x)
     return (p * qs.x) * qs.y;
 }
 
+/* slip with the product of the raw cell value and the low part of the fluid factor given
+ * (Ulo = Ur * fs_lo, formed once per cell by a multi-substep loop): the same value as slip */
+template <bool MIX, class V>
+__device__ __forceinline__ V slip_lo(V Ur, V fs_hi, V Ulo, V vel)
+{
+    if constexpr (MIX) return __fmaf_rn(Ur, fs_hi, -vel) + Ulo;
+    else return Ur * fs_hi - vel;
+}
+
 /* floor(label, v) (A:668-670); values outside int32 mark the parcel as lost.  floor(v) lies
  * in [-2^31, 2^31) exactly when v does (both bounds are integers), so the range test is made
  * on v and one round-down conversion gives the label. */

@@ -79,8 +79,10 @@ __global__ void __launch_bounds__(256, MinBlocks<V, ONE>::value) k_step(const St
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     constexpr bool DET = (DEP == DEP_DET1 || DEP == DEP_DET2);
 
-    pow_tab_fill();
-    __syncthreads();
+    if (!ONE) {   /* the table of x^0.687 serves the multi-substep loop */
+        pow_tab_fill();
+        __syncthreads();
+    }
     int cur = -1;
     Quant qp = {0.0, 0.0, 0};
     AmaxT<V> amax = (V)0;

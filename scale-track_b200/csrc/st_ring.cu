@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(HexShapeOf<V>::type::THREADS, 1)
     HexRing<P, V, DEP, ONE> step{a, DET ? a.one.acc : nullptr,
                                  DEP == DEP_ATOMIC ? a.one.src : nullptr, qp, lane, amax, ovf,
                                  nlost};
-    pow_tab_fill();   /* ring_block synchronises the block before any step */
+    if (!ONE) pow_tab_fill();   /* ring_block synchronises the block before any step */
     if (!ring_block<HexShape, P, V, false>(a.one, a.ctl, step, a.wait_cycles)) return;
     flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost);
 }

@@ -9,9 +9,9 @@
  * meshes).  A key range wider than 2^24 values is coarsened to 2^24 by dropping low bits
  * (of each of i, j, k for Morton keys, of the index otherwise): neighbouring cells then share
  * a key, which keeps the locality the sort is for.  Keys are ranked by a counting sort: per-key
- * counts with warp-aggregated atomics, an exclusive scan of the counts (two kernels of this
- * file), then each warp claims its slots of each key with one atomic.  Parcels of one key keep
- * their order inside a warp; across warps it follows the order of the atomics, which no
+ * counts with one atomic per run of equal keys in a warp, an exclusive scan of the counts (two
+ * kernels of this file), then each run claims its slots with one atomic.  Parcels of one run
+ * keep their order; across runs and warps the order follows the order of the atomics, which no
  * result depends on (the deposit is an exact integer sum and everything else is per parcel).
  * Then every SoA array and the parcel id are gathered out of place into the other buffer.
  * The reference has no re-sort: its parcels keep their Hilbert ordered initial positions
@@ -245,7 +245,21 @@ __global__ void k_sample(const uint32_t* __restrict__ inv, const int32_t* __rest
 constexpr unsigned FULL_WARP = 0xffffffffu;
 constexpr uint32_t NO_KEY = 0xffffffffu;   /* lanes past the end (keys are below 2^24) */
 
-/* bins[key] += number of parcels with that key; one atomic per distinct key and warp */
+/* Runs of equal keys among a warp's 32 consecutive parcels (the input is close to sorted
+ * between re-sorts): `heads` has a bit for the first lane of every run, `start` is the first
+ * lane of this lane's run and `len` its length (used by the run's first lane).  Equal keys in
+ * separate runs count and claim separately, which gives the same counts and distinct slots. */
+__device__ __forceinline__ void key_run(uint32_t key, int lane, int& start, int& len, bool& head)
+{
+    const uint32_t prev = __shfl_up_sync(FULL_WARP, key, 1);
+    head = lane == 0 || prev != key;
+    const unsigned heads = __ballot_sync(FULL_WARP, head);
+    start = 31 - __clz(heads & (FULL_WARP >> (31 - lane)));
+    const unsigned later = lane == 31 ? 0u : heads & (FULL_WARP << (lane + 1));
+    len = (later ? __ffs(later) - 1 : 32) - lane;
+}
+
+/* bins[key] += number of parcels with that key; one atomic per run of equal keys */
 __global__ void k_bin_count(const uint32_t* __restrict__ keys, int64_t n, uint32_t nbins,
                             uint32_t* __restrict__ bins)
 {
@@ -256,30 +270,32 @@ __global__ void k_bin_count(const uint32_t* __restrict__ keys, int64_t n, uint32
         const int64_t p = w * 32 + lane;
         /* keys are below nbins by construction; the clamp only guards the bins */
         const uint32_t key = p < n ? min(__ldcs(keys + p), nbins - 1u) : NO_KEY;
-        const unsigned same = __match_any_sync(FULL_WARP, key);
-        if (key != NO_KEY && lane == __ffs(same) - 1) atomicAdd(bins + key, (uint32_t)__popc(same));
+        int start, len;
+        bool head;
+        key_run(key, lane, start, len, head);
+        if (key != NO_KEY && head) atomicAdd(bins + key, (uint32_t)len);
     }
 }
 
-/* perm[slot] = p, slot = the key's offset + the parcel's rank among the parcels of the
- * same key; each warp reserves its parcels' slots of a key with one atomic (offsets are
- * the exclusive scan of the counts and move forward as slots are taken). */
+/* perm[slot] = p, slot = the key's offset + the parcel's place in its run of equal keys;
+ * each run reserves its slots with one atomic (offsets are the exclusive scan of the counts
+ * and move forward as slots are taken). */
 __global__ void k_bin_rank(const uint32_t* __restrict__ keys, int64_t n, uint32_t nbins,
                            uint32_t* __restrict__ offsets, uint32_t* __restrict__ perm)
 {
     const int lane = threadIdx.x & 31;
-    const unsigned below = (1u << lane) - 1u;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 < n;
          w += nw) {
         const int64_t p = w * 32 + lane;
         const uint32_t key = p < n ? min(__ldcs(keys + p), nbins - 1u) : NO_KEY;
-        const unsigned same = __match_any_sync(FULL_WARP, key);
-        const int leader = __ffs(same) - 1;
+        int start, len;
+        bool head;
+        key_run(key, lane, start, len, head);
         uint32_t base = 0;
-        if (key != NO_KEY && lane == leader) base = atomicAdd(offsets + key, (uint32_t)__popc(same));
-        base = __shfl_sync(FULL_WARP, base, leader);
-        if (key != NO_KEY) perm[base + __popc(same & below)] = (uint32_t)p;
+        if (key != NO_KEY && head) base = atomicAdd(offsets + key, (uint32_t)len);
+        base = __shfl_sync(FULL_WARP, base, start);
+        if (key != NO_KEY) perm[base + (uint32_t)(lane - start)] = (uint32_t)p;
     }
 }
 

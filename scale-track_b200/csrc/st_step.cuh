@@ -88,6 +88,9 @@ __device__ __forceinline__ void evolve_parcel(const StepArgs<P, V>& a, P pos[3],
     V velNew[3] = {vel[0], vel[1], vel[2]};
     V state0[3] = {vel[0], vel[1], vel[2]};                          /* A:1289 */
     V D[3] = {(V)0, (V)0, (V)0};                                     /* mixed: state0 - v */
+    V Ulo[3];                                 /* mixed: Ur * fs_lo, formed once per cell */
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Ulo[k] = MIX ? Ur[k] * a.fscale_lo : (V)0;
     bool bad = false;
     for (int t = 1; t <= ph.nsub; ++t) {                             /* A:1291 */
         V inc[3];
@@ -95,7 +98,7 @@ __device__ __forceinline__ void evolve_parcel(const StepArgs<P, V>& a, P pos[3],
             if constexpr (MIX) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    inc[k] = (f * slip<MIX>(Ur[k], a.fscale, a.fscale_lo, vel[k])) / ((V)1 + f);
+                    inc[k] = (f * slip_lo<MIX>(Ur[k], a.fscale, Ulo[k], vel[k])) / ((V)1 + f);
                     velNew[k] = vel[k] + inc[k];
                 }
             } else {
@@ -106,7 +109,7 @@ __device__ __forceinline__ void evolve_parcel(const StepArgs<P, V>& a, P pos[3],
         } else {
             V du[3];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) du[k] = slip<MIX>(Ur[k], a.fscale, a.fscale_lo, vel[k]);
+            for (int k = 0; k < 3; ++k) du[k] = slip_lo<MIX>(Ur[k], a.fscale, Ulo[k], vel[k]);
             V mag = st_sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2]);
             V Re = (mag * d) * ph.rnu;
             V pw;
@@ -168,6 +171,8 @@ __device__ __forceinline__ void evolve_parcel(const StepArgs<P, V>& a, P pos[3],
             Ur[0] = __ldg(Un);
             Ur[1] = __ldg(Un + 1);
             Ur[2] = __ldg(Un + 2);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) Ulo[k] = MIX ? Ur[k] * a.fscale_lo : (V)0;
             posI = ln.posI;
         }
 #pragma unroll
