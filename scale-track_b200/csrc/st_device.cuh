@@ -433,12 +433,14 @@ __device__ __forceinline__ void deposit_warp(int32_t key, const V dep[3],
  * range errors.  Called when a warp moves on to another cloud and at the end. */
 template <int DEP, class A>
 __device__ __forceinline__ void flush_ctl(CloudCtl* ctl, int lane, A& amax, unsigned& ovf,
-                                          unsigned& lost)
+                                          unsigned& lost, int* block_emax = nullptr)
 {
+    /* block_emax (shared memory): the warp's largest exponent goes there, and the kernel adds
+     * the block's maximum to the control block once */
     if (DEP != DEP_ATOMIC) {
         const int e = amax > (A)0 ? exp_of((double)amax) : EXP_NONE;
         const int wmax = __reduce_max_sync(FULL_MASK, e);
-        if (lane == 0 && wmax != EXP_NONE) atomicMax(&ctl->emax, wmax);
+        if (lane == 0 && wmax != EXP_NONE) atomicMax(block_emax ? block_emax : &ctl->emax, wmax);
     }
     const unsigned nlost = __reduce_add_sync(FULL_MASK, lost);
     const unsigned novf = __reduce_add_sync(FULL_MASK, ovf);

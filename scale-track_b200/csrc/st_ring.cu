@@ -149,8 +149,10 @@ __global__ void __launch_bounds__(HexShapeOf<V>::type::THREADS, 1)
                                  DEP == DEP_ATOMIC ? a.one.src : nullptr, qp, lane, amax, ovf,
                                  nlost};
     if (!ONE) pow_tab_fill();   /* ring_block synchronises the block before any step */
+    ring_emax_init();
     if (!ring_block<HexShape, P, V, false>(a.one, a.ctl, step, a.wait_cycles)) return;
-    flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost);
+    flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost, DEP != DEP_ATOMIC ? &s_ring_emax : nullptr);
+    if (DEP != DEP_ATOMIC) ring_emax_flush<HexShape>(a.ctl);
 }
 
 /* ------------------------------------------------------------------------------------ */

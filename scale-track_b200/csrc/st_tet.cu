@@ -446,14 +446,18 @@ __global__ void __launch_bounds__(TetShape::THREADS, 1) k_step_tet_ring(const Te
     const int lane = threadIdx.x & 31;
     const bool count_hops = a.hop_hist != nullptr;
     if (threadIdx.x < 8) s_tet_hist[threadIdx.x] = 0;   /* ring_block synchronises */
+    ring_emax_init();
     TetRing<V, DEP, ONE> step{a, DET ? a.one.acc : nullptr,
                               DEP == DEP_ATOMIC ? a.one.src : nullptr, qp, lane, count_hops,
                               amax, ovf, nlost};
     if (!ring_block<TetShape, double, V, true>(a.one, a.ctl, step, a.wait_cycles)) return;
-    flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost);
+    flush_ctl<DEP>(a.ctl, lane, amax, ovf, nlost, DEP != DEP_ATOMIC ? &s_ring_emax : nullptr);
     ring_consumers_sync<TetShape>();
     if (count_hops && threadIdx.x < 8 && s_tet_hist[threadIdx.x])
         atomicAdd(a.hop_hist + threadIdx.x, (unsigned long long)s_tet_hist[threadIdx.x]);
+    /* one device-scope atomic per block on the cloud's exponent word (see ring_emax_flush) */
+    if (DEP != DEP_ATOMIC && threadIdx.x == 0 && s_ring_emax != EXP_NONE)
+        atomicMax(&a.ctl->emax, s_ring_emax);
 }
 
 template <class V, int DEP, bool ONE>
