@@ -3,9 +3,9 @@ re-sort during stepping, the device-side order (st_get_order) is a permutation t
 parcels by owning cell in key order (the Morton code of the cell on cuboid meshes up to 1024
 cells per axis, the linear cell index on wider ones, the owning tet on tet meshes).  Key ranges
 wider than 2^24 values are coarsened by dropping low bits (of each Morton coordinate, or of the
-index), so the library's counting sort serves every mesh; both kinds of coarsening are
-covered.  Results do not depend on the order (the parity tests compare runs with and without
-re-sorting)."""
+index or tet number), so the library's counting sort serves every mesh; the three kinds of
+coarsening are covered.  Results do not depend on the order (the parity tests compare runs
+with and without re-sorting)."""
 import numpy as np
 import pytest
 
@@ -128,6 +128,27 @@ def test_tet_resort_groups_parcels_by_owning_tet():
             h.step(workload.DT, 1.0)
         h.synchronize()
         _check_grouped(h.get_order(), h.get_cells().astype(np.int64))
+
+
+@pytest.mark.slow
+def test_tet_mesh_above_2p24_tets_sorts_by_coarsened_tet():
+    """142^3 hexes x 6 = 17,179,728 tets (more than 2^24): owning-tet keys less their lowest
+    bit (25-bit tet numbers, 24-bit keys), at set-up and after a re-sort."""
+    n, m = 142, 200000
+    verts, tets, nbr, hex_ijk = workload.kuhn_tet_mesh(n, L, 0.15, 1)
+    assert tets.shape[0] > 1 << 24
+    xyz, _, d = workload.parcels(m, 4)
+    rng = np.random.default_rng(9)
+    uvw = rng.normal(0.0, 1.0, (3, m)).astype(np.float32).astype(np.float64)
+    desc = st.tet_mesh_desc(verts, tets, nbr, 0.0, L)
+    with st.ParcelTracker(_params(sort_interval=2), desc) as h:
+        h.set_parcels(xyz, uvw, d, hint=workload.tet_hints(xyz, hex_ijk, n, L))
+        _check_grouped(h.get_order(), h.get_cells().astype(np.int64) >> 1)
+        h.set_fluid_velocity(np.zeros((tets.shape[0], 3), np.float32))
+        for s in range(2):                         # the re-sort runs after the second step
+            h.step(workload.DT, 1.0)
+        h.synchronize()
+        _check_grouped(h.get_order(), h.get_cells().astype(np.int64) >> 1)
 
 
 def test_ragged_clouds_share_the_bins():
