@@ -248,6 +248,29 @@ class DevArray:
 
 
 # ----------------------------------------------------------------------------- our arm
+def sharded_step(st, torch, h, pg, dev, total):
+    """The step of one rank's shard of a cloud of `total` parcels over the process group `pg`
+    (torch.distributed): the library runs on torch's current stream, where the collectives
+    run; the ranks agree on one fixed-point scale (max of their largest-deposit exponents)
+    and sum their int64 accumulators exactly, so every rank converts the same integers and
+    the source equals that of one GPU stepping every parcel."""
+    st.lib().st_set_stream(h.handle, torch.cuda.current_stream(dev).cuda_stream)
+    h.shard_set_total(total)
+    acc_p, nacc, exp_p, nexp = h.shard_buffers()
+    acc_v = torch.as_tensor(DevArray(acc_p, nacc, "<i8"), device=dev)
+    exp_v = torch.as_tensor(DevArray(exp_p, nexp, "<i4"), device=dev)
+
+    def step(dt_, fs_):
+        if h.shard_needs_probe(dt_):
+            h.shard_probe(dt_, fs_)
+            pg.all_reduce(exp_v, op=pg.ReduceOp.MAX)
+        h.shard_deposit(dt_, fs_)
+        pg.all_reduce(acc_v)
+        pg.all_reduce(exp_v, op=pg.ReduceOp.MAX)
+        h.shard_finish()
+    return step
+
+
 def run_ours(args):
     import torch
     import scaletrack as st
@@ -292,23 +315,7 @@ def run_ours(args):
     h.set_fluid_velocity(U)
     step = h.step
     if pg is not None:
-        # sharded step: one stream for the library and the collectives; the ranks sum their
-        # fixed-point accumulators exactly (int64) and agree on one scale (max exponent), so
-        # the source is the same as one GPU stepping every parcel
-        st.lib().st_set_stream(h.handle, torch.cuda.current_stream(dev).cuda_stream)
-        h.shard_set_total(ws * npcl)
-        acc_p, nacc, exp_p, nexp = h.shard_buffers()
-        acc_v = torch.as_tensor(DevArray(acc_p, nacc, "<i8"), device=dev)
-        exp_v = torch.as_tensor(DevArray(exp_p, nexp, "<i4"), device=dev)
-
-        def step(dt_, fs_):
-            if h.shard_needs_probe(dt_):
-                h.shard_probe(dt_, fs_)
-                pg.all_reduce(exp_v, op=pg.ReduceOp.MAX)
-            h.shard_deposit(dt_, fs_)
-            pg.all_reduce(acc_v)
-            pg.all_reduce(exp_v, op=pg.ReduceOp.MAX)
-            h.shard_finish()
+        step = sharded_step(st, torch, h, pg, dev, ws * npcl)
     timer = DeviceTimer(torch, h.stream(), dev)
     k = 0
     # the clock sampler starts before the warm-up: nvidia-smi's start-up must not overlap
