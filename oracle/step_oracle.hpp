@@ -9,8 +9,9 @@
  * in this environment (no Julia, no OpenFOAM, no MPI) and it ships no tests, golden vectors
  * or fixtures.  This restatement is therefore pinned by analytic known-answer tests (Stokes
  * relaxation, wall-bounce symmetry, momentum bookkeeping) and by a second, independent
- * line-by-line float32 restatement in Python (tests/golden/gen_golden.py) whose outputs are
- * committed as fixtures.  In the strict sense the parity is "unpinned" against the running
+ * line-by-line restatement in Python (tests/golden/gen_golden.py: numpy float32 scalars and
+ * Python binary64 floats, for the FP32, mixed and FP64 modes) whose outputs are committed as
+ * fixtures.  In the strict sense the parity is "unpinned" against the running
  * reference.
  *
  * Reference file cited as A: run/icoJuliaParcelFoam/cavity3D/asyncParallelTracking.jl

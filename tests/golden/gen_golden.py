@@ -2,8 +2,16 @@
 
 An independent, line-by-line restatement of the reference's parcel step in numpy float32
 scalars (Julia Float32 arithmetic is IEEE binary32 without fma contraction, and so are
-numpy float32 scalar operations).  It deliberately shares no code with the C++ oracle, so
-agreement between the two is a cross-check of both restatements.
+numpy float32 scalar operations), and of the library's mixed-precision and all-FP64 modes
+in Python floats (binary64) and numpy float32 scalars.  It deliberately shares no code with
+the C++ oracle, so agreement between the two is a cross-check of both restatements.
+
+Fixtures: ref_stokes_fp32, sn_fp32, sn_bench_fp32 (FP32 reference mode, fluid factor 1);
+sn_mixed, sn_sub3_mixed, stokes_mixed, sn_bench_mixed, stokes_wide_mixed, sn_sub3_fp64,
+stokes_fp64, stokes_wide_fp64 (binary64 positions, a time-varying fluid factor per step in
+`fscale`, the mode in `precision`).  Each
+holds the last step's source twice: `src_f64`, the FP64 sum of the deposits in parcel order,
+and `src_quant`, the library's deterministic fixed-point source (fixed_point_source).
 
 Reference file (A:): run/icoJuliaParcelFoam/cavity3D/asyncParallelTracking.jl
   locate_ijk / locate ........................ A:663-697
@@ -160,6 +168,43 @@ def pow0687f(x):
     return F(F(p * q) * _ffrom((k + 127) << 23))
 
 
+# --------------------------------------------------------- the deterministic source model
+def fixed_point_source(step_logs, ncells, npcl, nsub, limbs):
+    """The library's deterministic source of the last step (project-defined; the reference
+    adds Float32 atomics), from each step's deposits [(1-based cell, [three components])]:
+    a component v != 0 becomes round(v 2^-L) (ties to even) and the integers are summed per
+    cell, so the order of the deposits does not matter; the source is the sum times 2^L.
+    The scale of a step is L = emax - H, emax the largest frexp exponent of the previous
+    step's deposits (of the same step's for the first one, which the library finds by a
+    read-only pass), H = 54 - nb headroom bits for one 64-bit limb (nb: smallest with
+    2^nb >= parcels x substeps, at least 1 and 2 deposits) or 54 for two limbs."""
+    nbound = max(2, npcl * nsub)
+    nb = 1
+    while nb < 62 and (1 << nb) < nbound:
+        nb += 1
+    H = 62 - 8 - nb if limbs == 1 else 62 - 8
+
+    def emax(log):
+        es = [math.frexp(v)[1] for _, comps in log for v in comps if v != 0.0]
+        return max(es) if es else None
+
+    e1 = emax(step_logs[0])
+    L = e1 - H if e1 is not None else -H
+    for k, log in enumerate(step_logs):
+        Q = [[0, 0, 0] for _ in range(ncells)]
+        for cell, comps in log:
+            for c, v in enumerate(comps):
+                if v == 0.0:
+                    continue
+                assert math.frexp(v)[1] - L <= H + 8, "deposit outside the fixed-point range"
+                Q[cell - 1][c] += round(math.ldexp(v, -L))
+        if k == len(step_logs) - 1:
+            return np.array([[math.ldexp(float(q), L) for q in row] for row in Q])
+        e = emax(log)
+        if e is not None:
+            L = e - H
+
+
 # ----------------------------------------------------------------------------- the step
 class Mesh:
     """construct_mesh (A:237-268) with decomposition (1,1,1)."""
@@ -199,7 +244,8 @@ def locate(m, x, y, z):
     return I, J, K, pos, part
 
 
-def evolve_particle(m, prm, X, Y, Z, U, V, W, dIn, Ucell, fs, dt, nsteps, UTrans32, UTrans64):
+def evolve_particle(m, prm, X, Y, Z, U, V, W, dIn, Ucell, fs, dt, nsteps, UTrans32, UTrans64,
+                    log):
     mu, rho_d, rr, rnu, drag = prm["mu"], prm["rho_d"], prm["rr"], prm["rnu"], prm["drag"]
     d = F(dIn * F(1.0))
     mB = F(F(F(rr * F(math.pi)) * F(F(d * d) * d)) / F(6))
@@ -214,10 +260,13 @@ def evolve_particle(m, prm, X, Y, Z, U, V, W, dIn, Ucell, fs, dt, nsteps, UTrans
     f = F(F(F(F(18) * mu) * dt) / F(rho_d * F(d * d)))
 
     def deposit(cell, s0, vn):
+        deps = []
         for c in range(3):
             dep = F(mB * F(s0[c] - vn[c]))
             UTrans32[cell - 1][c] = F(UTrans32[cell - 1][c] + dep)
             UTrans64[cell - 1][c] = UTrans64[cell - 1][c] + float(dep)
+            deps.append(float(dep))
+        log.append((cell, deps))
 
     for t in range(1, nsteps + 1):
         if drag == 0:
@@ -268,12 +317,14 @@ def run_case(n, origin, ending, mu_c, rho_c, rho_d, drag, nsub, xyz, uvw, d, Uce
     Uc = [[F(v) for v in row] for row in Ucell]
     dtF = F(F(dt) / F(nsub))
     ncells = n[0] * n[1] * n[2]
+    logs = []
     for s in range(nsteps):
         UT32 = [[F(0), F(0), F(0)] for _ in range(ncells)]
         UT64 = [[0.0, 0.0, 0.0] for _ in range(ncells)]
+        logs.append([])
         for i in range(npcl):
             p, v = evolve_particle(m, prm, X[i], Y[i], Z[i], U[i], V[i], W[i], D[i], Uc, F(1),
-                                   dtF, nsub, UT32, UT64)
+                                   dtF, nsub, UT32, UT64, logs[-1])
             X[i], Y[i], Z[i] = p
             U[i], V[i], W[i] = v
     cells = []
@@ -286,7 +337,234 @@ def run_case(n, origin, ending, mu_c, rho_c, rho_d, drag, nsub, xyz, uvw, d, Uce
         cells=np.array(cells, dtype=np.int32),
         src_f32=np.array(UT32, dtype=np.float32),
         src_f64=np.array(UT64, dtype=np.float64),
+        src_quant=fixed_point_source(logs, ncells, npcl, nsub, limbs=1),
     )
+
+
+# ------------------------------------------------- mixed precision and all-FP64 (P = double)
+# Project-defined modes of the library (the reference computes in Float32 only), restated
+# from their definitions: positions, the substep for positions and the cell location in
+# binary64 (Python floats); in mixed precision drag, velocity and deposit in binary32 with the
+# compensated slip u_c - v = fma(U, fs_hi, -v) + U fs_lo (fs = fs_hi + fs_lo, the step's FP64
+# fluid factor split into a float and its remainder) and the increment-tracked deposit
+# D = state0 - v (each substep subtracts its velocity increment, a bounced component keeps
+# its D, a deposit is m/rho_c D); all-FP64 follows the reference's form in binary64.
+
+class Mesh64:
+    """construct_mesh (A:237-268) with the spacing kept in binary64 (P = double)."""
+
+    def __init__(self, n, origin, ending):
+        self.N = [int(v) for v in n]
+        self.origin = [float(o) for o in origin]
+        self.rD = [1.0 / ((float(ending[a]) - float(origin[a])) / float(n[a]))
+                   for a in range(3)]
+        self.NxNy = self.N[0] * self.N[1]
+
+
+def locate64(m, x, y, z):
+    lab = []
+    for a, v in enumerate((x, y, z)):
+        f = math.floor((v - m.origin[a]) * m.rD[a])
+        assert -2.0 ** 31 <= f < 2.0 ** 31
+        lab.append(int(f))
+    I, J, K = lab
+    iP, iL = _divrem(I, m.N[0])
+    jP, jL = _divrem(J, m.N[1])
+    kP, kL = _divrem(K, m.N[2])
+    part = abs(kP) + abs(jP) + abs(iP) + 1
+    pos = abs(kL) * m.NxNy + abs(jL) * m.N[0] + abs(iL) + 1
+    return I, J, K, pos, part
+
+
+def _walls(m, I, J, K):
+    return [I < 0 or I >= m.N[0], J < 0 or J >= m.N[1], K < 0 or K >= m.N[2]]
+
+
+def evolve_particle_mixed(m, prm, pos, vel, dIn, Ucell, fs_hi, fs_lo, dtP, dtV, nsteps,
+                          UTrans64, log):
+    """evolve_particle! (A:1271-1365) with binary64 positions and binary32 drag/velocity."""
+    mu, rho_d, rr, rnu, drag = prm["mu"], prm["rho_d"], prm["rr"], prm["rnu"], prm["drag"]
+    d = F(dIn * F(1.0))
+    mB = F(F(F(rr * F(math.pi)) * F(F(d * d) * d)) / F(6))
+    f = F(F(F(F(F(18) * mu) * dtV) / F(rho_d * F(d * d))) * F(1.0))
+    pos, vel = list(pos), list(vel)
+    _, _, _, posI, part = locate64(m, *pos)
+    assert part == 1
+    Ur = [F(Ucell[posI - 1][c]) for c in range(3)]
+    D = [F(0), F(0), F(0)]
+
+    def slip(c):
+        return F(fmaf(Ur[c], fs_hi, F(-vel[c])) + F(Ur[c] * fs_lo))
+
+    def deposit(cell):
+        deps = [float(F(mB * D[c])) for c in range(3)]
+        for c in range(3):
+            UTrans64[cell - 1][c] = UTrans64[cell - 1][c] + deps[c]
+        log.append((cell, deps))
+
+    for t in range(1, nsteps + 1):
+        inc = [F(0)] * 3
+        if drag == 0:
+            inc = [F(F(f * slip(c)) / F(F(1) + f)) for c in range(3)]
+        else:
+            du = [slip(c) for c in range(3)]
+            mag = F(np.sqrt(F(F(F(du[0] * du[0]) + F(du[1] * du[1])) + F(du[2] * du[2]))))
+            Re = F(F(mag * d) * rnu)
+            g = F(f * F(F(1) + F(F(0.15) * pow0687f(Re))))
+            inc = [F(g * du[c]) for c in range(3)]
+        velNew = [F(vel[c] + inc[c]) for c in range(3)]
+        posNew = [pos[c] + float(velNew[c]) * dtP for c in range(3)]
+        I, J, K, posNewI, partNew = locate64(m, *posNew)
+        b = [False, False, False]
+        if posNewI != posI or partNew != 1:
+            b = _walls(m, I, J, K)
+            for c in range(3):
+                if b[c]:
+                    posNew[c] = pos[c]
+                    velNew[c] = F(-vel[c])
+            if any(b):
+                I, J, K, posNewI, partNew = locate64(m, *posNew)
+        for c in range(3):
+            if not b[c]:
+                D[c] = F(D[c] - inc[c])
+        if t != nsteps and posNewI != posI:
+            deposit(posI)
+            D = [F(0), F(0), F(0)]
+            Ur = [F(Ucell[posNewI - 1][c]) for c in range(3)]
+            posI = posNewI
+        vel, pos = velNew, posNew
+    deposit(posI)
+    return pos, vel
+
+
+def evolve_particle_fp64(m, prm, pos, vel, dIn, Ucell, fs, dtP, dtV, nsteps, UTrans64, log):
+    """evolve_particle! (A:1271-1365) in binary64 throughout, the reference's form."""
+    mu, rho_d, rr, rnu, drag = prm["mu"], prm["rho_d"], prm["rr"], prm["rnu"], prm["drag"]
+    d = dIn * 1.0
+    mB = ((rr * math.pi) * ((d * d) * d)) / 6.0
+    f = ((((18.0 * mu) * dtV) / (rho_d * (d * d)))) * 1.0
+    pos, vel = list(pos), list(vel)
+    _, _, _, posI, part = locate64(m, *pos)
+    assert part == 1
+    Ur = [float(Ucell[posI - 1][c]) for c in range(3)]
+    state0 = list(vel)
+
+    def deposit(cell, vn):
+        deps = [mB * (state0[c] - vn[c]) for c in range(3)]
+        for c in range(3):
+            UTrans64[cell - 1][c] = UTrans64[cell - 1][c] + deps[c]
+        log.append((cell, deps))
+
+    for t in range(1, nsteps + 1):
+        if drag == 0:
+            velNew = [(vel[c] + f * (Ur[c] * fs)) / (1.0 + f) for c in range(3)]
+        else:
+            du = [Ur[c] * fs - vel[c] for c in range(3)]
+            mag = math.sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2])
+            Re = (mag * d) * rnu
+            g = f * (1.0 + 0.15 * pow0687(Re))
+            velNew = [vel[c] + g * du[c] for c in range(3)]
+        posNew = [pos[c] + velNew[c] * dtP for c in range(3)]
+        I, J, K, posNewI, partNew = locate64(m, *posNew)
+        if posNewI != posI or partNew != 1:
+            b = _walls(m, I, J, K)
+            for c in range(3):
+                if b[c]:
+                    posNew[c] = pos[c]
+                    velNew[c] = -vel[c]
+                    state0[c] = state0[c] - 2.0 * vel[c]
+            if any(b):
+                I, J, K, posNewI, partNew = locate64(m, *posNew)
+        if t != nsteps and posNewI != posI:
+            deposit(posI, velNew)
+            state0 = list(velNew)
+            Ur = [float(Ucell[posNewI - 1][c]) for c in range(3)]
+            posI = posNewI
+        vel, pos = velNew, posNew
+    deposit(posI, velNew)
+    return pos, vel
+
+
+def run_case_p64(n, origin, ending, mu_c, rho_c, rho_d, drag, nsub, xyz, uvw, d, Ucell, dt,
+                 nsteps, fscale, precision):
+    """The CPU executor loop (A:818-823) in mixed precision or all-FP64; step s uses the
+    fluid factor fscale[s] on the cell velocities."""
+    m = Mesh64(n, origin, ending)
+    mixed = precision == "mixed"
+    V = F if mixed else float
+    prm = dict(mu=V(mu_c), rho_d=V(rho_d), rr=V(rho_d / rho_c), rnu=V(rho_c / mu_c), drag=drag)
+    npcl = d.shape[0]
+    P = [[float(v) for v in xyz[a]] for a in range(3)]
+    W = [[V(v) for v in uvw[a]] for a in range(3)]
+    D = [V(v) for v in d]
+    Uc = [[V(v) for v in row] for row in Ucell]
+    dtP = float(dt) / float(nsub)
+    dtV = V(dtP)
+    ncells = n[0] * n[1] * n[2]
+    logs = []
+    for s in range(nsteps):
+        UT64 = [[0.0, 0.0, 0.0] for _ in range(ncells)]
+        logs.append([])
+        fs = float(fscale[s])
+        for i in range(npcl):
+            pos = [P[0][i], P[1][i], P[2][i]]
+            vel = [W[0][i], W[1][i], W[2][i]]
+            if mixed:
+                hi = F(fs)
+                lo = F(fs - float(hi))
+                p, v = evolve_particle_mixed(m, prm, pos, vel, D[i], Uc, hi, lo, dtP, dtV, nsub,
+                                             UT64, logs[-1])
+            else:
+                p, v = evolve_particle_fp64(m, prm, pos, vel, D[i], Uc, fs, dtP, dtV, nsub,
+                                            UT64, logs[-1])
+            for a in range(3):
+                P[a][i] = p[a]
+                W[a][i] = v[a]
+    cells = []
+    for i in range(npcl):
+        _, _, _, pos, part = locate64(m, P[0][i], P[1][i], P[2][i])
+        cells.append(pos - 1 if part == 1 else -1)
+    return dict(
+        xyz=np.array(P, dtype=np.float64),
+        uvw=np.array(W, dtype=np.float32 if mixed else np.float64),
+        cells=np.array(cells, dtype=np.int32),
+        src_f64=np.array(UT64, dtype=np.float64),
+        src_quant=fixed_point_source(logs, ncells, npcl, nsub, limbs=1 if mixed else 2),
+    )
+
+
+def make_inputs64(seed, n, npcl, ending, dmin, dmax, precision, v0_random=True, dlog=False):
+    """Inputs of the binary64-position cases: positions uniform in the box as binary64 values
+    (not float32-representable), hand-placed parcels on walls, faces and one ulp inside the
+    upper walls; velocities, diameters and cell velocities in the velocity precision."""
+    rng = np.random.default_rng(seed)
+    vt = np.float32 if precision == "mixed" else np.float64
+    xyz = rng.random((3, npcl)) * float(ending)
+    h = float(ending) / n
+    top = np.nextafter(float(ending), 0.0)
+    special = [(0.0, 0.5 * ending, 0.5 * ending), (top, 0.5 * ending, 0.5 * ending),
+               (0.5 * ending, top, 0.5 * ending), (0.5 * ending, 0.5 * ending, top),
+               (h, h, h), (2 * h, 0.5 * ending, 3 * h), (0.0, 0.0, 0.0)]
+    for k, s3 in enumerate(special):
+        xyz[:, k] = s3
+    uvw = (rng.random((3, npcl)) * 2.0 - 1.0) if v0_random else np.zeros((3, npcl))
+    uvw[:, :7] = np.array([[-0.9, 0.1, 0.2], [0.8, -0.3, 0.1], [0.1, -0.95, 0.0],
+                           [0.0, 0.2, 0.9], [-0.5, -0.5, -0.5], [0.3, 0.0, -0.4],
+                           [-1.0, -1.0, -1.0]]).T
+    uvw = uvw.astype(vt)
+    if dlog:   # log-uniform: deposits over many decades, rounded at the fixed-point scale
+        d = np.exp(rng.random(npcl) * (math.log(dmax) - math.log(dmin)) + math.log(dmin))
+        d = d.astype(vt)
+    else:
+        d = (rng.random(npcl) * (dmax - dmin) + dmin).astype(vt)
+    Ucell = (rng.random((n ** 3, 3)) * 2.0 - 1.0).astype(vt)
+    return xyz, uvw, d, Ucell
+
+
+def fluid_factors(nsteps):
+    """A time-varying fluid factor per step whose values are not binary32-representable (so
+    the low part of the split is not zero)."""
+    return np.array([1.0 + 0.2 * math.sin(0.37 * (s + 1) + 0.3) for s in range(nsteps)])
 
 
 def make_inputs(seed, n, npcl, ending, dmin, dmax, v0_random=False, wall_cases=True):
@@ -330,13 +608,65 @@ CASES = {
                           nsteps=3),
 }
 
+# binary64-position cases: (name, precision, case); every one has a time-varying fluid factor
+CASES64 = {
+    # Schiller-Naumann, one substep, reference-physics box with dense parcels
+    "sn_mixed": dict(precision="mixed", seed=21, n=8, npcl=96, ending=1.0, dmin=5e-3, dmax=1e-2,
+                     mu_c=1e-3, rho_c=1e3, rho_d=1000.0, drag=1, nsub=1, dt=0.05, nsteps=4),
+    # Schiller-Naumann, three substeps: intermediate deposits at cell crossings
+    "sn_sub3_mixed": dict(precision="mixed", seed=22, n=8, npcl=96, ending=1.0, dmin=5e-3,
+                          dmax=1e-2, mu_c=1e-3, rho_c=1e3, rho_d=1000.0, drag=1, nsub=3,
+                          dt=0.15, nsteps=3),
+    # Stokes implicit, ten substeps, the reference's physics and a large step (walls, faces)
+    "stokes_mixed": dict(precision="mixed", seed=23, n=8, npcl=96, ending=1.0, dmin=5e-3,
+                         dmax=1e-2, mu_c=1e-3, rho_c=1e3, rho_d=1.0, drag=0, nsub=10, dt=0.6,
+                         nsteps=3),
+    # the benchmark's physical constants on a small box
+    "sn_bench_mixed": dict(precision="mixed", seed=24, n=6, npcl=64, ending=0.01, dmin=1e-5,
+                           dmax=4e-5, mu_c=1.8e-5, rho_c=1.2, rho_d=1000.0, drag=1, nsub=1,
+                           dt=4e-4, nsteps=3),
+    "sn_sub3_fp64": dict(precision="fp64", seed=25, n=8, npcl=96, ending=1.0, dmin=5e-3,
+                         dmax=1e-2, mu_c=1e-3, rho_c=1e3, rho_d=1000.0, drag=1, nsub=3,
+                         dt=0.15, nsteps=3),
+    "stokes_fp64": dict(precision="fp64", seed=26, n=8, npcl=96, ending=1.0, dmin=5e-3,
+                        dmax=1e-2, mu_c=1e-3, rho_c=1e3, rho_d=1.0, drag=0, nsub=10, dt=0.6,
+                        nsteps=3),
+    # diameters log-uniform over four decades: deposit magnitudes span about 2^40, so the
+    # small parcels' deposits are rounded at the fixed-point scale (one limb and two)
+    "stokes_wide_mixed": dict(precision="mixed", seed=27, n=8, npcl=96, ending=1.0, dmin=1e-6,
+                              dmax=1e-2, mu_c=1e-3, rho_c=1e3, rho_d=1000.0, drag=0, nsub=2,
+                              dt=0.1, nsteps=3, dlog=True),
+    "stokes_wide_fp64": dict(precision="fp64", seed=28, n=8, npcl=96, ending=1.0, dmin=1e-6,
+                             dmax=1e-2, mu_c=1e-3, rho_c=1e3, rho_d=1000.0, drag=0, nsub=2,
+                             dt=0.1, nsteps=3, dlog=True),
+}
+
 
 def _cells0(c, xyz):
     m = Mesh([c["n"]] * 3, [0.0] * 3, [c["ending"]] * 3)
     return np.array([locate(m, *xyz[:, i])[3] - 1 for i in range(xyz.shape[1])])
 
 
+def _cells0_64(c, xyz):
+    m = Mesh64([c["n"]] * 3, [0.0] * 3, [c["ending"]] * 3)
+    return np.array([locate64(m, *xyz[:, i])[3] - 1 for i in range(xyz.shape[1])])
+
+
 def main():
+    for name, c in CASES64.items():
+        xyz, uvw, d, Ucell = make_inputs64(c["seed"], c["n"], c["npcl"], c["ending"], c["dmin"],
+                                           c["dmax"], c["precision"], dlog=c.get("dlog", False))
+        fsc = fluid_factors(c["nsteps"])
+        out = run_case_p64([c["n"]] * 3, [0.0] * 3, [c["ending"]] * 3, c["mu_c"], c["rho_c"],
+                           c["rho_d"], c["drag"], c["nsub"], xyz, uvw, d, Ucell, c["dt"],
+                           c["nsteps"], fsc, c["precision"])
+        meta = np.array([c["n"], c["nsub"], c["drag"], c["nsteps"]], dtype=np.int64)
+        phys = np.array([c["ending"], c["mu_c"], c["rho_c"], c["rho_d"], c["dt"]])
+        np.savez(os.path.join(HERE, name + ".npz"), meta=meta, phys=phys, xyz0=xyz, uvw0=uvw,
+                 d=d, U=Ucell, fscale=fsc, precision=np.array(c["precision"]), **out)
+        moved_cells = int(np.sum(out["cells"] != _cells0_64(c, xyz)))
+        print(f"{name}: {c['npcl']} parcels, changed cell {moved_cells}, "
+              f"|src| max {np.abs(out['src_f64']).max():.3e}")
     for name, c in CASES.items():
         xyz, uvw, d, Ucell = make_inputs(c["seed"], c["n"], c["npcl"], c["ending"], c["dmin"],
                                          c["dmax"], c.get("v0_random", False))

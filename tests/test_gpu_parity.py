@@ -66,18 +66,24 @@ def check_against_oracle(prm, n, L, xyz, uvw, d, U, dt, fscales, nthreads=0):
 
 # ------------------------------------------------------------------------------------------
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
-def test_fp32_reference_mode_matches_golden(path):
+def test_step_matches_golden(path):
+    """The golden fixtures of the independent Python restatement, in the fixture's precision
+    mode (FP32 reference mode, mixed, FP64) and with its per-step fluid factors."""
     z = np.load(path)
     n, nsub, drag, nsteps = [int(v) for v in z["meta"]]
     ending, mu, rc, rd, dt = [float(v) for v in z["phys"]]
-    prm = st.params(mu_c=mu, rho_c=rc, rho_d=rd, drag_model=drag, precision="fp32",
+    prec = str(z["precision"]) if "precision" in z.files else "fp32"
+    fscales = [float(v) for v in z["fscale"]] if "fscale" in z.files else [1.0] * nsteps
+    prm = st.params(mu_c=mu, rho_c=rc, rho_d=rd, drag_model=drag, precision=prec,
                     n_substeps=nsub)
-    g = gpu_run(prm, n, ending, [(z["xyz0"], z["uvw0"], z["d"])], z["U"], dt, [1.0] * nsteps)[0]
-    assert np.array_equal(g[0].astype(np.float32), z["xyz"])
-    assert np.array_equal(g[1].astype(np.float32), z["uvw"])
+    g = gpu_run(prm, n, ending, [(z["xyz0"], z["uvw0"], z["d"])], z["U"], dt, fscales)[0]
+    assert np.array_equal(g[0].astype(z["xyz"].dtype), z["xyz"])
+    assert np.array_equal(g[1].astype(z["uvw"].dtype), z["uvw"])
     assert np.array_equal(g[2], z["cells"])
-    assert relerr(g[3], z["src_f64"]) <= TOL_SRC_1LIMB
-    r = oracle.run(oracle_cfg(n, ending, prm), z["xyz0"], z["uvw0"], z["d"], z["U"], nsteps, dt)
+    assert relerr(g[3], z["src_f64"]) <= (TOL_SRC_2LIMB if prec == "fp64" else TOL_SRC_1LIMB)
+    assert np.array_equal(g[3], z["src_quant"])
+    r = oracle.run(oracle_cfg(n, ending, prm), z["xyz0"], z["uvw0"], z["d"], z["U"], nsteps, dt,
+                   fscale=fscales)
     assert np.array_equal(g[3], r["src_quant"])
 
 

@@ -1,5 +1,6 @@
 """CPU tests of the oracle: pinned against the golden fixtures of the independent Python
-restatement (tests/golden/gen_golden.py) and against analytic known answers."""
+restatement (tests/golden/gen_golden.py) in all three precision modes (FP32 reference mode,
+mixed, FP64) and against analytic known answers."""
 import glob
 import os
 
@@ -17,33 +18,47 @@ def load_golden(path):
     z = np.load(path)
     n, nsub, drag, nsteps = [int(v) for v in z["meta"]]
     ending, mu, rc, rd, dt = [float(v) for v in z["phys"]]
+    prec = str(z["precision"]) if "precision" in z.files else "fp32"
+    fscale = z["fscale"] if "fscale" in z.files else None
     return z, dict(n=n, nsub=nsub, drag=drag, nsteps=nsteps, ending=ending, mu=mu, rc=rc,
-                   rd=rd, dt=dt)
+                   rd=rd, dt=dt, precision=prec, fscale=fscale)
+
+
+def test_golden_fixtures_cover_every_precision_mode():
+    precs = {load_golden(p)[1]["precision"] for p in GOLDEN}
+    assert precs == {"fp32", "mixed", "fp64"}
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
 def test_oracle_matches_golden_fixture(oracle_lib, path):
     z, c = load_golden(path)
+    prec = c["precision"]
     cfg = oracle.make_cfg(c["n"], 0.0, c["ending"], c["mu"], c["rc"], c["rd"], drag=c["drag"],
-                          precision="fp32", n_substeps=c["nsub"])
-    r = oracle.run(cfg, z["xyz0"], z["uvw0"], z["d"], z["U"], c["nsteps"], c["dt"])
+                          precision=prec, n_substeps=c["nsub"],
+                          quant_limbs=2 if prec == "fp64" else 1)
+    r = oracle.run(cfg, z["xyz0"], z["uvw0"], z["d"], z["U"], c["nsteps"], c["dt"],
+                   fscale=c["fscale"])
     assert r["status"] == 0
-    assert np.array_equal(r["xyz"].astype(np.float32), z["xyz"])
-    assert np.array_equal(r["uvw"].astype(np.float32), z["uvw"])
+    # positions in the position type, velocities in the velocity type: bit for bit
+    assert np.array_equal(r["xyz"].astype(z["xyz"].dtype), z["xyz"])
+    assert np.array_equal(r["uvw"].astype(z["uvw"].dtype), z["uvw"])
     assert np.array_equal(r["cells"], z["cells"])
-    # FP64 sum of the float deposits in parcel order: same order, same bits
+    # FP64 sum of the deposits in parcel order: same order, same bits
     assert np.array_equal(r["src_seq"], z["src_f64"])
-    # the reference's own Float32 accumulation (A:706) agrees to float rounding
-    ref32 = z["src_f32"].astype(np.float64)
-    scale = np.abs(z["src_f64"]).max()
-    assert np.abs(ref32 - r["src_seq"]).max() <= 1e-5 * scale
+    # the deterministic fixed-point source (scale from the previous step's largest deposit)
+    assert np.array_equal(r["src_quant"], z["src_quant"])
+    if "src_f32" in z.files:
+        # the reference's own Float32 accumulation (A:706) agrees to float rounding
+        ref32 = z["src_f32"].astype(np.float64)
+        scale = np.abs(z["src_f64"]).max()
+        assert np.abs(ref32 - r["src_seq"]).max() <= 1e-5 * scale
 
 
 def test_golden_fixtures_exercise_walls_and_crossings():
     for path in GOLDEN:
         z, c = load_golden(path)
         cfg = oracle.make_cfg(c["n"], 0.0, c["ending"], c["mu"], c["rc"], c["rd"],
-                              precision="fp32")
+                              precision=c["precision"])
         c0 = oracle.locate(cfg, z["xyz0"].astype(np.float64))
         assert np.sum(c0 != z["cells"]) >= 10, path
         assert np.abs(z["src_f64"]).max() > 0
