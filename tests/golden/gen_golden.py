@@ -24,6 +24,9 @@ The Schiller-Naumann drag is project-defined (the reference only has Stokes drag
 power functions follow the same algorithms as scale-track_b200/csrc/st_pow.h, restated here
 in Python floats (double) and numpy float32 scalars with an exact-rational fma (single).
 
+Tet fixtures (tests/golden/tet/*.npz): the library's face walk on a jittered tet mesh with
+the mixed and FP64 step, restated the same way (TetMesh, evolve_parcel_tet).
+
 Run:  python tests/golden/gen_golden.py      (rewrites the .npz files next to this script)
 """
 import math
@@ -652,7 +655,202 @@ def _cells0_64(c, xyz):
     return np.array([locate64(m, *xyz[:, i])[3] - 1 for i in range(xyz.shape[1])])
 
 
+# ------------------------------------------------ tetrahedral meshes (project-defined walk)
+# The library's face walk on a conforming tet mesh, restated from its definition: each tet's
+# vertex ids sorted increasingly (neighbours permuted with them); face f has the other three
+# vertices (p, q, r) in increasing order, n = (q - p) x (r - p), negated when n.(v_f - p) > 0,
+# c = n.p and s_f(x) = n.x - c in binary64; a walk moves across the face with the largest
+# positive s_f (ties to the lowest f) until no s_f is positive.  The parcel update and the
+# deposit rules are those of the cuboid mesh, with the wall rule applied per coordinate
+# against the box and the owning tet as the cell.
+
+TET_FACES = ((1, 2, 3), (0, 2, 3), (0, 1, 3), (0, 1, 2))
+
+
+class TetMesh:
+    def __init__(self, verts, tets, nbr, L):
+        self.v = [tuple(float(a) for a in row) for row in verts]
+        self.t, self.nb = [], []
+        for k in range(tets.shape[0]):
+            order = sorted(range(4), key=lambda j: int(tets[k, j]))
+            self.t.append([int(tets[k, j]) for j in order])
+            self.nb.append([int(nbr[k, j]) for j in order])
+        self.L = float(L)
+
+    def plane(self, t, f):
+        v = [self.v[i] for i in self.t[t]]
+        p, q, r = (v[j] for j in TET_FACES[f])
+        a = [q[k] - p[k] for k in range(3)]
+        b = [r[k] - p[k] for k in range(3)]
+        n = [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+        e = (n[0] * (v[f][0] - p[0]) + n[1] * (v[f][1] - p[1])) + n[2] * (v[f][2] - p[2])
+        if e > 0.0:
+            n = [-n[0], -n[1], -n[2]]
+        return n, (n[0] * p[0] + n[1] * p[1]) + n[2] * p[2]
+
+    def walk(self, t, x, hop_limit=64):
+        """(tet, hops) or (None, hops) when the walk leaves the mesh or exceeds the limit."""
+        hops = 0
+        while True:
+            s = []
+            for f in range(4):
+                n, c = self.plane(t, f)
+                s.append(((n[0] * x[0] + n[1] * x[1]) + n[2] * x[2]) - c)
+            fb = 0
+            for f in range(1, 4):
+                if s[f] > s[fb]:
+                    fb = f
+            if not (s[fb] > 0.0):
+                return t, hops
+            nb = self.nb[t][fb]
+            if nb < 0 or hops >= hop_limit:
+                return None, hops
+            t = nb
+            hops += 1
+
+
+def evolve_parcel_tet(m, prm, pos, vel, cell, dIn, Utet, fs_hi, fs_lo, dtP, dtV, nsteps,
+                      mixed, log, hist):
+    """One call of the step for one parcel on the tet mesh (positions binary64; velocities
+    binary32 in mixed precision, binary64 otherwise)."""
+    mu, rho_d, rr, rnu, drag = prm["mu"], prm["rho_d"], prm["rr"], prm["rnu"], prm["drag"]
+    if mixed:
+        d = F(dIn * F(1.0))
+        mB = F(F(F(rr * F(math.pi)) * F(F(d * d) * d)) / F(6))
+        f = F(F(F(F(F(18) * mu) * dtV) / F(rho_d * F(d * d))) * F(1.0))
+    else:
+        d = dIn * 1.0
+        mB = ((rr * math.pi) * ((d * d) * d)) / 6.0
+        f = ((((18.0 * mu) * dtV) / (rho_d * (d * d)))) * 1.0
+    pos, vel = list(pos), list(vel)
+    cur = tnew = cell
+    Ur = [Utet[cur][c] for c in range(3)]
+    state0 = list(vel)
+    D = [F(0)] * 3
+
+    def deposit(t, vn):
+        if mixed:
+            deps = [float(F(mB * D[c])) for c in range(3)]
+        else:
+            deps = [mB * (state0[c] - vn[c]) for c in range(3)]
+        log.append((t + 1, deps))
+
+    for t in range(1, nsteps + 1):
+        if mixed:
+            sl = [F(fmaf(Ur[c], fs_hi, F(-vel[c])) + F(Ur[c] * fs_lo)) for c in range(3)]
+            if drag == 0:
+                inc = [F(F(f * sl[c]) / F(F(1) + f)) for c in range(3)]
+            else:
+                mag = F(np.sqrt(F(F(F(sl[0] * sl[0]) + F(sl[1] * sl[1])) + F(sl[2] * sl[2]))))
+                g = F(f * F(F(1) + F(F(0.15) * pow0687f(F(F(mag * d) * rnu)))))
+                inc = [F(g * sl[c]) for c in range(3)]
+            velNew = [F(vel[c] + inc[c]) for c in range(3)]
+        else:
+            if drag == 0:
+                velNew = [(vel[c] + f * (Ur[c] * fs_hi)) / (1.0 + f) for c in range(3)]
+            else:
+                du = [Ur[c] * fs_hi - vel[c] for c in range(3)]
+                mag = math.sqrt((du[0] * du[0] + du[1] * du[1]) + du[2] * du[2])
+                g = f * (1.0 + 0.15 * pow0687((mag * d) * rnu))
+                velNew = [vel[c] + g * du[c] for c in range(3)]
+        posNew = [pos[c] + float(velNew[c]) * dtP for c in range(3)]
+        for c in range(3):
+            if posNew[c] < 0.0 or posNew[c] > m.L:
+                posNew[c] = pos[c]
+                velNew[c] = -vel[c]
+                if not mixed:
+                    state0[c] = state0[c] - 2.0 * vel[c]
+            elif mixed:
+                D[c] = F(D[c] - inc[c])
+        tnew, hops = m.walk(tnew, posNew)
+        assert tnew is not None, "a fixture parcel left the mesh"
+        hist[min(hops, 7)] += 1
+        if t != nsteps and tnew != cur:
+            deposit(cur, velNew)
+            state0 = list(velNew)
+            D = [F(0)] * 3
+            Ur = [Utet[tnew][c] for c in range(3)]
+            cur = tnew
+        vel, pos = velNew, posNew
+    deposit(cur, velNew)
+    return pos, vel, tnew
+
+
+TET_CASES = {
+    "tet_sn_sub3_mixed": dict(precision="mixed", seed=41, n=3, npcl=64, drag=1, nsub=3, dt=1e-3,
+                              speed=10.0, dmed=40e-6, nsteps=3),
+    "tet_stokes_sub2_fp64": dict(precision="fp64", seed=42, n=3, npcl=64, drag=0, nsub=2,
+                                 dt=1e-3, speed=20.0, dmed=20e-6, nsteps=3),
+}
+
+
+def run_tet_case(c):
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "scale-track_b200"))
+    import workload
+    mixed = c["precision"] == "mixed"
+    vt = np.float32 if mixed else np.float64
+    V = F if mixed else float
+    L = workload.L_BOX
+    verts, tets, nbr, hex_ijk = workload.kuhn_tet_mesh(c["n"], L, 0.15, 1)
+    rng = np.random.default_rng(c["seed"])
+    npcl = c["npcl"]
+    xyz = rng.random((3, npcl)) * L
+    uvw = rng.normal(0.0, c["speed"], (3, npcl)).astype(vt)
+    d = (c["dmed"] * np.exp(0.3 * rng.normal(size=npcl))).astype(vt)
+    Utet = (3.0 * (rng.random((tets.shape[0], 3)) * 2.0 - 1.0)).astype(vt)
+    hint = workload.tet_hints(xyz, hex_ijk, c["n"], L)
+    m = TetMesh(verts, tets, nbr, L)
+    cells0 = []
+    for i in range(npcl):
+        t, _ = m.walk(int(hint[i]), [float(xyz[a, i]) for a in range(3)], hop_limit=1024)
+        assert t is not None
+        cells0.append(t)
+    prm = dict(mu=V(workload.MU_F), rho_d=V(workload.RHO_P), rr=V(workload.RHO_P / workload.RHO_F),
+               rnu=V(workload.RHO_F / workload.MU_F), drag=c["drag"])
+    Uc = [[V(v) for v in row] for row in Utet]
+    fsc = fluid_factors(c["nsteps"])
+    dtP = float(c["dt"]) / float(c["nsub"])
+    dtV = V(dtP)
+    P = [[float(xyz[a, i]) for a in range(3)] for i in range(npcl)]
+    W = [[V(uvw[a, i]) for a in range(3)] for i in range(npcl)]
+    cells = list(cells0)
+    logs, hist = [], [0] * 8
+    for s in range(c["nsteps"]):
+        fs = float(fsc[s])
+        hi = F(fs) if mixed else fs
+        lo = F(fs - float(hi)) if mixed else 0.0
+        logs.append([])
+        for i in range(npcl):
+            P[i], W[i], cells[i] = evolve_parcel_tet(m, prm, P[i], W[i], cells[i], V(d[i]), Uc,
+                                                     hi, lo, dtP, dtV, c["nsub"], mixed,
+                                                     logs[-1], hist)
+    nt = tets.shape[0]
+    src64 = [[0.0, 0.0, 0.0] for _ in range(nt)]
+    for t, comps in logs[-1]:
+        for k in range(3):
+            src64[t - 1][k] += comps[k]
+    return dict(verts=verts, tets=tets, nbr=nbr, xyz0=xyz, uvw0=uvw, d=d, U=Utet, hint=hint,
+                cells0=np.array(cells0, dtype=np.int32), fscale=fsc,
+                precision=np.array(c["precision"]),
+                meta=np.array([c["n"], c["nsub"], c["drag"], c["nsteps"]], dtype=np.int64),
+                phys=np.array([L, workload.MU_F, workload.RHO_F, workload.RHO_P, c["dt"]]),
+                xyz=np.array(P, dtype=np.float64).T.copy(),
+                uvw=np.array(W, dtype=vt).T.copy(),
+                cells=np.array(cells, dtype=np.int32),
+                hop_hist=np.array(hist, dtype=np.int64),
+                src_f64=np.array(src64),
+                src_quant=fixed_point_source(logs, nt, npcl, c["nsub"], 1 if mixed else 2))
+
+
 def main():
+    os.makedirs(os.path.join(HERE, "tet"), exist_ok=True)
+    for name, c in TET_CASES.items():
+        out = run_tet_case(c)
+        np.savez(os.path.join(HERE, "tet", name + ".npz"), **out)
+        moved = int(np.sum(out["cells"] != out["cells0"]))
+        print(f"{name}: {c['npcl']} parcels, changed tet {moved}, hops {out['hop_hist'].tolist()}, "
+              f"|src| max {np.abs(out['src_f64']).max():.3e}")
     for name, c in CASES64.items():
         xyz, uvw, d, Ucell = make_inputs64(c["seed"], c["n"], c["npcl"], c["ending"], c["dmin"],
                                            c["dmax"], c["precision"], dlog=c.get("dlog", False))

@@ -6,6 +6,8 @@ and under a uniform carrier velocity (where the mesh cannot matter) the tet step
 same parcel states and the same total source as the cuboid-mesh oracle, which is itself pinned
 to the reference's golden vectors."""
 import ctypes
+import glob
+import os
 
 import numpy as np
 import pytest
@@ -156,3 +158,42 @@ def test_create_tet_validates_indices_on_the_host():
                                 ctypes.byref(st.tet_mesh_desc(verts, tets, badn, 0.0, L)), 0,
                                 ctypes.byref(h))
     assert rc == st.ST_ERR_INVALID_ARGUMENT and "neighbour" in st.last_error()
+
+
+TET_GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                           "tet", "*.npz")))
+
+
+def load_tet_golden(path):
+    z = np.load(path)
+    n, nsub, drag, nsteps = [int(v) for v in z["meta"]]
+    Lb, mu, rc, rd, dt = [float(v) for v in z["phys"]]
+    return z, dict(n=n, nsub=nsub, drag=drag, nsteps=nsteps, L=Lb, mu=mu, rc=rc, rd=rd, dt=dt,
+                   precision=str(z["precision"]))
+
+
+def test_tet_golden_fixtures_exist_in_both_precisions():
+    assert {load_tet_golden(p)[1]["precision"] for p in TET_GOLDEN} == {"mixed", "fp64"}
+
+
+@pytest.mark.parametrize("path", TET_GOLDEN, ids=[os.path.basename(p) for p in TET_GOLDEN])
+def test_tet_oracle_matches_golden_fixture(oracle_lib, path):
+    """The independent Python restatement of the face walk and the tet step
+    (tests/golden/gen_golden.py): start tets, positions, velocities, owning tets, walk-length
+    histogram, FP64 sum of the deposits and fixed-point source, bit for bit."""
+    z, c = load_tet_golden(path)
+    mesh = (z["verts"], z["tets"], z["nbr"])
+    cells0, status = oracle.tet_locate(mesh, z["xyz0"], z["hint"])
+    assert (status == 0).all() and np.array_equal(cells0, z["cells0"])
+    cfg = oracle.make_cfg(1, 0.0, c["L"], c["mu"], c["rc"], c["rd"], drag=c["drag"],
+                          precision=c["precision"], n_substeps=c["nsub"],
+                          quant_limbs=2 if c["precision"] == "fp64" else 1)
+    r = oracle.tet_run(cfg, mesh, z["xyz0"], z["uvw0"], z["d"], z["cells0"], z["U"],
+                       c["nsteps"], c["dt"], fscale=z["fscale"])
+    assert r["status"] == 0 and r["lost"] == 0 and r["overflow"] == 0
+    assert np.array_equal(r["xyz"], z["xyz"])
+    assert np.array_equal(r["uvw"].astype(z["uvw"].dtype), z["uvw"])
+    assert np.array_equal(r["cells"], z["cells"])
+    assert np.array_equal(r["hop_hist"], z["hop_hist"])
+    assert np.array_equal(r["src_seq"], z["src_f64"])
+    assert np.array_equal(r["src_quant"], z["src_quant"])
