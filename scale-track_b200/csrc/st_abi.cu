@@ -2626,6 +2626,9 @@ int st_evolve_cloud(double dt)
             h->launches += 1;
         }
         if ((rc = DISPATCH(h, do_step, h, dt, 1.0))) return rc;
+        /* the source is read on the handle's stream: after its conversion, wherever the
+         * handle runs that (st_set_finalize_overlap) */
+        if ((rc = join_fin(h))) return rc;
         {
             ProfScope ps(h, ST_KERNEL_OTHER);
             CK(launch_convert(h->dsrc, 8, is->second.dptr, is->second.tbytes, ncomp,
@@ -2657,7 +2660,7 @@ int st_evolve_cloud(double dt)
         h->dsrc32 = static_cast<float*>(h->dstage);
         rc = DISPATCH(h, do_step, h, dt, 1.0);
         h->dsrc32 = nullptr;
-        if (rc) return rc;
+        if (rc || (rc = join_fin(h))) return rc;
         /* source device -> host (A:1148-1152) */
         CK(cudaMemcpyAsync(is->second.ptr, h->dstage, ncomp * 4, cudaMemcpyDeviceToHost,
                            h->stream));
@@ -2717,7 +2720,9 @@ int st_evolve_cloud_async(double dt)
     const int ub = iu->second.tbytes;
     CK(cudaMemcpyAsync(A.duraw, iu->second.ptr, ncomp * ub, cudaMemcpyHostToDevice, A.copy));
     CK(cudaEventRecord(A.up, A.copy));
-    /* after step k-1: its bookkeeping, then est_k from its source */
+    /* after step k-1: its bookkeeping, then est_k from its source (once its conversion,
+     * wherever the handle runs that, has finished) */
+    if ((rc = join_fin(h))) return rc;
     CK(cudaMemcpyAsync(A.hctl, h->dctl, sizeof(CloudCtl) * nc, cudaMemcpyDeviceToHost,
                        h->stream));
     {

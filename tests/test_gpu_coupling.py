@@ -126,3 +126,35 @@ def test_setup_with_another_mesh_rejects_old_exchange_arrays():
         st.finalize()
     _setup(4)                      # a fresh allocation after st_finalize works again
     st.finalize()
+
+
+@pytest.mark.parametrize("mode", ["copy", "mapped"])
+@pytest.mark.parametrize("tbytes", [4, 8])
+def test_sync_shim_with_overlapped_finalize_turned_on(tbytes, mode):
+    """The shims' default handle converts each step's source in line; a caller may turn the
+    overlapped conversion on for it (st_set_finalize_overlap), and st_evolve_cloud must then
+    still hand out each step's own source, in both exchange modes."""
+    ref = _true_sources(tbytes)
+    U, UT = _setup(tbytes)
+    try:
+        st.set_exchange_mode(mode)
+        assert st.lib().st_set_finalize_overlap(st.default_handle(), 1) == 0
+        for k, Uk in enumerate(_fields()):
+            U[:] = Uk
+            st.evolve_cloud(workload.DT)
+            assert np.array_equal(UT.astype(np.float64), ref[k]), f"step {k}"
+    finally:
+        st.finalize()
+
+
+def test_async_shim_with_overlapped_finalize_turned_on():
+    ref = _async_outputs(8)
+    U, UT = _setup(8)
+    try:
+        assert st.lib().st_set_finalize_overlap(st.default_handle(), 1) == 0
+        for k, Uk in enumerate(_fields()):
+            U[:] = Uk
+            st.evolve_cloud_async(workload.DT)
+            assert np.array_equal(UT.astype(np.float64), ref[k]), f"call {k}"
+    finally:
+        st.finalize()
