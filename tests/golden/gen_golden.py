@@ -843,43 +843,42 @@ def run_tet_case(c):
                 src_quant=fixed_point_source(logs, nt, npcl, c["nsub"], 1 if mixed else 2))
 
 
-def main():
-    os.makedirs(os.path.join(HERE, "tet"), exist_ok=True)
+def main(folder=HERE, verbose=True):
+    """Writes every fixture under `folder` (this script's folder by default)."""
+    os.makedirs(os.path.join(folder, "tet"), exist_ok=True)
+    say = print if verbose else (lambda *a: None)
     for name, c in TET_CASES.items():
-        out = run_tet_case(c)
-        np.savez(os.path.join(HERE, "tet", name + ".npz"), **out)
-        moved = int(np.sum(out["cells"] != out["cells0"]))
-        print(f"{name}: {c['npcl']} parcels, changed tet {moved}, hops {out['hop_hist'].tolist()}, "
-              f"|src| max {np.abs(out['src_f64']).max():.3e}")
+        res = run_tet_case(c)
+        np.savez(os.path.join(folder, "tet", name + ".npz"), **res)
+        say(f"{name}: {c['npcl']} parcels, changed tet {int(np.sum(res['cells'] != res['cells0']))}, "
+            f"hops {res['hop_hist'].tolist()}, |src| max {np.abs(res['src_f64']).max():.3e}")
     for name, c in CASES64.items():
         xyz, uvw, d, Ucell = make_inputs64(c["seed"], c["n"], c["npcl"], c["ending"], c["dmin"],
                                            c["dmax"], c["precision"], dlog=c.get("dlog", False))
         fsc = fluid_factors(c["nsteps"])
-        out = run_case_p64([c["n"]] * 3, [0.0] * 3, [c["ending"]] * 3, c["mu_c"], c["rho_c"],
+        res = run_case_p64([c["n"]] * 3, [0.0] * 3, [c["ending"]] * 3, c["mu_c"], c["rho_c"],
                            c["rho_d"], c["drag"], c["nsub"], xyz, uvw, d, Ucell, c["dt"],
                            c["nsteps"], fsc, c["precision"])
         meta = np.array([c["n"], c["nsub"], c["drag"], c["nsteps"]], dtype=np.int64)
         phys = np.array([c["ending"], c["mu_c"], c["rho_c"], c["rho_d"], c["dt"]])
-        np.savez(os.path.join(HERE, name + ".npz"), meta=meta, phys=phys, xyz0=xyz, uvw0=uvw,
-                 d=d, U=Ucell, fscale=fsc, precision=np.array(c["precision"]), **out)
-        moved_cells = int(np.sum(out["cells"] != _cells0_64(c, xyz)))
-        print(f"{name}: {c['npcl']} parcels, changed cell {moved_cells}, "
-              f"|src| max {np.abs(out['src_f64']).max():.3e}")
+        np.savez(os.path.join(folder, name + ".npz"), meta=meta, phys=phys, xyz0=xyz, uvw0=uvw,
+                 d=d, U=Ucell, fscale=fsc, precision=np.array(c["precision"]), **res)
+        say(f"{name}: {c['npcl']} parcels, changed cell "
+            f"{int(np.sum(res['cells'] != _cells0_64(c, xyz)))}, "
+            f"|src| max {np.abs(res['src_f64']).max():.3e}")
     for name, c in CASES.items():
         xyz, uvw, d, Ucell = make_inputs(c["seed"], c["n"], c["npcl"], c["ending"], c["dmin"],
                                          c["dmax"], c.get("v0_random", False))
-        out = run_case([c["n"]] * 3, [0.0] * 3, [c["ending"]] * 3, c["mu_c"], c["rho_c"],
+        res = run_case([c["n"]] * 3, [0.0] * 3, [c["ending"]] * 3, c["mu_c"], c["rho_c"],
                        c["rho_d"], c["drag"], c["nsub"], xyz, uvw, d, Ucell, c["dt"],
                        c["nsteps"])
         meta = np.array([c["n"], c["nsub"], c["drag"], c["nsteps"]], dtype=np.int64)
         phys = np.array([c["ending"], c["mu_c"], c["rho_c"], c["rho_d"], c["dt"]])
-        np.savez(os.path.join(HERE, name + ".npz"), meta=meta, phys=phys, xyz0=xyz, uvw0=uvw,
-                 d=d, U=Ucell, **out)
-        moved = int(np.sum(out["cells"] >= 0))
-        x0 = xyz.astype(np.float64)
-        moved_cells = int(np.sum(out["cells"] != _cells0(c, xyz)))
-        print(f"{name}: {c['npcl']} parcels, located {moved}, changed cell {moved_cells}, "
-              f"|src| max {np.abs(out['src_f64']).max():.3e}")
+        np.savez(os.path.join(folder, name + ".npz"), meta=meta, phys=phys, xyz0=xyz, uvw0=uvw,
+                 d=d, U=Ucell, **res)
+        say(f"{name}: {c['npcl']} parcels, located {int(np.sum(res['cells'] >= 0))}, "
+            f"changed cell {int(np.sum(res['cells'] != _cells0(c, xyz)))}, "
+            f"|src| max {np.abs(res['src_f64']).max():.3e}")
 
 
 if __name__ == "__main__":

@@ -215,3 +215,23 @@ def test_lost_parcel_left_unchanged(oracle_lib):
     r = oracle.run(cfg, xyz, uvw, np.array([1e-3, 1e-3]), np.ones((64, 3)), 1, 1e-3)
     assert r["lost"] == 1 and (r["status"] & 1)
     assert r["xyz"][0, 1] == 1.5 and r["cells"][1] == -1
+
+
+def test_golden_fixtures_are_what_their_script_makes(tmp_path):
+    """The committed fixtures are exactly the output of tests/golden/gen_golden.py (regenerated
+    here into a temporary folder), so none was edited by hand."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location(
+        "gen_golden", os.path.join(HERE, "golden", "gen_golden.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    gen.main(str(tmp_path), verbose=False)
+    paths = GOLDEN + sorted(glob.glob(os.path.join(HERE, "golden", "tet", "*.npz")))
+    assert len(paths) == 13
+    for path in paths:
+        a = np.load(path)
+        b = np.load(os.path.join(str(tmp_path), os.path.relpath(path, os.path.join(HERE, "golden"))))
+        assert set(a.files) == set(b.files), path
+        for k in a.files:
+            assert np.array_equal(a[k], b[k]), (path, k)
