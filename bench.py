@@ -226,7 +226,10 @@ class DeviceTimer:
 
     def __init__(self, torch, stream_ptr, device):
         self.torch = torch
-        self.stream = torch.cuda.ExternalStream(stream_ptr, device=device)
+        # the library's own stream, or torch's default stream (pointer 0) when the library
+        # was set to run on it (the multi-rank path)
+        self.stream = (torch.cuda.ExternalStream(stream_ptr, device=device) if stream_ptr
+                       else torch.cuda.default_stream(device))
         self.a = torch.cuda.Event(enable_timing=True)
         self.b = torch.cuda.Event(enable_timing=True)
 

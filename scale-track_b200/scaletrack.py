@@ -414,7 +414,9 @@ class ParcelTracker:
         _check(lib().st_synchronize(self._h))
 
     def stream(self):
-        return lib().st_get_stream(self._h)
+        """The handle's cudaStream_t as an int (0: the legacy default stream, e.g. after
+        st_set_stream with torch's default stream)."""
+        return lib().st_get_stream(self._h) or 0
 
     def profile(self, on=True):
         _check(lib().st_profile_enable(self._h, 1 if on else 0))

@@ -71,5 +71,18 @@ def test_bench_sharded_step_on_one_rank_equals_plain_step(prec):
             xc, uc, _ = hc.get_parcels()
             xs, us, _ = hs.get_parcels()
             assert np.array_equal(xc, xs) and np.array_equal(uc, us)
+            # the rest of a rank's timed loop: CUDA events on the stream the library now
+            # shares with torch, the stop after the last source, the slowest rank's time
+            timer = bench.DeviceTimer(torch, hs.stream(), dev)
+            torch.cuda.synchronize()
+            dist.barrier()
+            timer.start()
+            for k in range(3):
+                step(workload.DT, workload.fluid_scale(steps + k))
+            hs.source_device_ptr(0)
+            ms = timer.stop()
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            assert float(t.item()) == ms > 0.0
     finally:
         dist.destroy_process_group()
