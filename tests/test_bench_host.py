@@ -42,3 +42,26 @@ def test_algorithmic_bytes_of_the_configured_step():
     assert round(workload.step_kernel_bytes("mixed", n, ncells) / 1e6) == 785
     nt = 6 * 96 ** 3
     assert workload.tet_step_kernel_bytes("mixed", 20_000_000, nt) == 20_000_000 * 84 + nt * 156
+
+
+def test_reference_arm_under_two_ranks_prints_one_line():
+    """`bench.py --impl reference` launched by torchrun with two ranks: rank 0 alone times the
+    reference's CPU path and prints one JSON line; the other rank exits 0 without output."""
+    import json
+    import socket
+    import subprocess
+    import sys
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl",
+           "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--nparcels", "20000"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
